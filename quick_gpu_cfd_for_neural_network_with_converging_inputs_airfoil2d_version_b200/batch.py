@@ -1,0 +1,143 @@
+"""Python mirror of the batched C API (amr_batch_* in include/amr_b200.h).
+
+Many meshes live in one device arena; each case keeps its own time, dt, retry counter and
+status, and is retired by the reference driver's steady rule (src/quick_airfoil.cpp:180-208)
+evaluated on the device in FP64.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _abi, cases
+from ._lib import errbuf, lib
+
+
+class BatchError(RuntimeError):
+    pass
+
+
+def case_control(tend, maxsteps, steady=True, mach=1.65, aoa=1.5, **kw):
+    c = _abi.CaseControl()
+    s = dict(cases.STEADY)
+    s.update(kw)
+    c.tend, c.maxsteps = float(tend), int(maxsteps)
+    c.first_check = s['first_check']
+    c.check_period = s['check_period'] if steady else 0.0
+    c.min_time, c.raw_tol, c.load_tol, c.hold = s['min_time'], s['raw_tol'], s['load_tol'], int(s['hold'])
+    for i in range(4):
+        c.region[i] = s['region'][i]
+    c.moment_x, c.moment_y = s['moment_x'], s['moment_y']
+    c.mach, c.aoa_degrees = mach, aoa
+    return c
+
+
+class Batch:
+    def __init__(self, precision=32, model=_abi.MODEL_LAMINAR, sa=True, flux=_abi.FLUX_HLLC, max_cases=256,
+                 max_cells=0, max_faces=0, max_walls=0, max_terms=0, max_srd=0, hbm_bytes=0, block_threads=0,
+                 grid_blocks=0, device=0):
+        cfg = _abi.BatchConfig()
+        cfg.precision, cfg.device, cfg.model, cfg.sa_model, cfg.flux = precision, device, model, int(sa), flux
+        cfg.max_cases = max_cases
+        cfg.max_cells, cfg.max_faces, cfg.max_walls, cfg.max_terms, cfg.max_srd = max_cells, max_faces, max_walls, max_terms, max_srd
+        cfg.hbm_bytes, cfg.block_threads, cfg.grid_blocks = hbm_bytes, block_threads, grid_blocks
+        out = C.c_void_p()
+        err = errbuf()
+        if lib().amr_batch_create(C.byref(cfg), C.byref(out), err, len(err)):
+            raise BatchError(err.value.decode())
+        self._h = out.value
+        self.nv = 5 if (model == _abi.MODEL_LAMINAR and sa) else 4
+        self.ncells = {}
+
+    def admit(self, mesh, params, u0, control):
+        u0 = np.ascontiguousarray(u0, dtype=np.float64)
+        view = mesh.view()
+        slot = C.c_int32(-1)
+        err = errbuf()
+        st = lib().amr_batch_admit(self._h, C.byref(view), C.byref(params), u0.ctypes.data, len(u0), C.byref(control),
+                                   C.byref(slot), err, len(err))
+        if st == 3:
+            return None
+        if st:
+            raise BatchError(err.value.decode())
+        self.ncells[slot.value] = mesh.n_cells
+        return slot.value
+
+    def advance(self, trials=32):
+        err = errbuf()
+        if lib().amr_batch_advance(self._h, int(trials), err, len(err)):
+            raise BatchError(err.value.decode())
+
+    def check(self):
+        err = errbuf()
+        if lib().amr_batch_check(self._h, err, len(err)):
+            raise BatchError(err.value.decode())
+
+    def status(self, slot):
+        s = _abi.CaseStatus()
+        lib().amr_batch_status(self._h, int(slot), C.byref(s))
+        return dict(time=s.time, steps=s.steps, rejected=s.rejected, status=s.status, finished=s.finished,
+                    converged=s.converged, checks=s.checks, hold=s.hold, residual=list(s.residual), cl=s.cl, cd=s.cd,
+                    cm=s.cm)
+
+    def download(self, slot):
+        u = np.empty(self.nv * self.ncells[slot])
+        err = errbuf()
+        if lib().amr_batch_download(self._h, int(slot), u.ctypes.data, len(u), err, len(err)):
+            raise BatchError(err.value.decode())
+        return u
+
+    def residual(self, slot):
+        r = np.empty(self.nv * self.ncells[slot])
+        err = errbuf()
+        if lib().amr_batch_residual(self._h, int(slot), r.ctypes.data, len(r), err, len(err)):
+            raise BatchError(err.value.decode())
+        return r
+
+    def set_target(self, slot, target, maxsteps):
+        err = errbuf()
+        if lib().amr_batch_set_target(self._h, int(slot), float(target), int(maxsteps), err, len(err)):
+            raise BatchError(err.value.decode())
+
+    def release(self, slot):
+        lib().amr_batch_release(self._h, int(slot))
+        self.ncells.pop(slot, None)
+
+    def autotune(self, trials=4):
+        err = errbuf()
+        if lib().amr_batch_autotune(self._h, int(trials), err, len(err)):
+            raise BatchError(err.value.decode())
+
+    def set_graph(self, on):
+        lib().amr_batch_set_graph(self._h, int(bool(on)))
+
+    def launch_config(self):
+        b = errbuf(128)
+        lib().amr_batch_launch_config(self._h, b, len(b))
+        return b.value.decode()
+
+    @property
+    def live(self):
+        return lib().amr_batch_live_cases(self._h)
+
+    @property
+    def free_cells(self):
+        return lib().amr_batch_free_cells(self._h)
+
+    @property
+    def last_advance_seconds(self):
+        return lib().amr_batch_last_advance_seconds(self._h)
+
+    @property
+    def kernel_launches(self):
+        return lib().amr_batch_kernel_launches(self._h)
+
+    def destroy(self):
+        if self._h:
+            lib().amr_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass

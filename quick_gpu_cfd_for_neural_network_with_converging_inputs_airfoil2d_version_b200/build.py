@@ -1,0 +1,75 @@
+"""Builds libamr_b200.so (sm_100a) in the package directory.
+
+    python -m quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200.build
+
+The FP64 unit is compiled with -fmad=false so its arithmetic rounds exactly like the
+reference CPU code; the FP32 unit keeps contraction on.
+"""
+import concurrent.futures
+import os
+import pathlib
+import shutil
+import subprocess
+import sys
+
+PKG = pathlib.Path(__file__).resolve().parent
+CSRC = PKG / 'csrc'
+BUILD = PKG / '_build'
+LIB = PKG / 'libamr_b200.so'
+ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
+COMMON = ['-O3', '-std=c++17', '-lineinfo', '-Xcompiler', '-fPIC', '-I', str(PKG.parent / 'include')]
+UNITS = {
+    'amr_engine_f64.cu': ['-fmad=false'],
+    'amr_engine_f32.cu': [],
+    'amr_capi.cu': [],
+}
+
+
+def nvcc():
+    path = shutil.which('nvcc') or '/usr/local/cuda/bin/nvcc'
+    if not os.path.exists(path):
+        raise RuntimeError('nvcc not found')
+    return path
+
+
+def _sources():
+    return sorted(CSRC.glob('*.cu')) + sorted(CSRC.glob('*.cuh')) + sorted(CSRC.glob('*.h')) + [PKG.parent / 'include' / 'amr_b200.h']
+
+
+def up_to_date():
+    if not LIB.exists():
+        return False
+    t = LIB.stat().st_mtime
+    return all(s.stat().st_mtime <= t for s in _sources())
+
+
+def build(force=False, verbose=False):
+    if not force and up_to_date():
+        return LIB
+    BUILD.mkdir(exist_ok=True)
+    cc = nvcc()
+
+    def compile_unit(item):
+        name, extra = item
+        obj = BUILD / (name + '.o')
+        cmd = [cc, *ARCH, *COMMON, *extra, '-c', str(CSRC / name), '-o', str(obj)]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode:
+            raise RuntimeError(f'nvcc failed for {name}:\n{r.stderr[-4000:]}')
+        if verbose:
+            print(r.stderr)
+        return obj
+
+    with concurrent.futures.ThreadPoolExecutor(max_workers=len(UNITS)) as ex:
+        objs = list(ex.map(compile_unit, UNITS.items()))
+    tmp = LIB.with_suffix('.so.tmp')
+    r = subprocess.run([cc, *ARCH, '-shared', '-o', str(tmp), *map(str, objs), '-lcudart'], capture_output=True, text=True)
+    if r.returncode:
+        raise RuntimeError('link failed:\n' + r.stderr[-4000:])
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == '__main__':
+    build(force='--force' in sys.argv, verbose='-v' in sys.argv)
+    print(LIB)

@@ -147,3 +147,13 @@ class CaseSpec:
 
     def initial_primitive(self, gamma=1.4):
         return freestream(self.mach, self.aoa, gamma)
+
+
+def initial_state(mesh, w, gamma=1.4):
+    """Uniform conserved state from primitives w = (rho, u, v, p), SoA u[var*n + cell]
+    (the reference's static_amr2d_initialize, src/static_amr2d.cpp:360-367)."""
+    n = mesh.n_cells
+    values = [w[0], w[0] * w[1], w[0] * w[2], w[3] / (gamma - 1) + 0.5 * w[0] * (w[1] * w[1] + w[2] * w[2])]
+    if mesh.nv == 5:
+        values.append(w[0] * float(mesh.transport['sa_nu_inf'][0]))
+    return np.concatenate([np.full(n, v, dtype=np.float64) for v in values])

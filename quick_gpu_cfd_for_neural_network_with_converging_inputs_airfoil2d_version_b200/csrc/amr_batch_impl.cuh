@@ -1,0 +1,995 @@
+// amr_batch_impl.cuh -- the batch arena and its launches, templated on the state precision.
+//
+// A Batch owns device tables sized at creation (cells, slots, walls, gradient terms, SRD
+// lists, cases, tiles).  Admission converts one reference-layout mesh into the engine layout
+// (amr_engine.cuh) inside free ranges of those tables; release returns the ranges.  Advance
+// replays one cooperative launch of the persistent trial kernel plus the control read-back,
+// captured in a CUDA graph that is recaptured whenever the case set changes.
+#pragma once
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "amr_engine.cuh"
+#include "amr_host.h"
+
+namespace amrb {
+
+inline bool cuda_ok(cudaError_t st, std::string* error, const char* what) {
+  if (st == cudaSuccess) return true;
+  if (error) *error = std::string(what) + ": " + cudaGetErrorString(st);
+  return false;
+}
+
+// First-fit allocator of index ranges.
+class RangeAlloc {
+ public:
+  explicit RangeAlloc(long long capacity = 0) : capacity_(capacity) {
+    if (capacity > 0) free_[0] = capacity;
+  }
+  long long alloc(long long n) {
+    if (n <= 0) return 0;
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second >= n) {
+        const long long b = it->first, size = it->second;
+        free_.erase(it);
+        if (size > n) free_[b + n] = size - n;
+        return b;
+      }
+    }
+    return -1;
+  }
+  void release(long long b, long long n) {
+    if (n <= 0) return;
+    auto it = free_.emplace(b, n).first;
+    auto next = std::next(it);
+    if (next != free_.end() && it->first + it->second == next->first) {
+      it->second += next->second;
+      free_.erase(next);
+    }
+    if (it != free_.begin()) {
+      auto prev = std::prev(it);
+      if (prev->first + prev->second == it->first) {
+        prev->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+  long long free_total() const {
+    long long s = 0;
+    for (auto& kv : free_) s += kv.second;
+    return s;
+  }
+  long long capacity() const { return capacity_; }
+
+ private:
+  long long capacity_;
+  std::map<long long, long long> free_;
+};
+
+template <class T> struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  bool alloc(size_t count, uint64_t* counter, std::string* error, const char* what) {
+    n = count ? count : 1;
+    if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&p), n * sizeof(T)), error, what)) return false;
+    if (counter) *counter += n * sizeof(T);
+    return true;
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+  }
+};
+
+struct Range {
+  long long b = 0, n = 0;
+};
+
+template <class R> struct HostCase {
+  bool live = false;
+  int n = 0;
+  Range cells, slots, walls, terms, groups, gmembers, qcells, qlist;
+  int slot = -1;
+  std::vector<int> nslot, nterm;  // per-cell slot and gradient-term counts (for tiling)
+  std::vector<Tile> tiles;
+  CaseCfg<R> cfg;
+};
+
+template <class R> class Batch final : public BatchBase {
+ public:
+  Batch() = default;
+  ~Batch() override { destroy(); }
+
+  bool init(const amr_batch_config_t& c, std::string* error) {
+    config_ = c;
+    model_ = c.model == AMR_B200_MODEL_EULER ? MODEL_EULER : (c.sa_model ? MODEL_SA : MODEL_LAMINAR);
+    flux_ = c.flux == AMR_B200_FLUX_AUSMPUP ? FLUX_AUSM : FLUX_HLLC;
+    nv_ = model_ == MODEL_SA ? 5 : 4;
+    if (c.max_cases < 1) return fail(error, "max_cases must be positive");
+    if (!cuda_ok(cudaSetDevice(c.device), error, "cudaSetDevice")) return false;
+    cudaDeviceProp prop;
+    if (!cuda_ok(cudaGetDeviceProperties(&prop, c.device), error, "device properties")) return false;
+    sms_ = prop.multiProcessorCount;
+    clock_khz_ = 1965000;
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrClockRate, c.device) == cudaSuccess && v > 0) clock_khz_ = v;
+    if (!prop.cooperativeLaunch) return fail(error, "device lacks cooperative launch");
+    long long cells = c.max_cells, slots = c.max_faces, walls = c.max_walls, terms = c.max_terms, srd = c.max_srd;
+    if (cells == 0) {
+      // size from the HBM budget: ~bytes per cell of tables and state for this model
+      const double per_cell = (model_ == MODEL_EULER ? 260.0 : 520.0) * sizeof(R) / 4.0 + 120.0;
+      const uint64_t budget = c.hbm_bytes ? c.hbm_bytes : (uint64_t)4 << 30;
+      cells = (long long)(budget / per_cell);
+    }
+    if (slots == 0) slots = 5 * cells;
+    if (walls == 0) walls = cells / 8 + 64 * c.max_cases;
+    if (terms == 0) terms = model_ == MODEL_EULER ? 1 : 6 * cells;
+    if (srd == 0) srd = cells / 8 + 64 * c.max_cases;
+    cap_cells_ = cells + c.max_cases;  // one closing entry per case
+    cap_slots_ = slots;
+    cap_walls_ = walls;
+    cap_terms_ = std::max<long long>(terms, 1);
+    cap_groups_ = srd;
+    cap_gmem_ = 8 * srd;
+    cap_q_ = 2 * srd;
+    cap_qlist_ = 8 * srd;
+    cap_tiles_ = cap_cells_ / 16 + 4 * c.max_cases;
+    a_cells_ = RangeAlloc(cap_cells_);
+    a_slots_ = RangeAlloc(cap_slots_);
+    a_walls_ = RangeAlloc(cap_walls_);
+    a_terms_ = RangeAlloc(cap_terms_);
+    a_groups_ = RangeAlloc(cap_groups_ + c.max_cases);
+    a_gmem_ = RangeAlloc(cap_gmem_);
+    a_q_ = RangeAlloc(cap_q_ + c.max_cases);
+    a_qlist_ = RangeAlloc(cap_qlist_);
+    cases_.assign(c.max_cases, HostCase<R>());
+    meta_.assign(c.max_cases, CaseMeta{});
+    if (!cuda_ok(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), error, "stream")) return false;
+    if (!cuda_ok(cudaEventCreate(&ev0_), error, "event") || !cuda_ok(cudaEventCreate(&ev1_), error, "event")) return false;
+    uint64_t* A = &stats_.allocated_bytes;
+    const long long nc = cap_cells_;
+    bool ok = ctl_.alloc(c.max_cases, A, error, "ctl") && cfg_.alloc(c.max_cases, A, error, "cfg") &&
+              tiles_.alloc(cap_tiles_, A, error, "tiles") && bar_.alloc(1, A, error, "barrier") &&
+              c_case_.alloc(nc, A, error, "cells") && c_vol_.alloc(nc, A, error, "cells") &&
+              c_area_.alloc(nc, A, error, "cells") && c_gvol_.alloc(nc, A, error, "cells") &&
+              c_flags_.alloc(nc, A, error, "cells") && c_slot_.alloc(nc, A, error, "cells") &&
+              c_wall_.alloc(nc, A, error, "cells") && c_term_.alloc(nc, A, error, "cells") &&
+              c_cx_.alloc(nc, A, error, "cells") && c_cy_.alloc(nc, A, error, "cells") &&
+              s_own_.alloc(cap_slots_, A, error, "slots") && s_nb_.alloc(cap_slots_, A, error, "slots") &&
+              s_meta_.alloc(cap_slots_, A, error, "slots") && s_len_.alloc(cap_slots_, A, error, "slots") &&
+              w_nx_.alloc(cap_walls_, A, error, "walls") && w_ny_.alloc(cap_walls_, A, error, "walls") &&
+              w_len_.alloc(cap_walls_, A, error, "walls") && w_dist_.alloc(cap_walls_, A, error, "walls") &&
+              w_donor_.alloc(cap_walls_, A, error, "walls") && w_xm_.alloc(cap_walls_, A, error, "walls") &&
+              w_ym_.alloc(cap_walls_, A, error, "walls") &&
+              g_mem_.alloc(cap_groups_ + c.max_cases, A, error, "srd") && g_cell_.alloc(cap_gmem_, A, error, "srd") &&
+              g_cnt_.alloc(cap_gmem_, A, error, "srd") && g_vol_.alloc(cap_groups_ + c.max_cases, A, error, "srd") &&
+              q_cell_.alloc(cap_q_ + c.max_cases, A, error, "srd") && q_grp_.alloc(cap_q_ + c.max_cases, A, error, "srd") &&
+              q_list_.alloc(cap_qlist_, A, error, "srd") && q_cnt_.alloc(cap_q_ + c.max_cases, A, error, "srd") &&
+              qhat_.alloc(4 * (cap_groups_ + c.max_cases), A, error, "srd") &&
+              U0_.alloc(nv_ * nc, A, error, "state") && U1_.alloc(nv_ * nc, A, error, "state") &&
+              U2_.alloc(nv_ * nc, A, error, "state") && R0_.alloc(nv_ * nc, A, error, "state") &&
+              diag_part_.alloc(9 * cap_tiles_, A, error, "diag") && diag_out_.alloc(9 * c.max_cases, A, error, "diag") &&
+              diag_cfg_.alloc(7 * c.max_cases, A, error, "diag") && case_tiles_.alloc(2 * c.max_cases, A, error, "diag");
+    if (!ok) return false;
+    if (model_ >= MODEL_LAMINAR) {
+      ok = s_geo_.alloc(6 * cap_slots_, A, error, "slots") && t_own_.alloc(cap_terms_, A, error, "terms") &&
+           t_src_.alloc(cap_terms_, A, error, "terms") && t_x_.alloc(cap_terms_, A, error, "terms") &&
+           t_y_.alloc(cap_terms_, A, error, "terms") && grad_.alloc(4 * nc, A, error, "scratch") &&
+           mu_.alloc(nc, A, error, "scratch") && eddy_.alloc(nc, A, error, "scratch");
+      if (!ok) return false;
+    }
+    if (model_ == MODEL_SA) {
+      ok = c_wd_.alloc(nc, A, error, "cells") && sgrad_.alloc(2 * nc, A, error, "scratch") &&
+           sdiff_.alloc(nc, A, error, "scratch") && ssrc_.alloc(nc, A, error, "scratch") &&
+           srate_.alloc(nc, A, error, "scratch");
+      if (!ok) return false;
+    }
+    cudaMemsetAsync(ctl_.p, 0, sizeof(CaseCtl) * c.max_cases, stream_);
+    cudaMemsetAsync(c_case_.p, 0xff, sizeof(int) * nc, stream_);
+    if (!cuda_ok(cudaHostAlloc(reinterpret_cast<void**>(&h_ctl_), sizeof(CaseCtl) * c.max_cases, cudaHostAllocDefault), error,
+                 "pinned control") ||
+        !cuda_ok(cudaHostAlloc(reinterpret_cast<void**>(&h_bar_), sizeof(GridBarrier), cudaHostAllocDefault), error,
+                 "pinned barrier"))
+      return false;
+    std::memset(h_ctl_, 0, sizeof(CaseCtl) * c.max_cases);
+    stats_.pinned_bytes += sizeof(CaseCtl) * c.max_cases + sizeof(GridBarrier);
+    block_ = c.block_threads > 0 ? c.block_threads : 256;
+    if (block_ % 32 || block_ < 64 || block_ > MAX_BLOCK) return fail(error, "block_threads must be 64..256, a multiple of 32");
+    grid_request_ = c.grid_blocks;
+    if (!configure_grid(error)) return false;
+    return cuda_ok(cudaStreamSynchronize(stream_), error, "batch init");
+  }
+
+  int admit(const amr_mesh_view_t* m, const amr_params_t* p, const double* u0, uint64_t u0_count, double time0,
+            long long steps0, long long rejected0, double target, long long maxsteps, int* slot_out,
+            std::string* error) override {
+    if (!m || !p || !u0) return fail1(error, "null mesh, parameters or state");
+    std::string why;
+    if (!validate(*m, *p, u0_count, &why)) return fail1(error, why);
+    if (!std::isfinite(time0) || time0 < 0) return fail1(error, "invalid initial time");
+    int slot = -1;
+    for (int i = 0; i < config_.max_cases; ++i)
+      if (!cases_[i].live) { slot = i; break; }
+    if (slot < 0) return 3;
+    HostCase<R> hc;
+    const long long n = (long long)m->n_cells;
+    const long long ns = (long long)m->face_offsets[n];
+    const long long nw = (long long)m->n_walls;
+    const long long nt = model_ >= MODEL_LAMINAR ? (long long)m->visc_offsets[n] : 0;
+    // SRD lists (only non-trivial neighbourhoods)
+    std::vector<unsigned char> simple(n, 1);
+    std::vector<int> group_index(n, -1);
+    std::vector<long long> groups_nt, cells_nt;
+    long long gmem = 0, qlist = 0;
+    const bool has_srd = m->small_cells > 0;
+    if (has_srd) {
+      for (long long k = 0; k < n; ++k) {
+        const uint64_t cnt = m->member_offsets[k + 1] - m->member_offsets[k];
+        const uint64_t size = m->group_offsets[k + 1] - m->group_offsets[k];
+        if (cnt == 0 || size == 0) return fail1(error, "empty SRD neighbourhood");
+        simple[k] = cnt == 1 && size == 1 && m->group_members[m->group_offsets[k]] == (uint64_t)k;
+      }
+      for (long long k = 0; k < n; ++k)
+        if (!simple[k]) {
+          group_index[k] = (int)groups_nt.size();
+          groups_nt.push_back(k);
+          gmem += (long long)(m->group_offsets[k + 1] - m->group_offsets[k]);
+          cells_nt.push_back(k);
+          qlist += (long long)(m->member_offsets[k + 1] - m->member_offsets[k]);
+        }
+      for (long long k : cells_nt)
+        for (uint64_t q = m->member_offsets[k]; q < m->member_offsets[k + 1]; ++q)
+          if (group_index[m->member_groups[q]] < 0) return fail1(error, "SRD neighbourhood references a trivial group");
+    }
+    // allocate ranges
+    hc.n = (int)n;
+    hc.cells = {a_cells_.alloc(n + 1), n + 1};
+    hc.slots = {a_slots_.alloc(ns), ns};
+    hc.walls = {a_walls_.alloc(nw), nw};
+    hc.terms = {a_terms_.alloc(nt), nt};
+    const long long ng = (long long)groups_nt.size();
+    hc.groups = {a_groups_.alloc(ng + 1), ng + 1};
+    hc.gmembers = {a_gmem_.alloc(gmem), gmem};
+    hc.qcells = {a_q_.alloc(ng + 1), ng + 1};
+    hc.qlist = {a_qlist_.alloc(qlist), qlist};
+    if (hc.cells.b < 0 || hc.slots.b < 0 || hc.walls.b < 0 || hc.terms.b < 0 || hc.groups.b < 0 || hc.gmembers.b < 0 ||
+        hc.qcells.b < 0 || hc.qlist.b < 0) {
+      release_ranges(hc);
+      return 3;
+    }
+    // tiles
+    hc.slot = slot;
+    hc.nslot.resize(n);
+    hc.nterm.assign(n, 0);
+    for (long long k = 0; k < n; ++k) {
+      hc.nslot[k] = (int)(m->face_offsets[k + 1] - m->face_offsets[k]);
+      if (model_ >= MODEL_LAMINAR) hc.nterm[k] = (int)(m->visc_offsets[k + 1] - m->visc_offsets[k]);
+    }
+    if (!make_tiles(hc, &why)) {
+      release_ranges(hc);
+      return fail1(error, why);
+    }
+    if (n_tiles_total() + (long long)hc.tiles.size() > cap_tiles_) {
+      release_ranges(hc);
+      return 3;
+    }
+    // build host staging arrays
+    const int cb = (int)hc.cells.b, sb = (int)hc.slots.b, wb = (int)hc.walls.b, tb = (int)hc.terms.b;
+    std::vector<int> c_case(n + 1, slot), c_slot(n + 1), c_wall(n + 1), c_term(n + 1);
+    c_case[n] = -1;
+    std::vector<double> c_vol(n + 1, 1.0), c_area(n + 1, 1.0), c_gvol(n + 1, 1.0), c_cx(n + 1, 0.0), c_cy(n + 1, 0.0);
+    std::vector<unsigned char> c_flags(n + 1, 0);
+    std::vector<R> c_wd(n + 1, R(1));
+    std::vector<int> s_own(ns), s_nb(ns), s_meta(ns);
+    std::vector<R> s_len(ns), s_geo(model_ >= MODEL_LAMINAR ? 6 * ns : 0);
+    std::vector<R> w_nx(nw), w_ny(nw), w_len(nw), w_dist(nw, R(1));
+    std::vector<double> w_xm(nw), w_ym(nw);
+    std::vector<int> w_donor(nw, cb);
+    std::vector<int> t_own(nt), t_src(nt);
+    std::vector<R> t_x(nt), t_y(nt);
+    int kinds[4];
+    for (int side = 0; side < 4; ++side) kinds[side] = m->boundaries[side].kind < 0 ? p->bc[side] : m->boundaries[side].kind;
+    long long wpos = 0;
+    for (long long k = 0; k < n; ++k) {
+      const amr_cell_t& c = m->cells[k];
+      c_vol[k] = c.volume;
+      c_area[k] = m->agglomerate_small ? c.volume : (c.x1 - c.x0) * (c.y1 - c.y0);
+      c_gvol[k] = has_srd ? m->group_volume[k] : 1.0;
+      c_flags[k] = has_srd && simple[k] ? 1 : 0;
+      c_cx[k] = c.cx;
+      c_cy[k] = c.cy;
+      c_slot[k] = sb + (int)m->face_offsets[k];
+      c_term[k] = tb + (model_ >= MODEL_LAMINAR ? (int)m->visc_offsets[k] : 0);
+      if (model_ == MODEL_SA) c_wd[k] = (R)m->wall_distance[k];
+      for (uint64_t q = m->face_offsets[k]; q < m->face_offsets[k + 1]; ++q) {
+        const uint64_t fi = m->cell_faces[q];
+        if (fi >= m->n_faces) return fail_release(hc, error, "cell_faces index out of range");
+        const amr_face_t& f = m->faces[fi];
+        const bool own_left = f.left == (int)k;
+        if (!own_left && f.right != (int)k) return fail_release(hc, error, "cell_faces lists a face of another cell");
+        const int other = own_left ? f.right : f.left;
+        if (other >= (int)n) return fail_release(hc, error, "face neighbour out of range");
+        if ((other < 0) != (f.boundary >= 0)) return fail_release(hc, error, "face boundary marker inconsistent");
+        const int side = f.boundary;
+        const int kind = side >= 0 ? kinds[side] : 0;
+        s_own[q] = cb + (int)k;
+        s_nb[q] = other >= 0 ? cb + other : -1;
+        s_meta[q] = (own_left ? 1 : 0) | ((f.axis & 1) << 1) | ((side + 1) << 2) | ((kind & 15) << 5);
+        s_len[q] = (R)f.length;
+        if (model_ >= MODEL_LAMINAR) {
+          const amr_face_geometry_t& g = m->face_geometry[fi];
+          s_geo[6 * q + 0] = (R)g.dx;
+          s_geo[6 * q + 1] = (R)g.dy;
+          s_geo[6 * q + 2] = (R)g.ex;
+          s_geo[6 * q + 3] = (R)g.ey;
+          s_geo[6 * q + 4] = (R)g.distance;
+          s_geo[6 * q + 5] = (R)m->face_samples[fi].distance;
+        }
+      }
+      c_wall[k] = wb + (int)wpos;
+      if (c.wall_begin != (uint64_t)wpos) return fail_release(hc, error, "walls are not grouped by owner cell");
+      for (uint64_t q = c.wall_begin; q < c.wall_begin + c.wall_count; ++q, ++wpos) {
+        const amr_wall_t& w = m->walls[q];
+        if (w.owner_cell != (uint64_t)k) return fail_release(hc, error, "wall owner mismatch");
+        w_nx[wpos] = (R)w.nx;
+        w_ny[wpos] = (R)w.ny;
+        w_len[wpos] = (R)w.length;
+        w_xm[wpos] = (w.x0 + w.x1) * .5;
+        w_ym[wpos] = (w.y0 + w.y1) * .5;
+        if (model_ >= MODEL_LAMINAR) {
+          const amr_wall_sample_t& s = m->wall_samples[q];
+          if (s.donor < 0 || s.donor >= n) return fail_release(hc, error, "wall donor out of range");
+          w_donor[wpos] = cb + s.donor;
+          w_dist[wpos] = (R)s.distance;
+        }
+      }
+      if (model_ >= MODEL_LAMINAR)
+        for (uint64_t q = m->visc_offsets[k]; q < m->visc_offsets[k + 1]; ++q) {
+          const amr_gradient_term_t& t = m->visc_terms[q];
+          t_own[q] = cb + (int)k;
+          if (t.source >= n) return fail_release(hc, error, "gradient source out of range");
+          t_src[q] = t.source >= 0 ? cb + t.source : (t.source == -1 ? -1 : -2 - t.side);
+          if (t.source == -2 && (t.side < 0 || t.side > 3)) return fail_release(hc, error, "gradient wall side out of range");
+          t_x[q] = (R)t.x;
+          t_y[q] = (R)t.y;
+        }
+    }
+    if (wpos != nw) return fail_release(hc, error, "wall count mismatch");
+    c_slot[n] = sb + (int)ns;
+    c_wall[n] = wb + (int)nw;
+    c_term[n] = tb + (int)nt;
+    // SRD arrays
+    const int gb = (int)hc.groups.b, gmb = (int)hc.gmembers.b, qb = (int)hc.qcells.b, qlb = (int)hc.qlist.b;
+    std::vector<int> g_mem(ng + 1), g_cell(gmem), q_cell(ng + 1, cb + (int)n), q_grp(ng + 1), q_list(qlist);
+    std::vector<double> g_cnt(gmem), g_vol(ng + 1, 1.0), q_cnt(ng + 1, 1.0);
+    {
+      long long pos = 0;
+      for (long long gi = 0; gi < ng; ++gi) {
+        const long long g = groups_nt[gi];
+        g_mem[gi] = gmb + (int)pos;
+        g_vol[gi] = m->group_volume[g];
+        for (uint64_t q = m->group_offsets[g]; q < m->group_offsets[g + 1]; ++q, ++pos) {
+          const uint64_t k = m->group_members[q];
+          g_cell[pos] = cb + (int)k;
+          g_cnt[pos] = (double)(m->member_offsets[k + 1] - m->member_offsets[k]);
+        }
+      }
+      g_mem[ng] = gmb + (int)pos;
+      long long lpos = 0;
+      for (long long qi = 0; qi < ng; ++qi) {
+        const long long k = cells_nt[qi];
+        q_cell[qi] = cb + (int)k;
+        q_grp[qi] = qlb + (int)lpos;
+        q_cnt[qi] = (double)(m->member_offsets[k + 1] - m->member_offsets[k]);
+        for (uint64_t q = m->member_offsets[k]; q < m->member_offsets[k + 1]; ++q, ++lpos)
+          q_list[lpos] = gb + group_index[m->member_groups[q]];
+      }
+      q_grp[ng] = qlb + (int)lpos;
+    }
+    // per-case constants
+    CaseCfg<R>& cf = hc.cfg;
+    std::memset(&cf, 0, sizeof(cf));
+    cf.cfl = p->cfl;
+    cf.dt_fixed = p->dt_fixed;
+    cf.viscous_cfl = m->transport.viscous_cfl;
+    cf.sa_cfl = m->transport.sa_cfl;
+    cf.gamma = (R)p->gamma;
+    cf.mco = (R)p->ausm_mco;
+    for (int side = 0; side < 4; ++side) {
+      const amr_boundary_t& b = m->boundaries[side];
+      cf.kind[side] = kinds[side];
+      Bnd<R>& d = cf.bnd[side];
+      d.kind = kinds[side];
+      for (int v = 0; v < 4; ++v) d.ref[v] = (R)b.reference[v];
+      d.total_pressure = (R)b.total_pressure;
+      d.total_temperature = (R)b.total_temperature;
+      d.gas_constant = (R)b.gas_constant;
+      d.dir[0] = (R)b.direction[0];
+      d.dir[1] = (R)b.direction[1];
+      d.outlet_pressure = (R)b.outlet_pressure;
+      d.wall_velocity[0] = (R)b.wall_velocity[0];
+      d.wall_velocity[1] = (R)b.wall_velocity[1];
+    }
+    cf.trn.law = m->transport.law;
+    cf.trn.mu_ref = (R)m->transport.mu_ref;
+    cf.trn.gas_constant = (R)m->transport.gas_constant;
+    cf.trn.temperature_ref = (R)m->transport.temperature_ref;
+    cf.trn.sutherland = (R)m->transport.sutherland;
+    cf.trn.viscous_cfl = (R)m->transport.viscous_cfl;
+    cf.trn.sa_nu_inf = (R)m->transport.sa_nu_inf;
+    cf.trn.sa_cfl = (R)m->transport.sa_cfl;
+    cf.agglomerated = m->agglomerate_small ? 1 : 0;
+    cf.has_srd = has_srd && ng > 0 ? 1 : 0;
+    cf.srd_g0 = gb;
+    cf.srd_g1 = gb + (int)ng;
+    cf.srd_q0 = qb;
+    cf.srd_q1 = qb + (int)ng;
+    // state
+    const long long ncap = cap_cells_;
+    std::vector<R> u(nv_ * (n + 1), R(1));
+    for (int v = 0; v < nv_; ++v)
+      for (long long k = 0; k < n; ++k) u[v * (n + 1) + k] = (R)u0[v * n + k];
+    // control
+    CaseCtl ctl;
+    std::memset(&ctl, 0, sizeof(ctl));
+    ctl.time = time0;
+    ctl.target = target;
+    ctl.steps = steps0;
+    ctl.rejected = rejected0;
+    ctl.maxsteps = maxsteps;
+    ctl.finished = time0 >= target;
+    ctl.live = 1;
+    ctl.cur = 0;
+    ctl.dtmin = DT_INF_BITS;
+    // uploads
+    uint64_t* G = &stats_.geometry_h2d_bytes;
+    bool ok = up(c_case_.p + cb, c_case, G) && up(c_vol_.p + cb, c_vol, G) && up(c_area_.p + cb, c_area, G) &&
+              up(c_gvol_.p + cb, c_gvol, G) && up(c_flags_.p + cb, c_flags, G) && up(c_slot_.p + cb, c_slot, G) &&
+              up(c_wall_.p + cb, c_wall, G) && up(c_term_.p + cb, c_term, G) && up(c_cx_.p + cb, c_cx, G) &&
+              up(c_cy_.p + cb, c_cy, G) && up(s_own_.p + sb, s_own, G) && up(s_nb_.p + sb, s_nb, G) &&
+              up(s_meta_.p + sb, s_meta, G) && up(s_len_.p + sb, s_len, G) && up(w_nx_.p + wb, w_nx, G) &&
+              up(w_ny_.p + wb, w_ny, G) && up(w_len_.p + wb, w_len, G) && up(w_dist_.p + wb, w_dist, G) &&
+              up(w_donor_.p + wb, w_donor, G) && up(w_xm_.p + wb, w_xm, G) && up(w_ym_.p + wb, w_ym, G) &&
+              up(g_mem_.p + gb, g_mem, G) && up(g_cell_.p + gmb, g_cell, G) && up(g_cnt_.p + gmb, g_cnt, G) &&
+              up(g_vol_.p + gb, g_vol, G) && up(q_cell_.p + qb, q_cell, G) && up(q_grp_.p + qb, q_grp, G) &&
+              up(q_list_.p + qlb, q_list, G) && up(q_cnt_.p + qb, q_cnt, G);
+    if (ok && model_ >= MODEL_LAMINAR)
+      ok = up(s_geo_.p + 6 * (long long)sb, s_geo, G) && up(t_own_.p + tb, t_own, G) && up(t_src_.p + tb, t_src, G) &&
+           up(t_x_.p + tb, t_x, G) && up(t_y_.p + tb, t_y, G);
+    if (ok && model_ == MODEL_SA) ok = up(c_wd_.p + cb, c_wd, G);
+    for (int v = 0; ok && v < nv_; ++v) {
+      ok = cuda_ok(cudaMemcpyAsync(U0_.p + v * ncap + cb, u.data() + v * (n + 1), sizeof(R) * (n + 1),
+                                   cudaMemcpyHostToDevice, stream_), error, "state upload");
+      stats_.state_h2d_bytes += sizeof(R) * (n + 1);
+    }
+    ok = ok && cuda_ok(cudaMemcpyAsync(cfg_.p + slot, &cf, sizeof(cf), cudaMemcpyHostToDevice, stream_), error, "cfg upload");
+    h_ctl_[slot] = ctl;
+    ok = ok && cuda_ok(cudaMemcpyAsync(ctl_.p + slot, &h_ctl_[slot], sizeof(CaseCtl), cudaMemcpyHostToDevice, stream_),
+                       error, "control upload");
+    stats_.control_h2d_bytes += sizeof(CaseCtl);
+    ok = ok && cuda_ok(cudaStreamSynchronize(stream_), error, "admit sync");
+    if (!ok) {
+      release_ranges(hc);
+      return 1;
+    }
+    hc.live = true;
+    cases_[slot] = std::move(hc);
+    live_++;
+    refresh_meta(slot);
+    tiles_dirty_ = true;
+    *slot_out = slot;
+    return 0;
+  }
+
+  int release(int slot) override {
+    if (slot < 0 || slot >= config_.max_cases || !cases_[slot].live) return 1;
+    // mark the control record dead on the device and in the mirror
+    h_ctl_[slot].live = 0;
+    h_ctl_[slot].active = 0;
+    cudaMemcpyAsync(ctl_.p + slot, &h_ctl_[slot], sizeof(CaseCtl), cudaMemcpyHostToDevice, stream_);
+    // the freed cell range no longer belongs to any case
+    HostCase<R>& hc = cases_[slot];
+    cudaMemsetAsync(c_case_.p + hc.cells.b, 0xff, sizeof(int) * hc.cells.n, stream_);
+    cudaStreamSynchronize(stream_);
+    release_ranges(hc);
+    hc = HostCase<R>();
+    live_--;
+    refresh_meta(slot);
+    tiles_dirty_ = true;
+    return 0;
+  }
+
+  int set_target(int slot, double target, long long maxsteps, std::string* error) override {
+    if (slot < 0 || slot >= config_.max_cases || !cases_[slot].live) return fail1(error, "no such case");
+    CaseCtl& c = h_ctl_[slot];
+    c.target = target;
+    c.maxsteps = maxsteps;
+    c.finished = c.time >= target;
+    stats_.control_h2d_bytes += sizeof(CaseCtl);
+    if (!cuda_ok(cudaMemcpyAsync(ctl_.p + slot, &c, sizeof(CaseCtl), cudaMemcpyHostToDevice, stream_), error, "target"))
+      return 1;
+    refresh_meta(slot);
+    return cuda_ok(cudaStreamSynchronize(stream_), error, "target sync") ? 0 : 1;
+  }
+
+  int advance(int trials, std::string* error) override {
+    if (trials < 1 || trials > 1024) return fail1(error, "trials must be 1..1024");
+    if (live_ == 0) return 0;
+    if (!sync_tiles(error)) return 1;
+    if (use_graph_ && (graph_dirty_ || graph_trials_ != trials)) {
+      if (!capture(trials, error)) {
+        use_graph_ = false;  // capture not available: launch directly
+        cudaGetLastError();
+      }
+    }
+    bool ok;
+    if (use_graph_ && graph_exec_) {
+      ok = cuda_ok(cudaGraphLaunch(graph_exec_, stream_), error, "graph launch");
+    } else {
+      ok = enqueue(trials, MODE_TRIALS, error);
+    }
+    ok = ok && cuda_ok(cudaStreamSynchronize(stream_), error, "advance");
+    launches_ += 1;
+    stats_.status_polls += 1;
+    stats_.control_d2h_bytes += sizeof(CaseCtl) * config_.max_cases;
+    float ms = 0;
+    if (ok && cudaEventElapsedTime(&ms, ev0_, ev1_) == cudaSuccess) {
+      last_seconds_ = ms * 1e-3;
+      if (event_timing_) {
+        stats_.advance_event_seconds += last_seconds_;
+        stats_.event_batches += 1;
+      }
+    }
+    if (!ok) return 1;
+    if (h_bar_->timeout) {
+      // a grid barrier gave up: mark every live case and report
+      for (int i = 0; i < config_.max_cases; ++i)
+        if (cases_[i].live && !h_ctl_[i].fatal) h_ctl_[i].fatal = STATUS_BARRIER_TIMEOUT;
+      cudaMemcpyAsync(ctl_.p, h_ctl_, sizeof(CaseCtl) * config_.max_cases, cudaMemcpyHostToDevice, stream_);
+      cudaStreamSynchronize(stream_);
+      for (int i = 0; i < config_.max_cases; ++i) refresh_meta(i);
+      return fail1(error, "grid barrier timed out; cases marked with status 9");
+    }
+    for (int i = 0; i < config_.max_cases; ++i) refresh_meta(i);
+    return 0;
+  }
+
+  int residual(std::string* error) override {
+    if (live_ == 0) return 0;
+    if (!sync_tiles(error)) return 1;
+    if (!enqueue(1, MODE_RESIDUAL, error)) return 1;
+    launches_ += 1;
+    return cuda_ok(cudaStreamSynchronize(stream_), error, "residual") ? 0 : 1;
+  }
+
+  int download_residual(int slot, double* out, uint64_t count, std::string* error) override {
+    return copy_out(R0_.p, slot, out, count, error);
+  }
+
+  int download(int slot, double* u, uint64_t count, std::string* error) override {
+    if (slot < 0 || slot >= config_.max_cases || !cases_[slot].live) return fail1(error, "no such case");
+    const int ok = copy_out(h_ctl_[slot].cur ? U1_.p : U0_.p, slot, u, count, error);
+    if (ok == 0) {
+      stats_.state_d2h_bytes += sizeof(R) * count;
+      stats_.full_downloads += 1;
+    }
+    return ok;
+  }
+
+  int diagnostics(const std::vector<int>& slots, const std::vector<double>& rm, std::vector<double>* out,
+                  std::string* error) override;
+
+  const CaseMeta& meta(int slot) const override { return meta_[slot]; }
+  int live_cases() const override { return live_; }
+  int max_cases() const override { return config_.max_cases; }
+  uint64_t free_cells() const override { return (uint64_t)a_cells_.free_total(); }
+  int nv() const override { return nv_; }
+  int n_cells(int slot) const override { return cases_[slot].n; }
+  double last_advance_seconds() const override { return last_seconds_; }
+  uint64_t kernel_launches() const override { return launches_; }
+  amr_gpu_stats_t stats() const override {
+    amr_gpu_stats_t s = stats_;
+    s.graph_nodes_per_trial = graph_nodes_;
+    return s;
+  }
+  void set_event_timing(bool on) override { event_timing_ = on; }
+  void set_graph(bool on) override {
+    use_graph_ = on;
+    graph_dirty_ = true;
+  }
+  std::string launch_config() const override {
+    return "block=" + std::to_string(block_) + " grid=" + std::to_string(grid_) + (use_graph_ ? " graph" : " direct");
+  }
+  int autotune(int trials, std::string* error) override;
+
+ private:
+  static bool fail(std::string* error, const std::string& text) {
+    if (error) *error = text;
+    return false;
+  }
+  static int fail1(std::string* error, const std::string& text) {
+    if (error) *error = text;
+    return 1;
+  }
+  int fail_release(HostCase<R>& hc, std::string* error, const std::string& text) {
+    release_ranges(hc);
+    return fail1(error, text);
+  }
+
+  template <class T> bool up(T* dst, const std::vector<T>& src, uint64_t* counter) {
+    if (src.empty()) return true;
+    *counter += sizeof(T) * src.size();
+    return cudaMemcpyAsync(dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, stream_) == cudaSuccess;
+  }
+
+  int copy_out(const R* buf, int slot, double* out, uint64_t count, std::string* error) {
+    if (slot < 0 || slot >= config_.max_cases || !cases_[slot].live) return fail1(error, "no such case");
+    const HostCase<R>& hc = cases_[slot];
+    const long long n = hc.n;
+    if (count != (uint64_t)(nv_ * n)) return fail1(error, "state size mismatch");
+    std::vector<R> tmp(nv_ * n);
+    for (int v = 0; v < nv_; ++v)
+      if (!cuda_ok(cudaMemcpyAsync(tmp.data() + v * n, buf + v * cap_cells_ + hc.cells.b, sizeof(R) * n,
+                                   cudaMemcpyDeviceToHost, stream_), error, "download"))
+        return 1;
+    if (!cuda_ok(cudaStreamSynchronize(stream_), error, "download sync")) return 1;
+    for (long long i = 0; i < nv_ * n; ++i) out[i] = (double)tmp[i];
+    return 0;
+  }
+
+  bool validate(const amr_mesh_view_t& m, const amr_params_t& p, uint64_t u0_count, std::string* why) const {
+    const auto finite = [](double x) { return std::isfinite(x); };
+    if (m.n_cells == 0 || m.n_faces == 0 || !m.cells || !m.faces || !m.face_offsets || !m.cell_faces)
+      return fail(why, "empty mesh");
+    if (m.n_cells + 1 > (uint64_t)0x3fffffff || m.face_offsets[m.n_cells] > (uint64_t)0x3fffffff)
+      return fail(why, "mesh too large for 32-bit indices");
+    const int sa = m.transport.sa_model ? 1 : 0;
+    const int model = m.transport.model == AMR_B200_MODEL_EULER ? MODEL_EULER : (sa ? MODEL_SA : MODEL_LAMINAR);
+    if (model != model_) return fail(why, "flow model differs from the batch's");
+    const int flux = p.flux == AMR_B200_FLUX_AUSMPUP ? FLUX_AUSM : FLUX_HLLC;
+    if (flux != flux_ && model_ >= 0) return fail(why, "numerical flux differs from the batch's");
+    if (u0_count != (uint64_t)(nv_ * m.n_cells)) return fail(why, "initial state size mismatch");
+    if (p.limiter != AMR_B200_LIMITER_FIRST_ORDER || p.time_integrator != AMR_B200_TIME_SSP_RK3 || !finite(p.gamma) ||
+        !(p.gamma > 1) || !(p.cfl > 0) || p.cfl > .5 || !finite(p.dt_fixed) || p.dt_fixed < 0 || !finite(p.ausm_mco) ||
+        p.ausm_mco <= 0 || (p.flux != AMR_B200_FLUX_HLLC && p.flux != AMR_B200_FLUX_AUSMPUP))
+      return fail(why, "invalid AMR GPU configuration");
+    // transport (reference src/static_amr2d_viscous.h:43-51)
+    const amr_transport_t& t = m.transport;
+    if (t.model == AMR_B200_MODEL_EULER) {
+      if (t.sa_model) return fail(why, "invalid transport");
+      for (int side = 0; side < 4; ++side)
+        if (m.boundaries[side].kind == AMR_B200_BC_NOSLIP) return fail(why, "no-slip wall requires laminar model");
+    } else {
+      const bool sa_ok = !t.sa_model || (t.sa_model == 1 && finite(t.sa_nu_inf) && t.sa_nu_inf >= 0 && finite(t.sa_cfl) &&
+                                         t.sa_cfl > 0 && t.sa_cfl <= .1);
+      if (!sa_ok || t.model != AMR_B200_MODEL_LAMINAR || (t.law != AMR_B200_MU_CONSTANT && t.law != AMR_B200_MU_SUTHERLAND) ||
+          !finite(t.mu_ref) || !(t.mu_ref > 0) || !finite(t.gas_constant) || !(t.gas_constant > 0) ||
+          !finite(t.temperature_ref) || !(t.temperature_ref > 0) || !finite(t.sutherland) || t.sutherland < 0 ||
+          !finite(t.viscous_cfl) || !(t.viscous_cfl > 0) || t.viscous_cfl > .2 ||
+          (t.stabilization != AMR_B200_VISCOUS_VOLUME && t.stabilization != AMR_B200_VISCOUS_SRD) ||
+          !finite(t.wall_probe_min_h) || t.wall_probe_min_h < 0 || t.wall_probe_min_h > 2)
+        return fail(why, "invalid laminar transport parameters");
+      if (!m.visc_offsets || !m.visc_terms || (m.n_walls && !m.wall_samples) || !m.face_samples || !m.face_geometry)
+        return fail(why, "viscous tables missing");
+      if (t.sa_model && !m.wall_distance) return fail(why, "SA wall distance missing");
+      if (t.stabilization == AMR_B200_VISCOUS_SRD && m.small_cells)
+        return fail(why, "SRD-rate viscous stabilization is not supported by this engine");
+    }
+    if (m.small_cells && (!m.group_offsets || !m.group_members || !m.member_offsets || !m.member_groups || !m.group_volume))
+      return fail(why, "SRD tables missing");
+    // boundaries (reference src/static_amr2d_boundary.h:32-47)
+    for (int side = 0; side < 4; ++side) {
+      const amr_boundary_t& b = m.boundaries[side];
+      if (b.kind < AMR_B200_BC_INHERIT) return fail(why, "invalid AMR GPU boundary configuration");
+      const int kind = b.kind < 0 ? p.bc[side] : b.kind;
+      if (kind == AMR_B200_BC_TRANSMISSIVE || kind == AMR_B200_BC_REFLECT) continue;
+      if (kind == AMR_B200_BC_NOSLIP) {
+        if (!finite(b.wall_velocity[0]) || !finite(b.wall_velocity[1]) || b.wall_velocity[side / 2] != 0)
+          return fail(why, "invalid AMR GPU boundary configuration");
+        continue;
+      }
+      const double* w = b.reference;
+      const bool prim = finite(w[0]) && w[0] > 0 && finite(w[1]) && finite(w[2]) && finite(w[3]) && w[3] > 0;
+      if (kind < AMR_B200_BC_FARFIELD || kind > AMR_B200_BC_PRESSURE_OUTLET || !prim)
+        return fail(why, "invalid AMR GPU boundary configuration");
+      if (kind == AMR_B200_BC_PRESSURE_OUTLET && !(finite(b.outlet_pressure) && b.outlet_pressure > 0))
+        return fail(why, "invalid AMR GPU boundary configuration");
+      if (kind == AMR_B200_BC_TOTAL_INLET) {
+        const double d2 = b.direction[0] * b.direction[0] + b.direction[1] * b.direction[1];
+        const double dn = (side % 2 ? 1.0 : -1.0) * b.direction[side / 2];
+        if (!(finite(d2) && std::fabs(d2 - 1) < 1e-12 && dn < 0 && finite(b.total_pressure) && b.total_pressure > 0 &&
+              finite(b.total_temperature) && b.total_temperature > 0 && finite(b.gas_constant) && b.gas_constant > 0))
+          return fail(why, "invalid AMR GPU boundary configuration");
+      }
+    }
+    return true;
+  }
+
+  bool make_tiles(HostCase<R>& hc, std::string* why) {
+    const long long n = hc.n;
+    const int cb = (int)hc.cells.b;
+    const int B = block_;
+    hc.tiles.clear();
+    long long k = 0;
+    bool first = true;
+    while (k < n) {
+      const long long start = k;
+      long long slots = 0, terms = 0;
+      while (k < n && k - start < B) {
+        const long long ds = hc.nslot[k], dt = hc.nterm[k];
+        if (slots + ds > B || terms + dt > B) break;
+        slots += ds;
+        terms += dt;
+        ++k;
+      }
+      if (k == start) return fail(why, "a cell has more faces or gradient terms than a thread block");
+      hc.tiles.push_back(Tile{hc.slot, cb + (int)start, cb + (int)k, first ? 1 : 0});
+      first = false;
+    }
+    return true;
+  }
+
+  bool retile(HostCase<R>& hc) {
+    std::string why;
+    return make_tiles(hc, &why);
+  }
+
+  long long n_tiles_total() const {
+    long long s = 0;
+    for (auto& c : cases_)
+      if (c.live) s += (long long)c.tiles.size();
+    return s;
+  }
+
+  void release_ranges(HostCase<R>& hc) {
+    a_cells_.release(hc.cells.b, hc.cells.b >= 0 ? hc.cells.n : 0);
+    a_slots_.release(hc.slots.b, hc.slots.b >= 0 ? hc.slots.n : 0);
+    a_walls_.release(hc.walls.b, hc.walls.b >= 0 ? hc.walls.n : 0);
+    a_terms_.release(hc.terms.b, hc.terms.b >= 0 ? hc.terms.n : 0);
+    a_groups_.release(hc.groups.b, hc.groups.b >= 0 ? hc.groups.n : 0);
+    a_gmem_.release(hc.gmembers.b, hc.gmembers.b >= 0 ? hc.gmembers.n : 0);
+    a_q_.release(hc.qcells.b, hc.qcells.b >= 0 ? hc.qcells.n : 0);
+    a_qlist_.release(hc.qlist.b, hc.qlist.b >= 0 ? hc.qlist.n : 0);
+    hc.cells = hc.slots = hc.walls = hc.terms = hc.groups = hc.gmembers = hc.qcells = hc.qlist = Range{0, 0};
+  }
+
+  void refresh_meta(int slot) {
+    const CaseCtl& c = h_ctl_[slot];
+    CaseMeta& m = meta_[slot];
+    m.time = c.time;
+    m.target = c.target;
+    m.dt = c.dt;
+    m.dt_trial = c.dt_trial;
+    m.steps = c.steps;
+    m.rejected = c.rejected;
+    m.maxsteps = c.maxsteps;
+    m.fatal = c.fatal;
+    m.finished = c.finished;
+    m.active = c.active;
+    m.live = c.live;
+    m.cur = c.cur;
+  }
+
+  bool sync_tiles(std::string* error) {
+    if (!tiles_dirty_) return true;
+    std::vector<Tile> all;
+    std::vector<int> ranges(2 * config_.max_cases, 0);
+    for (int i = 0; i < config_.max_cases; ++i) {
+      ranges[2 * i] = (int)all.size();
+      if (cases_[i].live) all.insert(all.end(), cases_[i].tiles.begin(), cases_[i].tiles.end());
+      ranges[2 * i + 1] = (int)all.size();
+    }
+    n_tiles_ = (int)all.size();
+    if (!all.empty() && !cuda_ok(cudaMemcpyAsync(tiles_.p, all.data(), sizeof(Tile) * all.size(), cudaMemcpyHostToDevice,
+                                                 stream_), error, "tiles"))
+      return false;
+    if (!cuda_ok(cudaMemcpyAsync(case_tiles_.p, ranges.data(), sizeof(int) * ranges.size(), cudaMemcpyHostToDevice, stream_),
+                 error, "tile ranges"))
+      return false;
+    case_tile_ranges_ = ranges;
+    tiles_dirty_ = false;
+    graph_dirty_ = true;
+    return cuda_ok(cudaStreamSynchronize(stream_), error, "tiles sync");
+  }
+
+  Dev<R> dev() const {
+    Dev<R> d;
+    std::memset(&d, 0, sizeof(d));
+    d.ctl = ctl_.p;
+    d.cfg = cfg_.p;
+    d.tiles = tiles_.p;
+    d.n_tiles = n_tiles_;
+    d.n_cases = config_.max_cases;
+    d.c_case = c_case_.p;
+    d.c_vol = c_vol_.p;
+    d.c_area = c_area_.p;
+    d.c_gvol = c_gvol_.p;
+    d.c_flags = c_flags_.p;
+    d.c_slot = c_slot_.p;
+    d.c_wall = c_wall_.p;
+    d.c_term = c_term_.p;
+    d.c_wd = c_wd_.p;
+    d.s_own = s_own_.p;
+    d.s_nb = s_nb_.p;
+    d.s_meta = s_meta_.p;
+    d.s_len = s_len_.p;
+    d.s_geo = s_geo_.p;
+    d.w_nx = w_nx_.p;
+    d.w_ny = w_ny_.p;
+    d.w_len = w_len_.p;
+    d.w_dist = w_dist_.p;
+    d.w_donor = w_donor_.p;
+    d.t_own = t_own_.p;
+    d.t_src = t_src_.p;
+    d.t_x = t_x_.p;
+    d.t_y = t_y_.p;
+    d.g_mem = g_mem_.p;
+    d.g_cell = g_cell_.p;
+    d.g_cnt = g_cnt_.p;
+    d.g_vol = g_vol_.p;
+    d.q_cell = q_cell_.p;
+    d.q_grp = q_grp_.p;
+    d.q_list = q_list_.p;
+    d.q_cnt = q_cnt_.p;
+    d.qhat = qhat_.p;
+    d.U0 = U0_.p;
+    d.U1 = U1_.p;
+    d.U2 = U2_.p;
+    d.R0 = R0_.p;
+    d.grad = grad_.p;
+    d.mu = mu_.p;
+    d.eddy = eddy_.p;
+    d.sgrad = sgrad_.p;
+    d.sdiff = sdiff_.p;
+    d.ssrc = ssrc_.p;
+    d.srate = srate_.p;
+    d.ncap = cap_cells_;
+    d.gcap = cap_groups_ + config_.max_cases;
+    d.bar = bar_.p;
+    d.barrier_cycles = (unsigned long long)clock_khz_ * 1000ull * 2ull;  // about two seconds
+    return d;
+  }
+
+  bool any_srd() const {
+    for (auto& c : cases_)
+      if (c.live && c.cfg.has_srd) return true;
+    return false;
+  }
+
+  bool configure_grid(std::string* error) {
+    int per_sm = 0;
+    if (!cuda_ok(EngineOps<R>::occupancy(model_, flux_, true, block_, &per_sm), error, "occupancy")) return false;
+    int per_sm2 = 0;
+    if (!cuda_ok(EngineOps<R>::occupancy(model_, flux_, false, block_, &per_sm2), error, "occupancy")) return false;
+    per_sm = std::min(per_sm, per_sm2);
+    if (per_sm < 1) return fail(error, "kernel does not fit on an SM");
+    max_grid_ = per_sm * sms_;
+    grid_ = grid_request_ > 0 ? std::min(grid_request_, max_grid_) : max_grid_;
+    return true;
+  }
+
+  bool enqueue(int trials, int mode, std::string* error) {
+    const int grid = mode == MODE_RESIDUAL ? std::min(grid_, std::max(1, n_tiles_)) : grid_;
+    bool ok = cuda_ok(cudaMemsetAsync(bar_.p, 0, sizeof(GridBarrier), stream_), error, "barrier reset") &&
+              cuda_ok(cudaEventRecord(ev0_, stream_), error, "event") &&
+              cuda_ok(EngineOps<R>::launch(dev(), model_, flux_, any_srd(), trials, mode, grid, block_, stream_, true),
+                      error, "trial kernel launch") &&
+              cuda_ok(cudaEventRecord(ev1_, stream_), error, "event");
+    if (ok && mode == MODE_TRIALS)
+      ok = cuda_ok(cudaMemcpyAsync(h_ctl_, ctl_.p, sizeof(CaseCtl) * config_.max_cases, cudaMemcpyDeviceToHost, stream_),
+                   error, "control read-back") &&
+           cuda_ok(cudaMemcpyAsync(h_bar_, bar_.p, sizeof(GridBarrier), cudaMemcpyDeviceToHost, stream_), error,
+                   "barrier read-back");
+    return ok;
+  }
+
+  bool capture(int trials, std::string* error) {
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    graph_exec_ = nullptr;
+    graph_ = nullptr;
+    if (!cuda_ok(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), error, "capture begin")) return false;
+    std::string err;
+    const bool ok = enqueue(trials, MODE_TRIALS, &err);
+    cudaGraph_t g = nullptr;
+    const cudaError_t end = cudaStreamEndCapture(stream_, &g);
+    if (!ok || end != cudaSuccess || !g) {
+      if (g) cudaGraphDestroy(g);
+      if (error) *error = "graph capture failed: " + err;
+      return false;
+    }
+    graph_ = g;
+    if (cudaGraphInstantiate(&graph_exec_, graph_, nullptr, nullptr, 0) != cudaSuccess) {
+      cudaGraphDestroy(graph_);
+      graph_ = nullptr;
+      graph_exec_ = nullptr;
+      return false;
+    }
+    size_t nodes = 0;
+    cudaGraphGetNodes(graph_, nullptr, &nodes);
+    graph_nodes_ = nodes;
+    graph_trials_ = trials;
+    graph_dirty_ = false;
+    return true;
+  }
+
+  void destroy() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    graph_exec_ = nullptr;
+    graph_ = nullptr;
+    DevBufFreeAll();
+    if (h_ctl_) cudaFreeHost(h_ctl_);
+    if (h_bar_) cudaFreeHost(h_bar_);
+    h_ctl_ = nullptr;
+    h_bar_ = nullptr;
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
+    ev0_ = ev1_ = nullptr;
+    if (stream_) cudaStreamDestroy(stream_);
+    stream_ = nullptr;
+  }
+
+  void DevBufFreeAll() {
+    ctl_.free(); cfg_.free(); tiles_.free(); bar_.free();
+    c_case_.free(); c_vol_.free(); c_area_.free(); c_gvol_.free(); c_flags_.free(); c_slot_.free(); c_wall_.free();
+    c_term_.free(); c_cx_.free(); c_cy_.free(); c_wd_.free();
+    s_own_.free(); s_nb_.free(); s_meta_.free(); s_len_.free(); s_geo_.free();
+    w_nx_.free(); w_ny_.free(); w_len_.free(); w_dist_.free(); w_donor_.free(); w_xm_.free(); w_ym_.free();
+    t_own_.free(); t_src_.free(); t_x_.free(); t_y_.free();
+    g_mem_.free(); g_cell_.free(); g_cnt_.free(); g_vol_.free(); q_cell_.free(); q_grp_.free(); q_list_.free(); q_cnt_.free();
+    qhat_.free();
+    U0_.free(); U1_.free(); U2_.free(); R0_.free(); grad_.free(); mu_.free(); eddy_.free(); sgrad_.free(); sdiff_.free();
+    ssrc_.free(); srate_.free(); diag_part_.free(); diag_out_.free(); diag_cfg_.free(); case_tiles_.free();
+  }
+
+  amr_batch_config_t config_{};
+  int model_ = 0, flux_ = 0, nv_ = 4, sms_ = 148, clock_khz_ = 1965000;
+  int block_ = 256, grid_ = 0, max_grid_ = 0, grid_request_ = 0;
+  long long cap_cells_ = 0, cap_slots_ = 0, cap_walls_ = 0, cap_terms_ = 0, cap_groups_ = 0, cap_gmem_ = 0, cap_q_ = 0,
+            cap_qlist_ = 0, cap_tiles_ = 0;
+  RangeAlloc a_cells_, a_slots_, a_walls_, a_terms_, a_groups_, a_gmem_, a_q_, a_qlist_;
+  std::vector<HostCase<R>> cases_;
+  std::vector<CaseMeta> meta_;
+  int live_ = 0, n_tiles_ = 0;
+  bool tiles_dirty_ = true, graph_dirty_ = true, use_graph_ = true, event_timing_ = true;
+  int graph_trials_ = 0;
+  uint64_t graph_nodes_ = 0, launches_ = 0;
+  double last_seconds_ = 0;
+  std::vector<int> case_tile_ranges_;
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t graph_exec_ = nullptr;
+  CaseCtl* h_ctl_ = nullptr;
+  GridBarrier* h_bar_ = nullptr;
+  amr_gpu_stats_t stats_{};
+  DevBuf<CaseCtl> ctl_;
+  DevBuf<CaseCfg<R>> cfg_;
+  DevBuf<Tile> tiles_;
+  DevBuf<GridBarrier> bar_;
+  DevBuf<int> c_case_, c_slot_, c_wall_, c_term_;
+  DevBuf<double> c_vol_, c_area_, c_gvol_, c_cx_, c_cy_;
+  DevBuf<unsigned char> c_flags_;
+  DevBuf<R> c_wd_;
+  DevBuf<int> s_own_, s_nb_, s_meta_;
+  DevBuf<R> s_len_, s_geo_;
+  DevBuf<R> w_nx_, w_ny_, w_len_, w_dist_;
+  DevBuf<double> w_xm_, w_ym_;
+  DevBuf<int> w_donor_;
+  DevBuf<int> t_own_, t_src_;
+  DevBuf<R> t_x_, t_y_;
+  DevBuf<int> g_mem_, g_cell_, q_cell_, q_grp_, q_list_;
+  DevBuf<double> g_cnt_, g_vol_, q_cnt_, qhat_;
+  DevBuf<R> U0_, U1_, U2_, R0_, grad_, mu_, eddy_, sgrad_, sdiff_, ssrc_, srate_;
+  DevBuf<double> diag_part_, diag_out_, diag_cfg_;
+  DevBuf<int> case_tiles_;
+};
+
+}  // namespace amrb

@@ -1,0 +1,56 @@
+// amr_host.h -- host-side engine interface shared by the C ABI (amr_capi.cu) and the two
+// precision instantiations (amr_engine_f64.cu, amr_engine_f32.cu).
+#pragma once
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/amr_b200.h"
+
+namespace amrb {
+
+// Host view of one case's device control record (mirrors CaseCtl).
+struct CaseMeta {
+  double time, target, dt, dt_trial;
+  long long steps, rejected, maxsteps;
+  int fatal, finished, active, live, cur;
+};
+
+class BatchBase {
+ public:
+  virtual ~BatchBase() = default;
+  // Admits a case; returns 0, 1 (invalid input, message in *error) or 3 (no room).
+  virtual int admit(const amr_mesh_view_t* mesh, const amr_params_t* params, const double* u0, uint64_t u0_count,
+                    double time0, long long steps0, long long rejected0, double target, long long maxsteps,
+                    int* slot, std::string* error) = 0;
+  virtual int release(int slot) = 0;
+  // Runs `trials` trials of every live case and refreshes the host copies of the controls.
+  virtual int advance(int trials, std::string* error) = 0;
+  // Sets a case's target time and step cap (the session's advance arguments).
+  virtual int set_target(int slot, double target, long long maxsteps, std::string* error) = 0;
+  // Residual of every live case's accepted state into the engine's residual buffer.
+  virtual int residual(std::string* error) = 0;
+  virtual int download_residual(int slot, double* out, uint64_t count, std::string* error) = 0;
+  virtual int download(int slot, double* u, uint64_t count, std::string* error) = 0;
+  // Region residual norms (5), region volume, Fx, Fy, Mz per requested case (9 doubles each).
+  virtual int diagnostics(const std::vector<int>& slots, const std::vector<double>& region_moment,
+                          std::vector<double>* out, std::string* error) = 0;
+  virtual const CaseMeta& meta(int slot) const = 0;
+  virtual int live_cases() const = 0;
+  virtual int max_cases() const = 0;
+  virtual uint64_t free_cells() const = 0;
+  virtual int nv() const = 0;
+  virtual int n_cells(int slot) const = 0;
+  virtual double last_advance_seconds() const = 0;
+  virtual uint64_t kernel_launches() const = 0;
+  virtual amr_gpu_stats_t stats() const = 0;
+  virtual int autotune(int trials, std::string* error) = 0;
+  virtual void set_event_timing(bool on) = 0;
+  virtual void set_graph(bool on) = 0;
+  virtual std::string launch_config() const = 0;
+};
+
+std::unique_ptr<BatchBase> make_batch_f64(const amr_batch_config_t& config, std::string* error);
+std::unique_ptr<BatchBase> make_batch_f32(const amr_batch_config_t& config, std::string* error);
+
+}  // namespace amrb
