@@ -163,6 +163,7 @@ typedef struct amr_gpu_options_t {
   int32_t device;        /* CUDA device ordinal */
   int32_t block_threads; /* 0 = autotuned */
   int32_t grid_blocks;   /* 0 = autotuned */
+  int32_t launch_mode;   /* AMR_B200_LAUNCH_*; AUTO with block_threads = grid_blocks = 0 autotunes */
 } amr_gpu_options_t;
 
 /* Same fields, order and layout as the reference's AmrGpuStats (src/static_amr2d_gpu.h:9-16). */
@@ -231,6 +232,9 @@ int amr_gpu_diagnostics(amr_gpu_session* session, const double region[4], double
  * Batched form.
  * ---------------------------------------------------------------------------------- */
 enum { AMR_B200_PRECISION_FP64 = 64, AMR_B200_PRECISION_FP32 = 32 };
+/* Launch modes: one persistent cooperative kernel per poll with grid barriers between phases,
+ * or one kernel per phase (one block per tile) replayed from a CUDA graph. */
+enum { AMR_B200_LAUNCH_AUTO = 0, AMR_B200_LAUNCH_PERSISTENT = 1, AMR_B200_LAUNCH_PHASES = 2 };
 
 typedef struct amr_batch_config_t {
   int32_t precision;      /* AMR_B200_PRECISION_FP32 or _FP64 */
@@ -241,8 +245,9 @@ typedef struct amr_batch_config_t {
   int32_t max_cases;
   uint64_t max_cells, max_faces, max_walls, max_terms, max_srd; /* arena capacities; 0 = sized from hbm_bytes */
   uint64_t hbm_bytes;     /* arena budget used when capacities are 0 */
-  int32_t block_threads;  /* 0 = autotuned */
-  int32_t grid_blocks;    /* 0 = autotuned */
+  int32_t block_threads;  /* 0 = 256 until amr_batch_autotune */
+  int32_t grid_blocks;    /* 0 = one wave of co-resident blocks */
+  int32_t launch_mode;    /* AMR_B200_LAUNCH_*; AUTO starts persistent until amr_batch_autotune */
 } amr_batch_config_t;
 
 /* Per-case run control and the steady retirement rule (reference driver,
@@ -286,6 +291,9 @@ int amr_batch_live_cases(const amr_batch* batch);
 uint64_t amr_batch_free_cells(const amr_batch* batch);
 /* Device time of the last amr_batch_advance in seconds (CUDA events on the launch stream). */
 double amr_batch_last_advance_seconds(const amr_batch* batch);
+/* Times every launch mode and block size on the live cases (state and controls are restored
+ * afterwards) and keeps the fastest. */
+int amr_batch_autotune(amr_batch* batch, int32_t trials, char* error, uint64_t error_size);
 /* Kernels launched by this batch so far. */
 uint64_t amr_batch_kernel_launches(const amr_batch* batch);
 void amr_batch_destroy(amr_batch* batch);

@@ -19,6 +19,7 @@ LIMITER_FIRST_ORDER = 3
 TIME_SSP_RK3 = 0
 STATUS_OK, STATUS_NONPHYSICAL_BASE, STATUS_MAXSTEPS, STATUS_DT_UNDERFLOW, STATUS_REJECTIONS, STATUS_BARRIER_TIMEOUT = 0, 2, 3, 4, 5, 9
 PRECISION_FP64, PRECISION_FP32 = 64, 32
+LAUNCH_AUTO, LAUNCH_PERSISTENT, LAUNCH_PHASES = 0, 1, 2
 
 CELL_DTYPE = np.dtype([('ix', '<i4'), ('iy', '<i4'), ('span', '<i4'), ('level', '<i4'),
                        ('x0', '<f8'), ('x1', '<f8'), ('y0', '<f8'), ('y1', '<f8'),
@@ -81,7 +82,8 @@ class MeshView(C.Structure):
 
 class GpuOptions(C.Structure):
     _fields_ = [('batch_trials', C.c_int32), ('graph', C.c_int32), ('fused', C.c_int32), ('event_timing', C.c_int32),
-                ('sa_fused', C.c_int32), ('device', C.c_int32), ('block_threads', C.c_int32), ('grid_blocks', C.c_int32)]
+                ('sa_fused', C.c_int32), ('device', C.c_int32), ('block_threads', C.c_int32), ('grid_blocks', C.c_int32),
+                ('launch_mode', C.c_int32)]
 
 
 class GpuStats(C.Structure):
@@ -102,7 +104,7 @@ class BatchConfig(C.Structure):
     _fields_ = [('precision', C.c_int32), ('device', C.c_int32), ('model', C.c_int32), ('sa_model', C.c_int32),
                 ('flux', C.c_int32), ('max_cases', C.c_int32), ('max_cells', C.c_uint64), ('max_faces', C.c_uint64),
                 ('max_walls', C.c_uint64), ('max_terms', C.c_uint64), ('max_srd', C.c_uint64), ('hbm_bytes', C.c_uint64),
-                ('block_threads', C.c_int32), ('grid_blocks', C.c_int32)]
+                ('block_threads', C.c_int32), ('grid_blocks', C.c_int32), ('launch_mode', C.c_int32)]
 
 
 class CaseControl(C.Structure):

@@ -34,12 +34,13 @@ def case_control(tend, maxsteps, steady=True, mach=1.65, aoa=1.5, **kw):
 class Batch:
     def __init__(self, precision=32, model=_abi.MODEL_LAMINAR, sa=True, flux=_abi.FLUX_HLLC, max_cases=256,
                  max_cells=0, max_faces=0, max_walls=0, max_terms=0, max_srd=0, hbm_bytes=0, block_threads=0,
-                 grid_blocks=0, device=0):
+                 grid_blocks=0, device=0, launch_mode=0):
         cfg = _abi.BatchConfig()
         cfg.precision, cfg.device, cfg.model, cfg.sa_model, cfg.flux = precision, device, model, int(sa), flux
         cfg.max_cases = max_cases
         cfg.max_cells, cfg.max_faces, cfg.max_walls, cfg.max_terms, cfg.max_srd = max_cells, max_faces, max_walls, max_terms, max_srd
         cfg.hbm_bytes, cfg.block_threads, cfg.grid_blocks = hbm_bytes, block_threads, grid_blocks
+        cfg.launch_mode = launch_mode
         out = C.c_void_p()
         err = errbuf()
         if lib().amr_batch_create(C.byref(cfg), C.byref(out), err, len(err)):

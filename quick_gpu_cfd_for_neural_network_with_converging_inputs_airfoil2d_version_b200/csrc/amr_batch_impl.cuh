@@ -201,6 +201,7 @@ template <class R> class Batch final : public BatchBase {
     block_ = c.block_threads > 0 ? c.block_threads : 256;
     if (block_ % 32 || block_ < 64 || block_ > MAX_BLOCK) return fail(error, "block_threads must be 64..256, a multiple of 32");
     grid_request_ = c.grid_blocks;
+    phases_ = c.launch_mode == AMR_B200_LAUNCH_PHASES;
     if (!configure_grid(error)) return false;
     return cuda_ok(cudaStreamSynchronize(stream_), error, "batch init");
   }
@@ -528,13 +529,16 @@ template <class R> class Batch final : public BatchBase {
       }
     }
     bool ok;
+    cudaGetLastError();  // clear any stale error of an earlier runtime call
     if (use_graph_ && graph_exec_) {
-      ok = cuda_ok(cudaGraphLaunch(graph_exec_, stream_), error, "graph launch");
+      ok = cuda_ok(cudaEventRecord(ev0_, stream_), error, "event") &&
+           cuda_ok(cudaGraphLaunch(graph_exec_, stream_), error, "graph launch") &&
+           cuda_ok(cudaEventRecord(ev1_, stream_), error, "event");
     } else {
       ok = enqueue(trials, MODE_TRIALS, error);
     }
     ok = ok && cuda_ok(cudaStreamSynchronize(stream_), error, "advance");
-    launches_ += 1;
+    launches_ += kernels_per_advance(trials);
     stats_.status_polls += 1;
     stats_.control_d2h_bytes += sizeof(CaseCtl) * config_.max_cases;
     float ms = 0;
@@ -544,6 +548,8 @@ template <class R> class Batch final : public BatchBase {
         stats_.advance_event_seconds += last_seconds_;
         stats_.event_batches += 1;
       }
+    } else {
+      cudaGetLastError();
     }
     if (!ok) return 1;
     if (h_bar_->timeout) {
@@ -562,8 +568,9 @@ template <class R> class Batch final : public BatchBase {
   int residual(std::string* error) override {
     if (live_ == 0) return 0;
     if (!sync_tiles(error)) return 1;
+    cudaGetLastError();
     if (!enqueue(1, MODE_RESIDUAL, error)) return 1;
-    launches_ += 1;
+    launches_ += phases_ ? (model_ >= MODEL_LAMINAR ? 2 : 1) : 1;
     return cuda_ok(cudaStreamSynchronize(stream_), error, "residual") ? 0 : 1;
   }
 
@@ -603,9 +610,11 @@ template <class R> class Batch final : public BatchBase {
     graph_dirty_ = true;
   }
   std::string launch_config() const override {
-    return "block=" + std::to_string(block_) + " grid=" + std::to_string(grid_) + (use_graph_ ? " graph" : " direct");
+    return std::string(phases_ ? "mode=phases" : "mode=persistent") + " block=" + std::to_string(block_) +
+           " grid=" + std::to_string(phases_ ? n_tiles_ : grid_) + (use_graph_ ? " graph" : " direct");
   }
   int autotune(int trials, std::string* error) override;
+  void restore(const std::vector<CaseCtl>& ctl_save, const DevBuf<R>& s0, const DevBuf<R>& s1, long long nbytes);
 
  private:
   static bool fail(std::string* error, const std::string& text) {
@@ -855,6 +864,12 @@ template <class R> class Batch final : public BatchBase {
     return d;
   }
 
+  uint64_t kernels_per_advance(int trials) const {
+    if (!phases_) return 1;
+    const uint64_t per_trial = 1 + 1 + 1 + 2 + (model_ >= MODEL_LAMINAR ? 3 : 0) + (any_srd() ? 3 : 0) + 1;
+    return 1 + per_trial * trials;
+  }
+
   bool any_srd() const {
     for (auto& c : cases_)
       if (c.live && c.cfg.has_srd) return true;
@@ -873,13 +888,22 @@ template <class R> class Batch final : public BatchBase {
     return true;
   }
 
-  bool enqueue(int trials, int mode, std::string* error) {
-    const int grid = mode == MODE_RESIDUAL ? std::min(grid_, std::max(1, n_tiles_)) : grid_;
-    bool ok = cuda_ok(cudaMemsetAsync(bar_.p, 0, sizeof(GridBarrier), stream_), error, "barrier reset") &&
-              cuda_ok(cudaEventRecord(ev0_, stream_), error, "event") &&
-              cuda_ok(EngineOps<R>::launch(dev(), model_, flux_, any_srd(), trials, mode, grid, block_, stream_, true),
-                      error, "trial kernel launch") &&
-              cuda_ok(cudaEventRecord(ev1_, stream_), error, "event");
+  // Launch sequence of one advance: barrier reset, the persistent kernel, and (trial mode)
+  // the control and barrier read-back.  Timing events are recorded around it only when the
+  // sequence is issued directly; a graph launch is timed by events outside the graph.
+  bool enqueue(int trials, int mode, std::string* error, bool events = true) {
+    bool ok = true;
+    if (events) ok = cuda_ok(cudaEventRecord(ev0_, stream_), error, "event");
+    if (phases_) {
+      ok = ok && cuda_ok(EngineOps<R>::launch_phases(dev(), model_, flux_, any_srd(), trials, mode, block_, stream_), error,
+                         "phase kernel launch");
+    } else {
+      const int grid = mode == MODE_RESIDUAL ? std::min(grid_, std::max(1, n_tiles_)) : grid_;
+      ok = ok && cuda_ok(cudaMemsetAsync(bar_.p, 0, sizeof(GridBarrier), stream_), error, "barrier reset") &&
+           cuda_ok(EngineOps<R>::launch(dev(), model_, flux_, any_srd(), trials, mode, grid, block_, stream_, true), error,
+                   "trial kernel launch");
+    }
+    if (events) ok = ok && cuda_ok(cudaEventRecord(ev1_, stream_), error, "event");
     if (ok && mode == MODE_TRIALS)
       ok = cuda_ok(cudaMemcpyAsync(h_ctl_, ctl_.p, sizeof(CaseCtl) * config_.max_cases, cudaMemcpyDeviceToHost, stream_),
                    error, "control read-back") &&
@@ -895,7 +919,7 @@ template <class R> class Batch final : public BatchBase {
     graph_ = nullptr;
     if (!cuda_ok(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), error, "capture begin")) return false;
     std::string err;
-    const bool ok = enqueue(trials, MODE_TRIALS, &err);
+    const bool ok = enqueue(trials, MODE_TRIALS, &err, false);
     cudaGraph_t g = nullptr;
     const cudaError_t end = cudaStreamEndCapture(stream_, &g);
     if (!ok || end != cudaSuccess || !g) {
@@ -952,6 +976,7 @@ template <class R> class Batch final : public BatchBase {
   amr_batch_config_t config_{};
   int model_ = 0, flux_ = 0, nv_ = 4, sms_ = 148, clock_khz_ = 1965000;
   int block_ = 256, grid_ = 0, max_grid_ = 0, grid_request_ = 0;
+  bool phases_ = false;  // launch mode: persistent cooperative kernel, or one kernel per phase
   long long cap_cells_ = 0, cap_slots_ = 0, cap_walls_ = 0, cap_terms_ = 0, cap_groups_ = 0, cap_gmem_ = 0, cap_q_ = 0,
             cap_qlist_ = 0, cap_tiles_ = 0;
   RangeAlloc a_cells_, a_slots_, a_walls_, a_terms_, a_groups_, a_gmem_, a_q_, a_qlist_;

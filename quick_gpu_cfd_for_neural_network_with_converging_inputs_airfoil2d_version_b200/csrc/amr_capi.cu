@@ -53,6 +53,7 @@ struct amr_gpu_session {
   amr_gpu_options_t options;
   uint64_t n = 0;
   int nv = 4;
+  double sa_nu_inf = 0;
   double setup_seconds = 0, advance_seconds = 0, download_seconds = 0;
 };
 
@@ -85,6 +86,7 @@ int amr_gpu_create(const amr_mesh_view_t* mesh, const amr_params_t* params, cons
   s->options = *options;
   s->n = mesh->n_cells;
   s->nv = mesh->transport.sa_model ? 5 : 4;
+  s->sa_nu_inf = mesh->transport.sa_nu_inf;
   amr_batch_config_t c;
   std::memset(&c, 0, sizeof(c));
   c.precision = AMR_B200_PRECISION_FP64;
@@ -95,6 +97,7 @@ int amr_gpu_create(const amr_mesh_view_t* mesh, const amr_params_t* params, cons
   c.max_cases = 1;
   c.block_threads = options->block_threads;
   c.grid_blocks = options->grid_blocks;
+  c.launch_mode = options->launch_mode;
   if (mesh->n_cells && mesh->face_offsets) size_for(*mesh, &c);
   std::string err;
   s->batch = make_batch(c, &err);
@@ -110,7 +113,7 @@ int amr_gpu_create(const amr_mesh_view_t* mesh, const amr_params_t* params, cons
   }
   s->batch->set_graph(options->graph != 0);
   s->batch->set_event_timing(options->event_timing != 0);
-  if (options->block_threads == 0 && options->grid_blocks == 0) {
+  if (options->block_threads == 0 && options->grid_blocks == 0 && options->launch_mode == AMR_B200_LAUNCH_AUTO) {
     if (s->batch->set_target(0, 1e300, LLONG_MAX, &err) || s->batch->autotune(4, &err) ||
         s->batch->set_target(0, time0, 0, &err)) {
       put(error, error_size, "autotune: " + err);
@@ -227,6 +230,7 @@ int amr_gpu_diagnostics(amr_gpu_session* s, const double region[4], double mx, d
   }
   const double volume = res[5];
   for (int v = 0; v < 5; ++v) out[v] = v < s->nv && volume > 0 ? res[v] / volume : 0.0;
+  if (s->nv == 5) out[4] /= s->sa_nu_inf;
   out[5] = res[6];
   out[6] = res[7];
   out[7] = res[8];

@@ -838,10 +838,88 @@ __global__ void __launch_bounds__(MAX_BLOCK) trials_kernel(Dev<R> d, int trials,
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// Phase kernels: the same phases as trials_kernel, one kernel per phase and one block per tile,
+// for batches large enough to fill the GPU many times over.  A trial is the launch sequence
+//   [grad 0] flux 0, first_update, [srd 1], [grad 1], flux 1, [srd 2], [grad 2], flux 2,
+//   [srd 3], commit
+// and a CUDA graph replays `trials` such sequences.
+// ------------------------------------------------------------------------------------------
+template <class R> __device__ __forceinline__ const R* stage_input(const Dev<R>& d, int stage, int cur) {
+  if (stage == STAGE_BASE || stage == STAGE_DIAG) return state_buf(d, cur);
+  return stage == STAGE_1 ? state_buf(d, cur ^ 1) : d.U2;
+}
+
+template <class R, int MODEL>
+__global__ void __launch_bounds__(MAX_BLOCK, 2) phase_grad_kernel(Dev<R> d, int stage) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* sm = reinterpret_cast<R*>(smem_raw);
+  const int rule = stage == STAGE_DIAG ? SKIP_LIVE : (stage == STAGE_BASE ? SKIP_ACTIVE : SKIP_STAGE);
+  for (int ti = blockIdx.x; ti < d.n_tiles; ti += gridDim.x) {
+    const TileView v = read_tile(d.tiles, d.ctl, ti, rule);
+    if (v.skip) continue;
+    phase_gradients<R, MODEL>(d, v.t, stage_input(d, stage, v.cur), sm);
+  }
+}
+
+template <class R, int MODEL, int FLUX>
+__global__ void __launch_bounds__(MAX_BLOCK, 2) phase_flux_kernel(Dev<R> d, int stage) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* sm = reinterpret_cast<R*>(smem_raw);
+  __shared__ bool s_bad;
+  __shared__ double s_dt;
+  const int rule = stage == STAGE_DIAG ? SKIP_LIVE : (stage == STAGE_BASE ? SKIP_ACTIVE : SKIP_STAGE);
+  for (int ti = blockIdx.x; ti < d.n_tiles; ti += gridDim.x) {
+    const TileView v = read_tile(d.tiles, d.ctl, ti, rule);
+    if (v.skip) continue;
+    if (threadIdx.x == 0) { s_bad = false; s_dt = __longlong_as_double(0x7FF0000000000000ll); }
+    __syncthreads();
+    R* ub = state_buf(d, v.cur);
+    R* un = state_buf(d, v.cur ^ 1);
+    phase_flux<R, MODEL, FLUX>(d, v.t, stage, stage_input(d, stage, v.cur), ub, un, sm, &s_bad, &s_dt);
+    if (threadIdx.x == 0 && stage != STAGE_DIAG) {
+      if (s_bad) atomicOr(&d.ctl[v.t.cs].bad, 1);
+      if (stage == STAGE_BASE) atomic_min_dt(&d.ctl[v.t.cs].dtmin, s_dt);
+    }
+  }
+}
+
+template <class R, int MODEL>
+__global__ void __launch_bounds__(MAX_BLOCK, 4) phase_first_kernel(Dev<R> d) {
+  for (int ti = blockIdx.x; ti < d.n_tiles; ti += gridDim.x) {
+    const TileView v = read_tile(d.tiles, d.ctl, ti, SKIP_ACTIVE);
+    if (v.skip) continue;
+    phase_first_update<R, MODEL>(d, v.t, state_buf(d, v.cur), state_buf(d, v.cur ^ 1));
+  }
+}
+
+// stage 1: SRD of U1, stage 2: of U2, stage 3: of the final candidate with the admissibility check.
+template <class R, int MODEL>
+__global__ void __launch_bounds__(MAX_BLOCK) phase_srd_kernel(Dev<R> d, int stage) {
+  for (int cs = blockIdx.x; cs < d.n_cases; cs += gridDim.x) {
+    int cur;
+    if (read_case_skip(d.ctl, cs, SKIP_STAGE, !d.cfg[cs].has_srd, &cur)) continue;
+    R* u = stage == 2 ? d.U2 : state_buf(d, cur ^ 1);
+    phase_srd<R, MODEL>(d, cs, u, stage == 3);
+  }
+}
+
+// Accept/reject the trial (unless begin_only) and begin the next one, one thread per case.
+static __global__ void phase_commit_kernel(CaseCtl* ctl, int n_cases, int begin_only) {
+  const int cs = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cs >= n_cases) return;
+  CaseCtl& c = ctl[cs];
+  if (!begin_only) case_commit(c);
+  case_begin(c);
+}
+
 // Host-visible launch helpers (defined in amr_engine_f64.cu / amr_engine_f32.cu).
 template <class R> struct EngineOps {
   static cudaError_t launch(const Dev<R>& d, int model, int flux, bool srd, int trials, int mode, int grid, int block,
                             cudaStream_t stream, bool cooperative);
+  // One trial (or, with mode MODE_RESIDUAL, one residual evaluation) as a sequence of phase kernels.
+  static cudaError_t launch_phases(const Dev<R>& d, int model, int flux, bool srd, int trials, int mode, int block,
+                                   cudaStream_t stream);
   static cudaError_t occupancy(int model, int flux, bool srd, int block, int* blocks_per_sm);
   static size_t smem_bytes(int block) { return size_t(12) * block * sizeof(R); }
 };

@@ -23,22 +23,28 @@ def rel_err(a, b, nv):
 
 
 def run_pair(mesh, spec, checkpoints, options=None):
+    """Advance to each cumulative step count; the maxsteps status is sticky in a session (as in
+    the reference), so each checkpoint continues in a new session created from the downloaded
+    state and counters."""
     params = spec.params()
     u0 = cases.initial_state(mesh, spec.initial_primitive())
     orc = Oracle(mesh, params)
-    s = StaticAmrGpu.create(mesh, params, u0, options=options)
     u_ref, st_ref = u0, dict(steps=0, time=0.0, rejected=0)
+    u_gpu, t_gpu, n_gpu, r_gpu = u0, 0.0, 0, 0
     errs = []
+    s = None
     for n in checkpoints:
         out = orc.run(u_ref, 1e30, n, time=st_ref['time'], steps=st_ref['steps'], rejected=st_ref['rejected'])
         assert out['error'] == 'maxsteps reached before tend'
         u_ref, st_ref = out['u'], out
+        s = StaticAmrGpu.create(mesh, params, u_gpu, time=t_gpu, steps=n_gpu, rejected=r_gpu, options=options)
         status = s.advance(1e30, n)
         assert status == 1 and 'status 3' in s.last_error, s.last_error
-        u = s.download()
-        assert (s.steps, s.rejected) == (out['steps'], out['rejected'])
-        assert s.time == out['time']
-        errs.append(rel_err(u, u_ref, mesh.nv))
+        assert s.advance(1e30, n + 5) == 1 and s.steps == n  # status 3 is sticky
+        u_gpu, t_gpu, n_gpu, r_gpu = s.download(), s.time, s.steps, s.rejected
+        assert (n_gpu, r_gpu) == (out['steps'], out['rejected'])
+        assert t_gpu == out['time']
+        errs.append(rel_err(u_gpu, u_ref, mesh.nv))
         assert errs[-1] <= TOL, (n, errs)
     return s, u_ref, errs
 
@@ -108,15 +114,18 @@ def test_fatal_statuses(golden):
     s = StaticAmrGpu.create(mesh, spec.params(), bad)
     assert s.advance(1.0, 5) == 1 and 'status 2' in s.last_error
     assert np.array_equal(s.download(), bad)
-    # dt underflow -> status 4
+    # dt underflow (time + dt == time) -> status 4
     spec4 = cases.CaseSpec(physics='euler', profile='LF1', dt_fixed=1e-300)
-    s = StaticAmrGpu.create(mesh, spec4.params(), u0)
-    assert s.advance(1.0, 5) == 1 and 'status 4' in s.last_error
+    ref4 = Oracle(mesh, spec4.params()).run(u0, 2.0, 5, time=1.0)
+    assert ref4['error'] == 'physical time step underflow'
+    s = StaticAmrGpu.create(mesh, spec4.params(), u0, time=1.0)
+    assert s.advance(2.0, 5) == 1 and 'status 4' in s.last_error
     # 21 rejections -> status 5
-    spec5 = cases.CaseSpec(physics='euler', profile='LF1', dt_fixed=50.0)
-    ref = Oracle(mesh, spec5.params()).run(u0, 1e3, 5)
+    spec5 = cases.CaseSpec(physics='euler', profile='LF1', dt_fixed=1e10)
+    ref = Oracle(mesh, spec5.params()).run(u0, 1e12, 5)
+    assert 'after 21 trials' in ref['error']
     s = StaticAmrGpu.create(mesh, spec5.params(), u0)
-    assert s.advance(1e3, 5) == 1 and 'status 5' in s.last_error
+    assert s.advance(1e12, 5) == 1 and 'status 5' in s.last_error
     assert s.rejected == ref['rejected'] == 21
     assert np.array_equal(s.download(), u0)
     # invalid advance arguments
