@@ -96,6 +96,7 @@ template <class R> struct HostCase {
   Range cells, slots, walls, terms, groups, gmembers, qcells, qlist;
   int slot = -1;
   std::vector<int> nslot, nterm;  // per-cell slot and gradient-term counts (for tiling)
+  std::vector<int> slot_prefix, term_prefix;  // n+1 running sums of nslot / nterm
   std::vector<Tile> tiles;
   CaseCfg<R> cfg;
 };
@@ -176,8 +177,9 @@ template <class R> class Batch final : public BatchBase {
               diag_part_.alloc(9 * cap_tiles_, A, error, "diag") && diag_out_.alloc(9 * c.max_cases, A, error, "diag") &&
               diag_cfg_.alloc(7 * c.max_cases, A, error, "diag") && case_tiles_.alloc(2 * c.max_cases, A, error, "diag");
     if (!ok) return false;
+    if (!s_geo_.alloc(6 * cap_slots_, A, error, "slots")) return false;
     if (model_ >= MODEL_LAMINAR) {
-      ok = s_geo_.alloc(6 * cap_slots_, A, error, "slots") && t_own_.alloc(cap_terms_, A, error, "terms") &&
+      ok = t_own_.alloc(cap_terms_, A, error, "terms") &&
            t_src_.alloc(cap_terms_, A, error, "terms") && t_x_.alloc(cap_terms_, A, error, "terms") &&
            t_y_.alloc(cap_terms_, A, error, "terms") && grad_.alloc(4 * nc, A, error, "scratch") &&
            mu_.alloc(nc, A, error, "scratch") && eddy_.alloc(nc, A, error, "scratch");
@@ -202,6 +204,7 @@ template <class R> class Batch final : public BatchBase {
     if (block_ % 32 || block_ < 64 || block_ > MAX_BLOCK) return fail(error, "block_threads must be 64..256, a multiple of 32");
     grid_request_ = c.grid_blocks;
     phases_ = c.launch_mode == AMR_B200_LAUNCH_PHASES;
+    if (phases_ && block_ != PHASE_BLOCK) return fail(error, "the phase launch mode runs 128-thread blocks");
     if (!configure_grid(error)) return false;
     return cuda_ok(cudaStreamSynchronize(stream_), error, "batch init");
   }
@@ -219,8 +222,8 @@ template <class R> class Batch final : public BatchBase {
     if (slot < 0) return 3;
     HostCase<R> hc;
     const long long n = (long long)m->n_cells;
-    const long long ns = (long long)m->face_offsets[n];
     const long long nw = (long long)m->n_walls;
+    const long long ns = (long long)m->face_offsets[n] + nw;  // face slots then wall slots, per cell
     const long long nt = model_ >= MODEL_LAMINAR ? (long long)m->visc_offsets[n] : 0;
     // SRD lists (only non-trivial neighbourhoods)
     std::vector<unsigned char> simple(n, 1);
@@ -268,8 +271,14 @@ template <class R> class Batch final : public BatchBase {
     hc.nslot.resize(n);
     hc.nterm.assign(n, 0);
     for (long long k = 0; k < n; ++k) {
-      hc.nslot[k] = (int)(m->face_offsets[k + 1] - m->face_offsets[k]);
+      hc.nslot[k] = (int)(m->face_offsets[k + 1] - m->face_offsets[k] + m->cells[k].wall_count);
       if (model_ >= MODEL_LAMINAR) hc.nterm[k] = (int)(m->visc_offsets[k + 1] - m->visc_offsets[k]);
+    }
+    hc.slot_prefix.assign(n + 1, 0);
+    hc.term_prefix.assign(n + 1, 0);
+    for (long long k = 0; k < n; ++k) {
+      hc.slot_prefix[k + 1] = hc.slot_prefix[k] + hc.nslot[k];
+      hc.term_prefix[k + 1] = hc.term_prefix[k] + hc.nterm[k];
     }
     if (!make_tiles(hc, &why)) {
       release_ranges(hc);
@@ -287,7 +296,7 @@ template <class R> class Batch final : public BatchBase {
     std::vector<unsigned char> c_flags(n + 1, 0);
     std::vector<R> c_wd(n + 1, R(1));
     std::vector<int> s_own(ns), s_nb(ns), s_meta(ns);
-    std::vector<R> s_len(ns), s_geo(model_ >= MODEL_LAMINAR ? 6 * ns : 0);
+    std::vector<R> s_len(ns), s_geo(6 * ns, R(0));
     std::vector<R> w_nx(nw), w_ny(nw), w_len(nw), w_dist(nw, R(1));
     std::vector<double> w_xm(nw), w_ym(nw);
     std::vector<int> w_donor(nw, cb);
@@ -295,7 +304,7 @@ template <class R> class Batch final : public BatchBase {
     std::vector<R> t_x(nt), t_y(nt);
     int kinds[4];
     for (int side = 0; side < 4; ++side) kinds[side] = m->boundaries[side].kind < 0 ? p->bc[side] : m->boundaries[side].kind;
-    long long wpos = 0;
+    long long wpos = 0, spos = 0;
     for (long long k = 0; k < n; ++k) {
       const amr_cell_t& c = m->cells[k];
       c_vol[k] = c.volume;
@@ -304,10 +313,10 @@ template <class R> class Batch final : public BatchBase {
       c_flags[k] = has_srd && simple[k] ? 1 : 0;
       c_cx[k] = c.cx;
       c_cy[k] = c.cy;
-      c_slot[k] = sb + (int)m->face_offsets[k];
+      c_slot[k] = sb + (int)spos;
       c_term[k] = tb + (model_ >= MODEL_LAMINAR ? (int)m->visc_offsets[k] : 0);
       if (model_ == MODEL_SA) c_wd[k] = (R)m->wall_distance[k];
-      for (uint64_t q = m->face_offsets[k]; q < m->face_offsets[k + 1]; ++q) {
+      for (uint64_t q = m->face_offsets[k]; q < m->face_offsets[k + 1]; ++q, ++spos) {
         const uint64_t fi = m->cell_faces[q];
         if (fi >= m->n_faces) return fail_release(hc, error, "cell_faces index out of range");
         const amr_face_t& f = m->faces[fi];
@@ -315,26 +324,26 @@ template <class R> class Batch final : public BatchBase {
         if (!own_left && f.right != (int)k) return fail_release(hc, error, "cell_faces lists a face of another cell");
         const int other = own_left ? f.right : f.left;
         if (other >= (int)n) return fail_release(hc, error, "face neighbour out of range");
-        if ((other < 0) != (f.boundary >= 0)) return fail_release(hc, error, "face boundary marker inconsistent");
+        if ((other < 0) != (f.boundary >= 0) || f.boundary > 3) return fail_release(hc, error, "face boundary marker inconsistent");
         const int side = f.boundary;
         const int kind = side >= 0 ? kinds[side] : 0;
-        s_own[q] = cb + (int)k;
-        s_nb[q] = other >= 0 ? cb + other : -1;
-        s_meta[q] = (own_left ? 1 : 0) | ((f.axis & 1) << 1) | ((side + 1) << 2) | ((kind & 15) << 5);
-        s_len[q] = (R)f.length;
+        s_own[spos] = cb + (int)k;
+        s_nb[spos] = other >= 0 ? cb + other : -1;
+        s_meta[spos] = (own_left ? 1 : 0) | ((f.axis & 1) << 1) | ((side + 1) << 2) | ((kind & 15) << 5);
+        s_len[spos] = (R)f.length;
         if (model_ >= MODEL_LAMINAR) {
           const amr_face_geometry_t& g = m->face_geometry[fi];
-          s_geo[6 * q + 0] = (R)g.dx;
-          s_geo[6 * q + 1] = (R)g.dy;
-          s_geo[6 * q + 2] = (R)g.ex;
-          s_geo[6 * q + 3] = (R)g.ey;
-          s_geo[6 * q + 4] = (R)g.distance;
-          s_geo[6 * q + 5] = (R)m->face_samples[fi].distance;
+          s_geo[6 * spos + 0] = (R)g.dx;
+          s_geo[6 * spos + 1] = (R)g.dy;
+          s_geo[6 * spos + 2] = (R)g.ex;
+          s_geo[6 * spos + 3] = (R)g.ey;
+          s_geo[6 * spos + 4] = (R)g.distance;
+          s_geo[6 * spos + 5] = (R)m->face_samples[fi].distance;
         }
       }
       c_wall[k] = wb + (int)wpos;
       if (c.wall_begin != (uint64_t)wpos) return fail_release(hc, error, "walls are not grouped by owner cell");
-      for (uint64_t q = c.wall_begin; q < c.wall_begin + c.wall_count; ++q, ++wpos) {
+      for (uint64_t q = c.wall_begin; q < c.wall_begin + c.wall_count; ++q, ++wpos, ++spos) {
         const amr_wall_t& w = m->walls[q];
         if (w.owner_cell != (uint64_t)k) return fail_release(hc, error, "wall owner mismatch");
         w_nx[wpos] = (R)w.nx;
@@ -342,11 +351,20 @@ template <class R> class Batch final : public BatchBase {
         w_len[wpos] = (R)w.length;
         w_xm[wpos] = (w.x0 + w.x1) * .5;
         w_ym[wpos] = (w.y0 + w.y1) * .5;
+        s_own[spos] = cb + (int)k;
+        s_nb[spos] = -1;
+        s_meta[spos] = SLOT_WALL;
+        s_len[spos] = (R)w.length;
+        s_geo[6 * spos + 0] = (R)w.nx;
+        s_geo[6 * spos + 1] = (R)w.ny;
+        s_geo[6 * spos + 2] = R(1);
         if (model_ >= MODEL_LAMINAR) {
-          const amr_wall_sample_t& s = m->wall_samples[q];
-          if (s.donor < 0 || s.donor >= n) return fail_release(hc, error, "wall donor out of range");
-          w_donor[wpos] = cb + s.donor;
-          w_dist[wpos] = (R)s.distance;
+          const amr_wall_sample_t& smp = m->wall_samples[q];
+          if (smp.donor < 0 || smp.donor >= n) return fail_release(hc, error, "wall donor out of range");
+          w_donor[wpos] = cb + smp.donor;
+          w_dist[wpos] = (R)smp.distance;
+          s_nb[spos] = cb + smp.donor;
+          s_geo[6 * spos + 2] = (R)smp.distance;
         }
       }
       if (model_ >= MODEL_LAMINAR)
@@ -360,7 +378,7 @@ template <class R> class Batch final : public BatchBase {
           t_y[q] = (R)t.y;
         }
     }
-    if (wpos != nw) return fail_release(hc, error, "wall count mismatch");
+    if (wpos != nw || spos != ns) return fail_release(hc, error, "wall count mismatch");
     c_slot[n] = sb + (int)ns;
     c_wall[n] = wb + (int)nw;
     c_term[n] = tb + (int)nt;
@@ -459,8 +477,9 @@ template <class R> class Batch final : public BatchBase {
               up(g_mem_.p + gb, g_mem, G) && up(g_cell_.p + gmb, g_cell, G) && up(g_cnt_.p + gmb, g_cnt, G) &&
               up(g_vol_.p + gb, g_vol, G) && up(q_cell_.p + qb, q_cell, G) && up(q_grp_.p + qb, q_grp, G) &&
               up(q_list_.p + qlb, q_list, G) && up(q_cnt_.p + qb, q_cnt, G);
+    ok = ok && up(s_geo_.p + 6 * (long long)sb, s_geo, G);
     if (ok && model_ >= MODEL_LAMINAR)
-      ok = up(s_geo_.p + 6 * (long long)sb, s_geo, G) && up(t_own_.p + tb, t_own, G) && up(t_src_.p + tb, t_src, G) &&
+      ok = up(t_own_.p + tb, t_own, G) && up(t_src_.p + tb, t_src, G) &&
            up(t_x_.p + tb, t_x, G) && up(t_y_.p + tb, t_y, G);
     if (ok && model_ == MODEL_SA) ok = up(c_wd_.p + cb, c_wd, G);
     for (int v = 0; ok && v < nv_; ++v) {
@@ -737,7 +756,16 @@ template <class R> class Batch final : public BatchBase {
         ++k;
       }
       if (k == start) return fail(why, "a cell has more faces or gradient terms than a thread block");
-      hc.tiles.push_back(Tile{hc.slot, cb + (int)start, cb + (int)k, first ? 1 : 0});
+      Tile t;
+      t.cs = hc.slot;
+      t.c0 = cb + (int)start;
+      t.c1 = cb + (int)k;
+      t.leader = first ? 1 : 0;
+      t.s0 = (int)hc.slots.b + hc.slot_prefix[start];
+      t.s1 = (int)hc.slots.b + hc.slot_prefix[k];
+      t.t0 = (int)hc.terms.b + hc.term_prefix[start];
+      t.t1 = (int)hc.terms.b + hc.term_prefix[k];
+      hc.tiles.push_back(t);
       first = false;
     }
     return true;

@@ -37,7 +37,7 @@ std::unique_ptr<BatchBase> make_batch(const amr_batch_config_t& c, std::string* 
 void size_for(const amr_mesh_view_t& m, amr_batch_config_t* c) {
   const uint64_t n = m.n_cells;
   c->max_cells = n;
-  c->max_faces = m.face_offsets ? m.face_offsets[n] : 0;
+  c->max_faces = (m.face_offsets ? m.face_offsets[n] : 0) + m.n_walls;  // face and wall slots
   c->max_walls = m.n_walls ? m.n_walls : 1;
   c->max_terms = (m.transport.model == AMR_B200_MODEL_LAMINAR && m.visc_offsets) ? m.visc_offsets[n] + 1 : 1;
   uint64_t nontrivial = 1;

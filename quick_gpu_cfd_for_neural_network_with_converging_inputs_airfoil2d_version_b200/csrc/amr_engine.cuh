@@ -57,9 +57,11 @@ template <class R> struct CaseCfg {
   int srd_g0, srd_g1, srd_q0, srd_q1;  // SRD group / cell list ranges
 };
 
+// A run of whole cells of one case: cells [c0, c1), their slots [s0, s1) and gradient terms [t0, t1).
 struct Tile {
-  int cs, c0, c1, leader;
+  int cs, c0, c1, leader, s0, s1, t0, t1;
 };
+constexpr int SLOT_WALL = 1 << 9;  // s_meta flag: the slot is a wall fragment of its owner cell
 
 struct GridBarrier {
   unsigned int count, gen;
@@ -224,7 +226,7 @@ __device__ void phase_gradients(const Dev<R>& d, const Tile& t, const R* Uin, R*
   const long long n = d.ncap;
   const CaseCfg<R>& cf = d.cfg[t.cs];
   const R g = cf.gamma;
-  const int t0 = d.c_term[t.c0], t1 = d.c_term[t.c1];
+  const int t0 = t.t0, t1 = t.t1;
   if (i < t1 - t0) {
     const int q = t0 + i, k = __ldg(d.t_own + q), src = __ldg(d.t_src + q);
     const R x = __ldg(d.t_x + q), y = __ldg(d.t_y + q);
@@ -301,138 +303,197 @@ __device__ void phase_gradients(const Dev<R>& d, const Tile& t, const R* Uin, R*
 // src/static_amr2d_viscous.cpp:177-206, src/static_amr2d_sa.cpp:81-96, 395-426).
 // ------------------------------------------------------------------------------------------
 template <class R, int MODEL, int FLUX>
+__device__ __forceinline__ void slot_face(const Dev<R>& d, const CaseCfg<R>& cf, int s, int k, int nb, int meta,
+                                          const R* Uin, bool base, R* sm, int B, int i, bool& bad) {
+  const long long n = d.ncap;
+  const R g = cf.gamma;
+  const bool own_left = meta & 1;
+  const int axis = (meta >> 1) & 1, side = ((meta >> 2) & 7) - 1, kind = (meta >> 5) & 15;
+  // Every load of this slot is issued up front and unconditionally (an exterior face reads its
+  // own cell twice), so the whole neighbourhood arrives in one memory round trip.
+  const int m = nb >= 0 ? nb : k;
+  const R len = __ldg(d.s_len + s);
+  R uk[5], um[5];
+  for (int v = 0; v < 4; ++v) { uk[v] = Uin[v * n + k]; um[v] = Uin[v * n + m]; }
+  if (MODEL == MODEL_SA) { uk[4] = Uin[4 * n + k]; um[4] = Uin[4 * n + m]; }
+  R gk[4], gm[4], geo[6], mk = 0, mm = 0, ek = 0, em = 0, sgk[2] = {0, 0}, sgm[2] = {0, 0}, sdk = 0, sdm = 0;
+  if (MODEL >= MODEL_LAMINAR) {
+    for (int v = 0; v < 4; ++v) { gk[v] = d.grad[v * n + k]; gm[v] = d.grad[v * n + m]; }
+    mk = d.mu[k]; mm = d.mu[m]; ek = d.eddy[k]; em = d.eddy[m];
+    const R* gp = d.s_geo + 6 * (long long)s;
+    for (int v = 0; v < 6; ++v) geo[v] = __ldg(gp + v);
+    if (MODEL == MODEL_SA) {
+      sgk[0] = d.sgrad[k]; sgk[1] = d.sgrad[n + k]; sgm[0] = d.sgrad[m]; sgm[1] = d.sgrad[n + m];
+      sdk = d.sdiff[k]; sdm = d.sdiff[m];
+    }
+  }
+  Prim<R> wk, wn;
+  wk.rho = uk[0]; wk.u = uk[1] / uk[0]; wk.v = uk[2] / uk[0]; wk.p = (g - R(1)) * (uk[3] - R(0.5) * (uk[1] * wk.u + uk[2] * wk.v));
+  wn.rho = um[0]; wn.u = um[1] / um[0]; wn.v = um[2] / um[0]; wn.p = (g - R(1)) * (um[3] - R(0.5) * (um[1] * wn.u + um[2] * wn.v));
+  // face-oriented states: a = left, b = right
+  R a[4], b[4];
+  a[0] = own_left ? wk.rho : wn.rho; a[1] = own_left ? wk.u : wn.u; a[2] = own_left ? wk.v : wn.v; a[3] = own_left ? wk.p : wn.p;
+  b[0] = own_left ? wn.rho : wk.rho; b[1] = own_left ? wn.u : wk.u; b[2] = own_left ? wn.v : wk.v; b[3] = own_left ? wn.p : wk.p;
+  if (side >= 0) {
+    const R wi[4] = {wk.rho, wk.u, wk.v, wk.p};
+    R wo[4];
+    if (!bc_state(cf.bnd[side], kind, g, side, wi, wo)) bad = true;
+    if (own_left) { b[0] = wo[0]; b[1] = wo[1]; b[2] = wo[2]; b[3] = wo[3]; }
+    else { a[0] = wo[0]; a[1] = wo[1]; a[2] = wo[2]; a[3] = wo[3]; }
+  }
+  const R an = axis ? a[2] : a[1], at = axis ? a[1] : a[2];
+  const R bn = axis ? b[2] : b[1], bt = axis ? b[1] : b[2];
+  R F[4];
+  if (side >= 0 && kind == BC_NOSLIP) {
+    F[0] = 0; F[1] = wk.p; F[2] = 0; F[3] = 0;
+  } else if (FLUX == FLUX_HLLC) {
+    flux_hllc(a[0], an, at, a[3], b[0], bn, bt, b[3], g, F);
+  } else {
+    flux_ausmpup(a[0], an, at, a[3], b[0], bn, bt, b[3], g, cf.mco, F);
+  }
+  // conserved components: normal momentum goes to 1+axis, tangential to 2-axis
+  const R f0 = F[0] * len, fn = F[1] * len, ft = F[2] * len, f3 = F[3] * len;
+  for (int v = 0; v < 4; ++v) if (!isfinite(F[v])) bad = true;
+  const R sg = own_left ? R(1) : R(-1);
+  sm[0 * B + i] = sg * f0;
+  sm[1 * B + i] = sg * (axis ? ft : fn);
+  sm[2 * B + i] = sg * (axis ? fn : ft);
+  sm[3 * B + i] = sg * f3;
+  if (base) {
+    const R speed = rmax(R(fabs(an)) + sqrt(g * a[3] / a[0]), R(fabs(bn)) + sqrt(g * b[3] / b[0]));
+    sm[8 * B + i] = speed * len;
+  }
+  if (MODEL >= MODEL_LAMINAR) {
+    R gv[4], mu, uf, vf, nu, distance;
+    if (side < 0) {
+      Prim<R> wl, wr;
+      wl.rho = own_left ? wk.rho : wn.rho; wl.u = own_left ? wk.u : wn.u; wl.v = own_left ? wk.v : wn.v; wl.p = own_left ? wk.p : wn.p;
+      wr.rho = own_left ? wn.rho : wk.rho; wr.u = own_left ? wn.u : wk.u; wr.v = own_left ? wn.v : wk.v; wr.p = own_left ? wn.p : wk.p;
+      R gl[4], grr[4];
+      for (int v = 0; v < 4; ++v) { gl[v] = own_left ? gk[v] : gm[v]; grr[v] = own_left ? gm[v] : gk[v]; }
+      correct_gradient(gl, grr, geo[0], geo[1], wr.u - wl.u, wr.v - wl.v, gv);
+      uf = R(.5) * (wl.u + wr.u) + gv[0] * geo[2] + gv[1] * geo[3];
+      vf = R(.5) * (wl.v + wr.v) + gv[2] * geo[2] + gv[3] * geo[3];
+      const R el = own_left ? ek : em, er = own_left ? em : ek, ml = own_left ? mk : mm, mr = own_left ? mm : mk;
+      const R temp = R(.5) * (wl.p / wl.rho + wr.p / wr.rho) / cf.trn.gas_constant;
+      mu = dyn_visc(cf.trn, temp) + R(.5) * (el + er);
+      nu = rmax((ml + el) / wl.rho, (mr + er) / wr.rho);
+      distance = geo[4];
+    } else {
+      for (int v = 0; v < 4; ++v) gv[v] = gk[v];
+      mu = mk + ek;
+      uf = wk.u;
+      vf = wk.v;
+      nu = mu / wk.rho;
+      distance = geo[5];
+      const R sside = side % 2 ? R(1) : R(-1);
+      if (kind == BC_NOSLIP) {
+        mu = mk;
+        uf = cf.bnd[side].wall_velocity[0];
+        vf = cf.bnd[side].wall_velocity[1];
+        wall_gradient(axis == 0 ? sside : R(0), axis == 1 ? sside : R(0), distance, uf - wk.u, vf - wk.v, gv);
+      } else if (kind == BC_REFLECT) {
+        gv[1] = 0; gv[2] = 0;
+        if (axis == 0) uf = 0; else vf = 0;
+      } else {
+        if (axis) { gv[1] = 0; gv[3] = 0; } else { gv[0] = 0; gv[2] = 0; }
+        uf += gv[0] * geo[2] + gv[1] * geo[3];
+        vf += gv[2] * geo[2] + gv[3] * geo[3];
+      }
+    }
+    R fv[4];
+    visc_flux(mu, gv, axis == 0 ? R(1) : R(0), axis == 1 ? R(1) : R(0), uf, vf, fv);
+    for (int v = 0; v < 4; ++v) {
+      if (!isfinite(fv[v])) bad = true;
+      sm[(4 + v) * B + i] = sg * (fv[v] * len);
+    }
+    if (base) sm[9 * B + i] = R(4.0 / 3) * nu / distance * len;
+    if (MODEL == MODEL_SA) {
+      const R mass = f0 - fv[0] * len;
+      const R phk = uk[4] / wk.rho;
+      const R phn = nb >= 0 ? um[4] / wn.rho : cf.trn.sa_nu_inf;
+      const R left = own_left ? phk : phn, right = own_left ? phn : phk;
+      R diff = 0, fc = 0;
+      if (side < 0) {
+        const R gl[4] = {own_left ? sgk[0] : sgm[0], own_left ? sgk[1] : sgm[1], 0, 0};
+        const R grr[4] = {own_left ? sgm[0] : sgk[0], own_left ? sgm[1] : sgk[1], 0, 0};
+        R gs[4];
+        correct_gradient(gl, grr, geo[0], geo[1], right - left, R(0), gs);
+        const R rl = own_left ? wk.rho : wn.rho, rr = own_left ? wn.rho : wk.rho;
+        const R dl = own_left ? sdk : sdm, dr = own_left ? sdm : sdk;
+        const R coefficient = R(.5) * (rl * dl + rr * dr);
+        diff = coefficient * (axis ? gs[1] : gs[0]) * len;
+        fc = coefficient / geo[4] * len;
+      } else {
+        const bool inflow = own_left ? mass < R(0) : mass > R(0);
+        const R sside = side % 2 ? R(1) : R(-1);
+        if (kind == BC_NOSLIP || inflow) {
+          const R wall = kind == BC_NOSLIP ? R(0) : cf.trn.sa_nu_inf;
+          const R coefficient = kind == BC_NOSLIP ? mk / R(AMRB_SIG) : wk.rho * sdk;
+          diff = sside * coefficient * (wall - phk) / distance * len;
+          fc = coefficient / distance * len;
+        }
+      }
+      sm[10 * B + i] = sg * (mass * (mass >= R(0) ? left : right) - diff);
+      if (base) sm[11 * B + i] = fc;
+    }
+  }
+}
+
+// A wall fragment of cell k: pressure force (reference src/static_amr2d.cpp:193-195), viscous wall
+// flux from the visible donor (src/static_amr2d_viscous.cpp:192-196) and the SA wall flux
+// (src/static_amr2d_sa.cpp:91), with their spectral-radius contributions.
+template <class R, int MODEL>
+__device__ __forceinline__ void slot_wall(const Dev<R>& d, const CaseCfg<R>& cf, int s, int k, int dn,
+                                          const R* Uin, bool base, R* sm, int B, int i, bool& bad) {
+  const long long n = d.ncap;
+  const R g = cf.gamma;
+  const R wl = __ldg(d.s_len + s);
+  const R* geo = d.s_geo + 6 * (long long)s;
+  const R nx = __ldg(geo + 0), ny = __ldg(geo + 1);
+  const Prim<R> wk = prim(Uin, n, k, g);
+  sm[0 * B + i] = 0;
+  sm[1 * B + i] = wk.p * nx * wl;
+  sm[2 * B + i] = wk.p * ny * wl;
+  sm[3 * B + i] = 0;
+  if (base) sm[8 * B + i] = sqrt(g * wk.p / wk.rho) * wl;
+  if (MODEL >= MODEL_LAMINAR) {
+    const R wdist = __ldg(geo + 2);
+    const R rd = Uin[dn], ud = Uin[n + dn] / rd, vd = Uin[2 * n + dn] / rd;
+    const R md = d.mu[dn];
+    R gw[4], fw[4];
+    wall_gradient(nx, ny, wdist, -ud, -vd, gw);
+    visc_flux(md, gw, nx, ny, R(0), R(0), fw);
+    for (int v = 0; v < 4; ++v) {
+      if (!isfinite(fw[v])) bad = true;
+      sm[(4 + v) * B + i] = fw[v] * wl;
+    }
+    if (base) sm[9 * B + i] = R(4.0 / 3) * rmax(md / rd, d.mu[k] / wk.rho) / wdist * wl;
+    if (MODEL == MODEL_SA) {
+      const R swc = md / R(AMRB_SIG) / wdist * wl;
+      sm[10 * B + i] = -swc * (Uin[4 * n + dn] / rd);
+      if (base) sm[11 * B + i] = swc;
+    }
+  }
+}
+
+template <class R, int MODEL, int FLUX>
 __device__ void phase_flux(const Dev<R>& d, const Tile& t, int stage, const R* Uin, R* Ub, R* Un, R* sm,
                            bool* tile_bad, double* tile_dt) {
   const int B = blockDim.x, i = threadIdx.x;
   const long long n = d.ncap;
   const CaseCfg<R>& cf = d.cfg[t.cs];
   const R g = cf.gamma;
-  const int s0 = d.c_slot[t.c0], s1 = d.c_slot[t.c1];
+  const int s0 = t.s0, s1 = t.s1;
   const bool base = stage == STAGE_BASE;
   bool bad = false;
   if (i < s1 - s0) {
     const int s = s0 + i;
     const int k = __ldg(d.s_own + s), nb = __ldg(d.s_nb + s), meta = __ldg(d.s_meta + s);
-    const bool own_left = meta & 1;
-    const int axis = (meta >> 1) & 1, side = ((meta >> 2) & 7) - 1, kind = (meta >> 5) & 15;
-    const int normal = 1 + axis, tangent = 2 - axis;
-    const R len = __ldg(d.s_len + s);
-    const Prim<R> wk = prim(Uin, n, k, g);
-    const Prim<R> wn = nb >= 0 ? prim(Uin, n, nb, g) : wk;
-    // face-oriented states: a = left, b = right
-    R a[4], b[4];
-    a[0] = own_left ? wk.rho : wn.rho; a[1] = own_left ? wk.u : wn.u; a[2] = own_left ? wk.v : wn.v; a[3] = own_left ? wk.p : wn.p;
-    b[0] = own_left ? wn.rho : wk.rho; b[1] = own_left ? wn.u : wk.u; b[2] = own_left ? wn.v : wk.v; b[3] = own_left ? wn.p : wk.p;
-    if (side >= 0) {
-      const R wi[4] = {wk.rho, wk.u, wk.v, wk.p};
-      R wo[4];
-      if (!bc_state(cf.bnd[side], kind, g, side, wi, wo)) bad = true;
-      if (own_left) { b[0] = wo[0]; b[1] = wo[1]; b[2] = wo[2]; b[3] = wo[3]; }
-      else { a[0] = wo[0]; a[1] = wo[1]; a[2] = wo[2]; a[3] = wo[3]; }
-    }
-    const R an = axis ? a[2] : a[1], at = axis ? a[1] : a[2];
-    const R bn = axis ? b[2] : b[1], bt = axis ? b[1] : b[2];
-    R F[4];
-    if (side >= 0 && kind == BC_NOSLIP) {
-      F[0] = 0; F[1] = wk.p; F[2] = 0; F[3] = 0;
-    } else if (FLUX == FLUX_HLLC) {
-      flux_hllc(a[0], an, at, a[3], b[0], bn, bt, b[3], g, F);
-    } else {
-      flux_ausmpup(a[0], an, at, a[3], b[0], bn, bt, b[3], g, cf.mco, F);
-    }
-    // conserved components: normal momentum goes to 1+axis, tangential to 2-axis
-    const R f0 = F[0] * len, fn = F[1] * len, ft = F[2] * len, f3 = F[3] * len;
-    R Fl[4];
-    Fl[0] = f0;
-    Fl[1] = axis ? ft : fn;
-    Fl[2] = axis ? fn : ft;
-    Fl[3] = f3;
-    for (int v = 0; v < 4; ++v) if (!isfinite(F[v])) bad = true;
-    const R sg = own_left ? R(1) : R(-1);
-    for (int v = 0; v < 4; ++v) sm[v * B + i] = sg * Fl[v];
-    if (base) {
-      const R speed = rmax(R(fabs(an)) + sqrt(g * a[3] / a[0]), R(fabs(bn)) + sqrt(g * b[3] / b[0]));
-      sm[8 * B + i] = speed * len;
-    }
-    if (MODEL >= MODEL_LAMINAR) {
-      const R* geo = d.s_geo + 6 * (long long)s;
-      R gv[4], mu, uf, vf, nu, distance;
-      if (side < 0) {
-        const int l = own_left ? k : nb, r = own_left ? nb : k;
-        Prim<R> wl, wr;
-        wl.rho = own_left ? wk.rho : wn.rho; wl.u = own_left ? wk.u : wn.u; wl.v = own_left ? wk.v : wn.v; wl.p = own_left ? wk.p : wn.p;
-        wr.rho = own_left ? wn.rho : wk.rho; wr.u = own_left ? wn.u : wk.u; wr.v = own_left ? wn.v : wk.v; wr.p = own_left ? wn.p : wk.p;
-        R gl[4], grr[4];
-        for (int v = 0; v < 4; ++v) { gl[v] = d.grad[v * n + l]; grr[v] = d.grad[v * n + r]; }
-        const R dx = __ldg(geo + 0), dy = __ldg(geo + 1), ex = __ldg(geo + 2), ey = __ldg(geo + 3);
-        correct_gradient(gl, grr, dx, dy, wr.u - wl.u, wr.v - wl.v, gv);
-        uf = R(.5) * (wl.u + wr.u) + gv[0] * ex + gv[1] * ey;
-        vf = R(.5) * (wl.v + wr.v) + gv[2] * ex + gv[3] * ey;
-        const R el = d.eddy[l], er = d.eddy[r], ml = d.mu[l], mr = d.mu[r];
-        const R temp = R(.5) * (wl.p / wl.rho + wr.p / wr.rho) / cf.trn.gas_constant;
-        mu = dyn_visc(cf.trn, temp) + R(.5) * (el + er);
-        nu = rmax((ml + el) / wl.rho, (mr + er) / wr.rho);
-        distance = __ldg(geo + 4);
-      } else {
-        for (int v = 0; v < 4; ++v) gv[v] = d.grad[v * n + k];
-        const R mk = d.mu[k];
-        mu = mk + d.eddy[k];
-        uf = wk.u;
-        vf = wk.v;
-        nu = mu / wk.rho;
-        distance = __ldg(geo + 5);
-        const R sside = side % 2 ? R(1) : R(-1);
-        if (kind == BC_NOSLIP) {
-          mu = mk;
-          uf = cf.bnd[side].wall_velocity[0];
-          vf = cf.bnd[side].wall_velocity[1];
-          wall_gradient(axis == 0 ? sside : R(0), axis == 1 ? sside : R(0), distance, uf - wk.u, vf - wk.v, gv);
-        } else if (kind == BC_REFLECT) {
-          gv[1] = 0; gv[2] = 0;
-          if (axis == 0) uf = 0; else vf = 0;
-        } else {
-          const R ex = __ldg(geo + 2), ey = __ldg(geo + 3);
-          if (axis) { gv[1] = 0; gv[3] = 0; } else { gv[0] = 0; gv[2] = 0; }
-          uf += gv[0] * ex + gv[1] * ey;
-          vf += gv[2] * ex + gv[3] * ey;
-        }
-      }
-      R fv[4];
-      visc_flux(mu, gv, axis == 0 ? R(1) : R(0), axis == 1 ? R(1) : R(0), uf, vf, fv);
-      for (int v = 0; v < 4; ++v) {
-        if (!isfinite(fv[v])) bad = true;
-        sm[(4 + v) * B + i] = sg * (fv[v] * len);
-      }
-      if (base) sm[9 * B + i] = R(4.0 / 3) * nu / distance * len;
-      if (MODEL == MODEL_SA) {
-        const R mass = Fl[0] - fv[0] * len;
-        const R phk = Uin[4 * n + k] / wk.rho;
-        const R phn = nb >= 0 ? Uin[4 * n + nb] / wn.rho : cf.trn.sa_nu_inf;
-        const R left = own_left ? phk : phn, right = own_left ? phn : phk;
-        R diff = 0, fc = 0;
-        if (side < 0) {
-          const int l = own_left ? k : nb, r = own_left ? nb : k;
-          const R gl[4] = {d.sgrad[l], d.sgrad[n + l], 0, 0}, grr[4] = {d.sgrad[r], d.sgrad[n + r], 0, 0};
-          R gs[4];
-          correct_gradient(gl, grr, R(__ldg(geo + 0)), R(__ldg(geo + 1)), right - left, R(0), gs);
-          const R rl = own_left ? wk.rho : wn.rho, rr = own_left ? wn.rho : wk.rho;
-          const R coefficient = R(.5) * (rl * d.sdiff[l] + rr * d.sdiff[r]);
-          diff = coefficient * (axis ? gs[1] : gs[0]) * len;
-          fc = coefficient / __ldg(geo + 4) * len;
-        } else {
-          const bool inflow = own_left ? mass < R(0) : mass > R(0);
-          const R sside = side % 2 ? R(1) : R(-1);
-          if (kind == BC_NOSLIP || inflow) {
-            const R wall = kind == BC_NOSLIP ? R(0) : cf.trn.sa_nu_inf;
-            const R coefficient = kind == BC_NOSLIP ? d.mu[k] / R(AMRB_SIG) : wk.rho * d.sdiff[k];
-            diff = sside * coefficient * (wall - phk) / distance * len;
-            fc = coefficient / distance * len;
-          }
-        }
-        sm[10 * B + i] = sg * (mass * (mass >= R(0) ? left : right) - diff);
-        if (base) sm[11 * B + i] = fc;
-      }
-    }
+    if (meta & SLOT_WALL)
+      slot_wall<R, MODEL>(d, cf, s, k, nb, Uin, base, sm, B, i, bad);
+    else
+      slot_face<R, MODEL, FLUX>(d, cf, s, k, nb, meta, Uin, base, sm, B, i, bad);
   }
   __syncthreads();
   double cell_dt = __longlong_as_double(0x7FF0000000000000ll);
@@ -441,14 +502,15 @@ __device__ void phase_flux(const Dev<R>& d, const Tile& t, int stage, const R* U
     const double V = d.c_vol[k];
     const Prim<R> wk = prim(Uin, n, k, g);
     if (!prim_ok(Uin, n, k, wk)) bad = true;
+    // slots of cell k: faces [a, e) in CSR order, then walls [e, b)
     const int a = d.c_slot[k] - s0, b = d.c_slot[k + 1] - s0;
+    const int e = b - (d.c_wall[k + 1] - d.c_wall[k]);
     R sum[4] = {0, 0, 0, 0};
-    for (int q = a; q < b; ++q)
+    for (int q = a; q < e; ++q)
       for (int v = 0; v < 4; ++v) sum[v] += sm[v * B + q];
-    const int w0 = d.c_wall[k], w1 = d.c_wall[k + 1];
-    for (int q = w0; q < w1; ++q) {
-      sum[1] += wk.p * __ldg(d.w_nx + q) * __ldg(d.w_len + q);
-      sum[2] += wk.p * __ldg(d.w_ny + q) * __ldg(d.w_len + q);
+    for (int q = e; q < b; ++q) {
+      sum[1] += sm[1 * B + q];
+      sum[2] += sm[2 * B + q];
     }
     R res[5];
     for (int v = 0; v < 4; ++v) res[v] = (R)(-sum[v] / V);
@@ -459,33 +521,17 @@ __device__ void phase_flux(const Dev<R>& d, const Tile& t, int stage, const R* U
         for (int v = 0; v < 4; ++v) vs[v] += sm[(4 + v) * B + q];
         if (base) vspec += sm[9 * B + q];
       }
-      R snet = 0;
-      if (MODEL == MODEL_SA)
-        for (int q = a; q < b; ++q) {
+      for (int v = 0; v < 4; ++v) res[v] += (R)(vs[v] / V);
+      if (MODEL == MODEL_SA) {
+        R snet = 0;
+        for (int q = a; q < e; ++q) {
           snet += sm[10 * B + q];
           if (base) sspec += sm[11 * B + q];
         }
-      for (int q = w0; q < w1; ++q) {
-        const int dn = __ldg(d.w_donor + q);
-        const R nx = __ldg(d.w_nx + q), ny = __ldg(d.w_ny + q), wl = __ldg(d.w_len + q), wdist = __ldg(d.w_dist + q);
-        const R rd = Uin[dn], ud = Uin[n + dn] / rd, vd = Uin[2 * n + dn] / rd;
-        const R md = d.mu[dn];
-        R gw[4], fw[4];
-        wall_gradient(nx, ny, wdist, -ud, -vd, gw);
-        visc_flux(md, gw, nx, ny, R(0), R(0), fw);
-        for (int v = 0; v < 4; ++v) {
-          if (!isfinite(fw[v])) bad = true;
-          vs[v] += fw[v] * wl;
+        for (int q = e; q < b; ++q) {
+          snet -= sm[10 * B + q];
+          if (base) sspec += sm[11 * B + q];
         }
-        if (base) vspec += R(4.0 / 3) * rmax(md / rd, d.mu[k] / wk.rho) / wdist * wl;
-        if (MODEL == MODEL_SA) {
-          const R swc = md / R(AMRB_SIG) / wdist * wl;
-          snet -= -swc * (Uin[4 * n + dn] / rd);
-          if (base) sspec += swc;
-        }
-      }
-      for (int v = 0; v < 4; ++v) res[v] += (R)(vs[v] / V);
-      if (MODEL == MODEL_SA) {
         res[4] = (R)(-snet / V) + d.ssrc[k];
         if (!isfinite(res[4])) bad = true;
       }
@@ -494,8 +540,6 @@ __device__ void phase_flux(const Dev<R>& d, const Tile& t, int stage, const R* U
     if (base) {
       R spectral = 0;
       for (int q = a; q < b; ++q) spectral += sm[8 * B + q];
-      const R c = sqrt(g * wk.p / wk.rho);
-      for (int q = w0; q < w1; ++q) spectral += c * __ldg(d.w_len + q);
       if (spectral > R(0)) cell_dt = cf.cfl * d.c_area[k] / (double)spectral;
       if (MODEL >= MODEL_LAMINAR) {
         const double vdt = vspec > R(0) ? cf.viscous_cfl * V / (double)vspec : __longlong_as_double(0x7FF0000000000000ll);
@@ -845,13 +889,23 @@ __global__ void __launch_bounds__(MAX_BLOCK) trials_kernel(Dev<R> d, int trials,
 //   [srd 3], commit
 // and a CUDA graph replays `trials` such sequences.
 // ------------------------------------------------------------------------------------------
+// Phase kernels run 128-thread blocks; the occupancy target sets the register budget
+// (FP32: 8 blocks -> 64 registers, FP64: 3 blocks -> 168 registers).
+constexpr int PHASE_BLOCK = 128;
+#ifndef AMRB_FLUX_MINB_F32
+#define AMRB_FLUX_MINB_F32 8
+#endif
+template <class R> struct PhaseOcc;
+template <> struct PhaseOcc<float> { static constexpr int flux = AMRB_FLUX_MINB_F32, grad = 8; };
+template <> struct PhaseOcc<double> { static constexpr int flux = 3, grad = 4; };
+
 template <class R> __device__ __forceinline__ const R* stage_input(const Dev<R>& d, int stage, int cur) {
   if (stage == STAGE_BASE || stage == STAGE_DIAG) return state_buf(d, cur);
   return stage == STAGE_1 ? state_buf(d, cur ^ 1) : d.U2;
 }
 
 template <class R, int MODEL>
-__global__ void __launch_bounds__(MAX_BLOCK, 2) phase_grad_kernel(Dev<R> d, int stage) {
+__global__ void __launch_bounds__(PHASE_BLOCK, PhaseOcc<R>::grad) phase_grad_kernel(Dev<R> d, int stage) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* sm = reinterpret_cast<R*>(smem_raw);
   const int rule = stage == STAGE_DIAG ? SKIP_LIVE : (stage == STAGE_BASE ? SKIP_ACTIVE : SKIP_STAGE);
@@ -863,7 +917,7 @@ __global__ void __launch_bounds__(MAX_BLOCK, 2) phase_grad_kernel(Dev<R> d, int 
 }
 
 template <class R, int MODEL, int FLUX>
-__global__ void __launch_bounds__(MAX_BLOCK, 2) phase_flux_kernel(Dev<R> d, int stage) {
+__global__ void __launch_bounds__(PHASE_BLOCK, PhaseOcc<R>::flux) phase_flux_kernel(Dev<R> d, int stage) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* sm = reinterpret_cast<R*>(smem_raw);
   __shared__ bool s_bad;
@@ -890,6 +944,42 @@ __global__ void __launch_bounds__(MAX_BLOCK, 4) phase_first_kernel(Dev<R> d) {
     const TileView v = read_tile(d.tiles, d.ctl, ti, SKIP_ACTIVE);
     if (v.skip) continue;
     phase_first_update<R, MODEL>(d, v.t, state_buf(d, v.cur), state_buf(d, v.cur ^ 1));
+  }
+}
+
+// U1 = U + dt R0, one thread per cell (phase mode).  Every thread derives its case's step size
+// from the control record; the first cell of each case records it.
+template <class R, int MODEL>
+__global__ void __launch_bounds__(MAX_BLOCK) phase_first_cells_kernel(Dev<R> d, int ncells) {
+  const long long n = d.ncap;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ncells; k += gridDim.x * blockDim.x) {
+    const int cs = d.c_case[k];
+    if (cs < 0) continue;
+    const CaseCtl& c = d.ctl[cs];
+    if (!c.active) continue;
+    const CaseCfg<R>& cf = d.cfg[cs];
+    double dt;
+    int fatal;
+    const bool ok = choose_dt(c, cf.dt_fixed, &dt, &fatal);
+    if (k == 0 || d.c_case[k - 1] != cs) {
+      if (ok) {
+        d.ctl[cs].dt_trial = dt;
+        if (!c.retrying) d.ctl[cs].attempt = 0;
+      } else {
+        d.ctl[cs].fatal = fatal;
+      }
+    }
+    if (!ok) continue;
+    const R dtr = (R)dt;
+    R* Ub = state_buf(d, c.cur);
+    R* Un = state_buf(d, c.cur ^ 1);
+    const bool simple = cf.has_srd && (d.c_flags[k] & 1);
+    const int nv = MODEL == MODEL_SA ? 5 : 4;
+    for (int v = 0; v < nv; ++v) {
+      R u = Ub[v * n + k] + dtr * d.R0[v * n + k];
+      if (simple && v < 4) u = srd_self(u, d.c_vol[k], d.c_gvol[k]);
+      Un[v * n + k] = u;
+    }
   }
 }
 

@@ -49,7 +49,7 @@ static cudaError_t launch_phases_t(const Dev<R>& d, bool srd, int trials, int mo
   for (int t = 0; t < trials; ++t) {
     if (MODEL >= MODEL_LAMINAR) phase_grad_kernel<R, MODEL><<<tiles, block, sm, st>>>(d, STAGE_BASE);
     phase_flux_kernel<R, MODEL, FLUX><<<tiles, block, sm, st>>>(d, STAGE_BASE);
-    phase_first_kernel<R, MODEL><<<tiles, block, 0, st>>>(d);
+    phase_first_cells_kernel<R, MODEL><<<(int)((d.ncap + 255) / 256), 256, 0, st>>>(d, (int)d.ncap);
     for (int stage = 1; stage <= 2; ++stage) {
       if (srd) phase_srd_kernel<R, MODEL><<<cases, block, 0, st>>>(d, stage);
       if (MODEL >= MODEL_LAMINAR) phase_grad_kernel<R, MODEL><<<tiles, block, sm, st>>>(d, stage);
@@ -200,6 +200,7 @@ template <class R> int Batch<R>::autotune(int trials, std::string* error) {
   use_graph_ = false;
   for (int phases = 0; phases <= 1; ++phases) {
     for (int block : {128, 256}) {
+      if (phases && block != PHASE_BLOCK) continue;
       phases_ = phases != 0;
       block_ = block;
       grid_request_ = 0;
