@@ -228,6 +228,25 @@ int amr_gpu_residual(amr_gpu_session* session, double* r_out, uint64_t r_count,
 int amr_gpu_diagnostics(amr_gpu_session* session, const double region[4], double moment_x,
                         double moment_y, double out[8], char* error, uint64_t error_size);
 
+/* Residual dU/dt of the inviscid (Euler) model that allocates no device memory.  It has no
+ * counterpart in the reference.  It is for callers that cannot call cudaMalloc at the point where
+ * they need a residual: code running under another framework's memory pool or allocator, a
+ * latency-critical loop in which an allocation would synchronise the device, or a plug-in that
+ * is handed device buffers but may not own memory.  The caller passes device pointers to its own
+ * copies of the mesh records (cells, faces, walls, face_offsets, cell_faces in the layout above),
+ * the state u[4*n_cells] and the output r[4*n_cells]; boundaries[4] and params are host records;
+ * stream is a cudaStream_t (NULL: the default stream).  The scratch (primitives and face fluxes)
+ * lives in one static device array of 1.8 MB that every GPU loading the library holds until the
+ * process exits, so meshes are limited to 16384 cells and 40960 faces; larger ones are rejected
+ * with an error.  The first call on a device looks up that array's device address, so make it
+ * before any stream capture.  All calls on a device share the array: calls whose kernels
+ * overlap on the GPU (other streams or host threads) race.  Synchronises `stream`; returns 1
+ * with a message for a nonphysical state, like amr_gpu_residual. */
+int amr_euler_residual_static(const amr_cell_t* cells, uint64_t n_cells, const amr_face_t* faces, uint64_t n_faces,
+                              const amr_wall_t* walls, uint64_t n_walls, const uint64_t* face_offsets,
+                              const uint64_t* cell_faces, const amr_boundary_t* boundaries, const amr_params_t* params,
+                              const double* u, double* r, void* stream, char* error, uint64_t error_size);
+
 /* ----------------------------------------------------------------------------------
  * Batched form.
  * ---------------------------------------------------------------------------------- */

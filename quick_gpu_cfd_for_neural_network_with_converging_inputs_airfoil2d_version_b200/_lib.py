@@ -21,6 +21,8 @@ SIGNATURES = {
     'amr_gpu_destroy': (None, [_P]),
     'amr_gpu_residual': (C.c_int, [_P, _P, C.c_uint64, _S, C.c_uint64]),
     'amr_gpu_diagnostics': (C.c_int, [_P, _P, C.c_double, C.c_double, _P, _S, C.c_uint64]),
+    'amr_euler_residual_static': (C.c_int, [_P, C.c_uint64, _P, C.c_uint64, _P, C.c_uint64, _P, _P, _P, _P, _P, _P, _P,
+                                            _S, C.c_uint64]),
     'amr_batch_create': (C.c_int, [_P, _P, _S, C.c_uint64]),
     'amr_batch_admit': (C.c_int, [_P, _P, _P, _P, C.c_uint64, _P, _P, _S, C.c_uint64]),
     'amr_batch_advance': (C.c_int, [_P, C.c_int32, _S, C.c_uint64]),

@@ -23,6 +23,7 @@ UNITS = {
     'amr_engine_f64.cu': ['-fmad=false'],
     'amr_engine_f32.cu': ['--use_fast_math'],
     'amr_capi.cu': [],
+    'amr_static.cu': ['-fmad=false'],
 }
 
 
