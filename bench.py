@@ -126,7 +126,8 @@ def parse_launch(cfg):
     """(block, grid, launch_mode) of a launch_config() string."""
     block = int(cfg.split('block=')[1].split()[0])
     grid = int(cfg.split('grid=')[1].split()[0])
-    mode = _abi.LAUNCH_PHASES if 'mode=phases' in cfg else _abi.LAUNCH_PERSISTENT
+    mode = (_abi.LAUNCH_PHASES if 'mode=phases' in cfg else _abi.LAUNCH_SPLIT if 'mode=split' in cfg
+            else _abi.LAUNCH_PERSISTENT)
     return block, grid, mode
 
 
@@ -329,7 +330,7 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--cases', type=int, default=256)
     ap.add_argument('--no-cpu', action='store_true')
-    ap.add_argument('--profile', choices=['persistent', 'phases'], default=None,
+    ap.add_argument('--profile', choices=['persistent', 'phases', 'split'], default=None,
                     help='only the timed batched loop, with this launch mode and --block (for ncu)')
     ap.add_argument('--block', type=int, default=128)
     ap.add_argument('--precision', type=int, default=32, choices=[32, 64])
@@ -341,7 +342,7 @@ def main():
         return
     case_list = batched_cases(args.cases, seed=20261203 + rank)
     if args.profile:
-        mode = _abi.LAUNCH_PHASES if args.profile == 'phases' else _abi.LAUNCH_PERSISTENT
+        mode = {'phases': _abi.LAUNCH_PHASES, 'split': _abi.LAUNCH_SPLIT}.get(args.profile, _abi.LAUNCH_PERSISTENT)
         b = Batch(precision=args.precision, model=_abi.MODEL_LAMINAR, sa=True, max_cases=len(case_list),
                   max_cells=sum(m.n_cells for _, m in case_list) + 64, device=local, block_threads=args.block,
                   launch_mode=mode)

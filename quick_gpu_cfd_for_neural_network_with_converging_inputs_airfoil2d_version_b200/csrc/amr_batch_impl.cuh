@@ -93,7 +93,7 @@ struct Range {
 template <class R> struct HostCase {
   bool live = false;
   int n = 0;
-  Range cells, slots, walls, terms, groups, gmembers, qcells, qlist;
+  Range cells, slots, walls, terms, groups, gmembers, qcells, qlist, faces;
   int slot = -1;
   std::vector<int> nslot, nterm;  // per-cell slot and gradient-term counts (for tiling)
   std::vector<int> slot_prefix, term_prefix;  // n+1 running sums of nslot / nterm
@@ -133,15 +133,17 @@ template <class R> class Batch final : public BatchBase {
     if (srd == 0) srd = cells / 8 + 64 * c.max_cases;
     cap_cells_ = cells + c.max_cases;  // one closing entry per case
     cap_slots_ = slots;
+    cap_faces_ = slots;  // every face is listed by at least one cell
     cap_walls_ = walls;
     cap_terms_ = std::max<long long>(terms, 1);
     cap_groups_ = srd;
     cap_gmem_ = 8 * srd;
     cap_q_ = 2 * srd;
     cap_qlist_ = 8 * srd;
-    cap_tiles_ = cap_cells_ / 16 + 4 * c.max_cases;
+    cap_tiles_ = cap_cells_ / 2 + 4 * c.max_cases;  // a tile holds at least one cell, normally 5-10
     a_cells_ = RangeAlloc(cap_cells_);
     a_slots_ = RangeAlloc(cap_slots_);
+    a_faces_ = RangeAlloc(cap_faces_);
     a_walls_ = RangeAlloc(cap_walls_);
     a_terms_ = RangeAlloc(cap_terms_);
     a_groups_ = RangeAlloc(cap_groups_ + c.max_cases);
@@ -178,6 +180,13 @@ template <class R> class Batch final : public BatchBase {
               diag_cfg_.alloc(7 * c.max_cases, A, error, "diag") && case_tiles_.alloc(2 * c.max_cases, A, error, "diag");
     if (!ok) return false;
     if (!s_geo_.alloc(6 * cap_slots_, A, error, "slots")) return false;
+    // face and wall records of the split launch mode
+    ok = s_item_.alloc(cap_slots_, A, error, "slots") && f_case_.alloc(cap_faces_, A, error, "faces") &&
+         f_own_.alloc(cap_faces_, A, error, "faces") && f_nb_.alloc(cap_faces_, A, error, "faces") &&
+         f_meta_.alloc(cap_faces_, A, error, "faces") && f_len_.alloc(cap_faces_, A, error, "faces") &&
+         f_geo_.alloc(6 * cap_faces_, A, error, "faces") && fval_.alloc(SM_COLS * cap_faces_, A, error, "faces") &&
+         w_owner_.alloc(cap_walls_, A, error, "walls") && wval_.alloc(SM_COLS * cap_walls_, A, error, "walls");
+    if (!ok) return false;
     if (model_ >= MODEL_LAMINAR) {
       ok = t_own_.alloc(cap_terms_, A, error, "terms") &&
            t_src_.alloc(cap_terms_, A, error, "terms") && t_x_.alloc(cap_terms_, A, error, "terms") &&
@@ -193,18 +202,25 @@ template <class R> class Batch final : public BatchBase {
     }
     cudaMemsetAsync(ctl_.p, 0, sizeof(CaseCtl) * c.max_cases, stream_);
     cudaMemsetAsync(c_case_.p, 0xff, sizeof(int) * nc, stream_);
+    cudaMemsetAsync(f_case_.p, 0xff, sizeof(int) * cap_faces_, stream_);
+    cudaMemsetAsync(w_owner_.p, 0xff, sizeof(int) * cap_walls_, stream_);
     if (!cuda_ok(cudaHostAlloc(reinterpret_cast<void**>(&h_ctl_), sizeof(CaseCtl) * c.max_cases, cudaHostAllocDefault), error,
                  "pinned control") ||
         !cuda_ok(cudaHostAlloc(reinterpret_cast<void**>(&h_bar_), sizeof(GridBarrier), cudaHostAllocDefault), error,
                  "pinned barrier"))
       return false;
     std::memset(h_ctl_, 0, sizeof(CaseCtl) * c.max_cases);
+    std::memset(h_bar_, 0, sizeof(GridBarrier));
+    cudaMemsetAsync(bar_.p, 0, sizeof(GridBarrier), stream_);
     stats_.pinned_bytes += sizeof(CaseCtl) * c.max_cases + sizeof(GridBarrier);
     block_ = c.block_threads > 0 ? c.block_threads : 256;
     if (block_ % 32 || block_ < 64 || block_ > MAX_BLOCK) return fail(error, "block_threads must be 64..256, a multiple of 32");
     grid_request_ = c.grid_blocks;
-    phases_ = c.launch_mode == AMR_B200_LAUNCH_PHASES;
-    if (phases_ && block_ != PHASE_BLOCK) return fail(error, "the phase launch mode runs 128-thread blocks");
+    if (c.launch_mode < AMR_B200_LAUNCH_AUTO || c.launch_mode > AMR_B200_LAUNCH_SPLIT)
+      return fail(error, "unknown launch mode");
+    mode_ = c.launch_mode == AMR_B200_LAUNCH_AUTO ? AMR_B200_LAUNCH_PERSISTENT : c.launch_mode;
+    if (mode_ != AMR_B200_LAUNCH_PERSISTENT && block_ != PHASE_BLOCK)
+      return fail(error, "the phase and split launch modes run 128-thread blocks");
     if (!configure_grid(error)) return false;
     return cuda_ok(cudaStreamSynchronize(stream_), error, "batch init");
   }
@@ -225,6 +241,7 @@ template <class R> class Batch final : public BatchBase {
     const long long nw = (long long)m->n_walls;
     const long long ns = (long long)m->face_offsets[n] + nw;  // face slots then wall slots, per cell
     const long long nt = model_ >= MODEL_LAMINAR ? (long long)m->visc_offsets[n] : 0;
+    const long long nf = (long long)m->n_faces;
     // SRD lists (only non-trivial neighbourhoods)
     std::vector<unsigned char> simple(n, 1);
     std::vector<int> group_index(n, -1);
@@ -261,8 +278,9 @@ template <class R> class Batch final : public BatchBase {
     hc.gmembers = {a_gmem_.alloc(gmem), gmem};
     hc.qcells = {a_q_.alloc(ng + 1), ng + 1};
     hc.qlist = {a_qlist_.alloc(qlist), qlist};
+    hc.faces = {a_faces_.alloc(nf), nf};
     if (hc.cells.b < 0 || hc.slots.b < 0 || hc.walls.b < 0 || hc.terms.b < 0 || hc.groups.b < 0 || hc.gmembers.b < 0 ||
-        hc.qcells.b < 0 || hc.qlist.b < 0) {
+        hc.qcells.b < 0 || hc.qlist.b < 0 || hc.faces.b < 0) {
       release_ranges(hc);
       return 3;
     }
@@ -302,6 +320,9 @@ template <class R> class Batch final : public BatchBase {
     std::vector<int> w_donor(nw, cb);
     std::vector<int> t_own(nt), t_src(nt);
     std::vector<R> t_x(nt), t_y(nt);
+    const int fb = (int)hc.faces.b;
+    std::vector<int> s_item(ns), f_case(nf, slot), f_own(nf), f_nb(nf), f_meta(nf), w_owner(nw);
+    std::vector<R> f_len(nf), f_geo(6 * nf, R(0));
     int kinds[4];
     for (int side = 0; side < 4; ++side) kinds[side] = m->boundaries[side].kind < 0 ? p->bc[side] : m->boundaries[side].kind;
     long long wpos = 0, spos = 0;
@@ -331,6 +352,7 @@ template <class R> class Batch final : public BatchBase {
         s_nb[spos] = other >= 0 ? cb + other : -1;
         s_meta[spos] = (own_left ? 1 : 0) | ((f.axis & 1) << 1) | ((side + 1) << 2) | ((kind & 15) << 5);
         s_len[spos] = (R)f.length;
+        s_item[spos] = fb + (int)fi;
         if (model_ >= MODEL_LAMINAR) {
           const amr_face_geometry_t& g = m->face_geometry[fi];
           s_geo[6 * spos + 0] = (R)g.dx;
@@ -355,6 +377,8 @@ template <class R> class Batch final : public BatchBase {
         s_nb[spos] = -1;
         s_meta[spos] = SLOT_WALL;
         s_len[spos] = (R)w.length;
+        s_item[spos] = wb + (int)wpos;
+        w_owner[wpos] = cb + (int)k;
         s_geo[6 * spos + 0] = (R)w.nx;
         s_geo[6 * spos + 1] = (R)w.ny;
         s_geo[6 * spos + 2] = R(1);
@@ -379,6 +403,30 @@ template <class R> class Batch final : public BatchBase {
         }
     }
     if (wpos != nw || spos != ns) return fail_release(hc, error, "wall count mismatch");
+    // face records in face orientation (left to right; a boundary face's inside cell is its owner)
+    for (long long fi = 0; fi < nf; ++fi) {
+      const amr_face_t& f = m->faces[fi];
+      const bool own_left = f.left >= 0;
+      const int own = own_left ? f.left : f.right;
+      const int other = own_left ? f.right : -1;
+      if (own < 0 || own >= (int)n || other >= (int)n || (other < 0) != (f.boundary >= 0) || f.boundary > 3)
+        return fail_release(hc, error, "face cells or boundary marker inconsistent");
+      const int side = f.boundary;
+      const int kind = side >= 0 ? kinds[side] : 0;
+      f_own[fi] = cb + own;
+      f_nb[fi] = other >= 0 ? cb + other : -1;
+      f_meta[fi] = (own_left ? 1 : 0) | ((f.axis & 1) << 1) | ((side + 1) << 2) | ((kind & 15) << 5);
+      f_len[fi] = (R)f.length;
+      if (model_ >= MODEL_LAMINAR) {
+        const amr_face_geometry_t& g = m->face_geometry[fi];
+        f_geo[6 * fi + 0] = (R)g.dx;
+        f_geo[6 * fi + 1] = (R)g.dy;
+        f_geo[6 * fi + 2] = (R)g.ex;
+        f_geo[6 * fi + 3] = (R)g.ey;
+        f_geo[6 * fi + 4] = (R)g.distance;
+        f_geo[6 * fi + 5] = (R)m->face_samples[fi].distance;
+      }
+    }
     c_slot[n] = sb + (int)ns;
     c_wall[n] = wb + (int)nw;
     c_term[n] = tb + (int)nt;
@@ -477,7 +525,10 @@ template <class R> class Batch final : public BatchBase {
               up(g_mem_.p + gb, g_mem, G) && up(g_cell_.p + gmb, g_cell, G) && up(g_cnt_.p + gmb, g_cnt, G) &&
               up(g_vol_.p + gb, g_vol, G) && up(q_cell_.p + qb, q_cell, G) && up(q_grp_.p + qb, q_grp, G) &&
               up(q_list_.p + qlb, q_list, G) && up(q_cnt_.p + qb, q_cnt, G);
-    ok = ok && up(s_geo_.p + 6 * (long long)sb, s_geo, G);
+    ok = ok && up(s_geo_.p + 6 * (long long)sb, s_geo, G) && up(s_item_.p + sb, s_item, G) &&
+         up(f_case_.p + fb, f_case, G) && up(f_own_.p + fb, f_own, G) && up(f_nb_.p + fb, f_nb, G) &&
+         up(f_meta_.p + fb, f_meta, G) && up(f_len_.p + fb, f_len, G) && up(f_geo_.p + 6 * (long long)fb, f_geo, G) &&
+         up(w_owner_.p + wb, w_owner, G);
     if (ok && model_ >= MODEL_LAMINAR)
       ok = up(t_own_.p + tb, t_own, G) && up(t_src_.p + tb, t_src, G) &&
            up(t_x_.p + tb, t_x, G) && up(t_y_.p + tb, t_y, G);
@@ -515,6 +566,8 @@ template <class R> class Batch final : public BatchBase {
     // the freed cell range no longer belongs to any case
     HostCase<R>& hc = cases_[slot];
     cudaMemsetAsync(c_case_.p + hc.cells.b, 0xff, sizeof(int) * hc.cells.n, stream_);
+    if (hc.faces.n) cudaMemsetAsync(f_case_.p + hc.faces.b, 0xff, sizeof(int) * hc.faces.n, stream_);
+    if (hc.walls.n) cudaMemsetAsync(w_owner_.p + hc.walls.b, 0xff, sizeof(int) * hc.walls.n, stream_);
     cudaStreamSynchronize(stream_);
     release_ranges(hc);
     hc = HostCase<R>();
@@ -571,7 +624,7 @@ template <class R> class Batch final : public BatchBase {
       cudaGetLastError();
     }
     if (!ok) return 1;
-    if (h_bar_->timeout) {
+    if (mode_ == AMR_B200_LAUNCH_PERSISTENT && h_bar_->timeout) {
       // a grid barrier gave up: mark every live case and report
       for (int i = 0; i < config_.max_cases; ++i)
         if (cases_[i].live && !h_ctl_[i].fatal) h_ctl_[i].fatal = STATUS_BARRIER_TIMEOUT;
@@ -589,7 +642,7 @@ template <class R> class Batch final : public BatchBase {
     if (!sync_tiles(error)) return 1;
     cudaGetLastError();
     if (!enqueue(1, MODE_RESIDUAL, error)) return 1;
-    launches_ += phases_ ? (model_ >= MODEL_LAMINAR ? 2 : 1) : 1;
+    launches_ += mode_ == AMR_B200_LAUNCH_PERSISTENT ? 1 : (model_ >= MODEL_LAMINAR ? 3 : 2) - (mode_ == AMR_B200_LAUNCH_PHASES);
     return cuda_ok(cudaStreamSynchronize(stream_), error, "residual") ? 0 : 1;
   }
 
@@ -629,8 +682,12 @@ template <class R> class Batch final : public BatchBase {
     graph_dirty_ = true;
   }
   std::string launch_config() const override {
-    return std::string(phases_ ? "mode=phases" : "mode=persistent") + " block=" + std::to_string(block_) +
-           " grid=" + std::to_string(phases_ ? n_tiles_ : grid_) + (use_graph_ ? " graph" : " direct");
+    const char* name = mode_ == AMR_B200_LAUNCH_PHASES ? "mode=phases" : mode_ == AMR_B200_LAUNCH_SPLIT ? "mode=split" : "mode=persistent";
+    const int grid = mode_ == AMR_B200_LAUNCH_PHASES  ? (n_tiles_ + block_ / 32 - 1) / (block_ / 32)
+                     : mode_ == AMR_B200_LAUNCH_SPLIT ? (int)((hw_cells_ + PHASE_BLOCK - 1) / PHASE_BLOCK)
+                                                      : grid_;
+    return std::string(name) + " block=" + std::to_string(block_) + " grid=" + std::to_string(grid) +
+           (use_graph_ ? " graph" : " direct");
   }
   int autotune(int trials, std::string* error) override;
   void restore(const std::vector<CaseCtl>& ctl_save, const DevBuf<R>& s0, const DevBuf<R>& s1, long long nbytes);
@@ -741,7 +798,7 @@ template <class R> class Batch final : public BatchBase {
   bool make_tiles(HostCase<R>& hc, std::string* why) {
     const long long n = hc.n;
     const int cb = (int)hc.cells.b;
-    const int B = block_;
+    const int B = TILE_W;
     hc.tiles.clear();
     long long k = 0;
     bool first = true;
@@ -755,7 +812,7 @@ template <class R> class Batch final : public BatchBase {
         terms += dt;
         ++k;
       }
-      if (k == start) return fail(why, "a cell has more faces or gradient terms than a thread block");
+      if (k == start) return fail(why, "a cell has more faces or gradient terms than a tile (32)");
       Tile t;
       t.cs = hc.slot;
       t.c0 = cb + (int)start;
@@ -792,7 +849,8 @@ template <class R> class Batch final : public BatchBase {
     a_gmem_.release(hc.gmembers.b, hc.gmembers.b >= 0 ? hc.gmembers.n : 0);
     a_q_.release(hc.qcells.b, hc.qcells.b >= 0 ? hc.qcells.n : 0);
     a_qlist_.release(hc.qlist.b, hc.qlist.b >= 0 ? hc.qlist.n : 0);
-    hc.cells = hc.slots = hc.walls = hc.terms = hc.groups = hc.gmembers = hc.qcells = hc.qlist = Range{0, 0};
+    a_faces_.release(hc.faces.b, hc.faces.b >= 0 ? hc.faces.n : 0);
+    hc.cells = hc.slots = hc.walls = hc.terms = hc.groups = hc.gmembers = hc.qcells = hc.qlist = hc.faces = Range{0, 0};
   }
 
   void refresh_meta(int slot) {
@@ -822,6 +880,13 @@ template <class R> class Batch final : public BatchBase {
       ranges[2 * i + 1] = (int)all.size();
     }
     n_tiles_ = (int)all.size();
+    hw_cells_ = hw_faces_ = hw_walls_ = 0;  // ends of the highest live ranges (split-mode grids)
+    for (auto& c : cases_)
+      if (c.live) {
+        hw_cells_ = std::max(hw_cells_, c.cells.b + c.cells.n);
+        hw_faces_ = std::max(hw_faces_, c.faces.b + c.faces.n);
+        hw_walls_ = std::max(hw_walls_, c.walls.b + c.walls.n);
+      }
     if (!all.empty() && !cuda_ok(cudaMemcpyAsync(tiles_.p, all.data(), sizeof(Tile) * all.size(), cudaMemcpyHostToDevice,
                                                  stream_), error, "tiles"))
       return false;
@@ -885,6 +950,19 @@ template <class R> class Batch final : public BatchBase {
     d.sdiff = sdiff_.p;
     d.ssrc = ssrc_.p;
     d.srate = srate_.p;
+    d.f_case = f_case_.p;
+    d.f_own = f_own_.p;
+    d.f_nb = f_nb_.p;
+    d.f_meta = f_meta_.p;
+    d.f_len = f_len_.p;
+    d.f_geo = f_geo_.p;
+    d.w_owner = w_owner_.p;
+    d.s_item = s_item_.p;
+    d.fval = fval_.p;
+    d.wval = wval_.p;
+    d.n_faces = (int)hw_faces_;
+    d.n_walls = (int)hw_walls_;
+    d.n_cells = (int)hw_cells_;
     d.ncap = cap_cells_;
     d.gcap = cap_groups_ + config_.max_cases;
     d.bar = bar_.p;
@@ -893,8 +971,11 @@ template <class R> class Batch final : public BatchBase {
   }
 
   uint64_t kernels_per_advance(int trials) const {
-    if (!phases_) return 1;
-    const uint64_t per_trial = 1 + 1 + 1 + 2 + (model_ >= MODEL_LAMINAR ? 3 : 0) + (any_srd() ? 3 : 0) + 1;
+    if (mode_ == AMR_B200_LAUNCH_PERSISTENT) return 1;
+    // per trial: three flux stages (one kernel, or item + gather), gradients per stage, the
+    // first update, SRD after each stage and the commit; plus the opening commit
+    const uint64_t flux = mode_ == AMR_B200_LAUNCH_SPLIT ? 2 : 1;
+    const uint64_t per_trial = 3 * flux + (model_ >= MODEL_LAMINAR ? 3 : 0) + 1 + (any_srd() ? 3 : 0) + 1;
     return 1 + per_trial * trials;
   }
 
@@ -922,11 +1003,14 @@ template <class R> class Batch final : public BatchBase {
   bool enqueue(int trials, int mode, std::string* error, bool events = true) {
     bool ok = true;
     if (events) ok = cuda_ok(cudaEventRecord(ev0_, stream_), error, "event");
-    if (phases_) {
+    if (mode_ == AMR_B200_LAUNCH_PHASES) {
       ok = ok && cuda_ok(EngineOps<R>::launch_phases(dev(), model_, flux_, any_srd(), trials, mode, block_, stream_), error,
                          "phase kernel launch");
+    } else if (mode_ == AMR_B200_LAUNCH_SPLIT) {
+      ok = ok && cuda_ok(EngineOps<R>::launch_split(dev(), model_, flux_, any_srd(), trials, mode, stream_), error,
+                         "split kernel launch");
     } else {
-      const int grid = mode == MODE_RESIDUAL ? std::min(grid_, std::max(1, n_tiles_)) : grid_;
+      const int grid = mode == MODE_RESIDUAL ? std::min(grid_, std::max(1, (n_tiles_ + block_ / 32 - 1) / (block_ / 32))) : grid_;
       ok = ok && cuda_ok(cudaMemsetAsync(bar_.p, 0, sizeof(GridBarrier), stream_), error, "barrier reset") &&
            cuda_ok(EngineOps<R>::launch(dev(), model_, flux_, any_srd(), trials, mode, grid, block_, stream_, true), error,
                    "trial kernel launch");
@@ -934,8 +1018,9 @@ template <class R> class Batch final : public BatchBase {
     if (events) ok = ok && cuda_ok(cudaEventRecord(ev1_, stream_), error, "event");
     if (ok && mode == MODE_TRIALS)
       ok = cuda_ok(cudaMemcpyAsync(h_ctl_, ctl_.p, sizeof(CaseCtl) * config_.max_cases, cudaMemcpyDeviceToHost, stream_),
-                   error, "control read-back") &&
-           cuda_ok(cudaMemcpyAsync(h_bar_, bar_.p, sizeof(GridBarrier), cudaMemcpyDeviceToHost, stream_), error,
+                   error, "control read-back");
+    if (ok && mode == MODE_TRIALS && mode_ == AMR_B200_LAUNCH_PERSISTENT)
+      ok = cuda_ok(cudaMemcpyAsync(h_bar_, bar_.p, sizeof(GridBarrier), cudaMemcpyDeviceToHost, stream_), error,
                    "barrier read-back");
     return ok;
   }
@@ -992,7 +1077,9 @@ template <class R> class Batch final : public BatchBase {
     ctl_.free(); cfg_.free(); tiles_.free(); bar_.free();
     c_case_.free(); c_vol_.free(); c_area_.free(); c_gvol_.free(); c_flags_.free(); c_slot_.free(); c_wall_.free();
     c_term_.free(); c_cx_.free(); c_cy_.free(); c_wd_.free();
-    s_own_.free(); s_nb_.free(); s_meta_.free(); s_len_.free(); s_geo_.free();
+    s_own_.free(); s_nb_.free(); s_meta_.free(); s_len_.free(); s_geo_.free(); s_item_.free();
+    f_case_.free(); f_own_.free(); f_nb_.free(); f_meta_.free(); f_len_.free(); f_geo_.free(); fval_.free();
+    w_owner_.free(); wval_.free();
     w_nx_.free(); w_ny_.free(); w_len_.free(); w_dist_.free(); w_donor_.free(); w_xm_.free(); w_ym_.free();
     t_own_.free(); t_src_.free(); t_x_.free(); t_y_.free();
     g_mem_.free(); g_cell_.free(); g_cnt_.free(); g_vol_.free(); q_cell_.free(); q_grp_.free(); q_list_.free(); q_cnt_.free();
@@ -1004,7 +1091,10 @@ template <class R> class Batch final : public BatchBase {
   amr_batch_config_t config_{};
   int model_ = 0, flux_ = 0, nv_ = 4, sms_ = 148, clock_khz_ = 1965000;
   int block_ = 256, grid_ = 0, max_grid_ = 0, grid_request_ = 0;
-  bool phases_ = false;  // launch mode: persistent cooperative kernel, or one kernel per phase
+  int mode_ = AMR_B200_LAUNCH_PERSISTENT;  // persistent cooperative kernel, one kernel per phase, or split
+  long long hw_cells_ = 0, hw_faces_ = 0, hw_walls_ = 0;
+  long long cap_faces_ = 0;
+  RangeAlloc a_faces_;
   long long cap_cells_ = 0, cap_slots_ = 0, cap_walls_ = 0, cap_terms_ = 0, cap_groups_ = 0, cap_gmem_ = 0, cap_q_ = 0,
             cap_qlist_ = 0, cap_tiles_ = 0;
   RangeAlloc a_cells_, a_slots_, a_walls_, a_terms_, a_groups_, a_gmem_, a_q_, a_qlist_;
@@ -1031,8 +1121,10 @@ template <class R> class Batch final : public BatchBase {
   DevBuf<double> c_vol_, c_area_, c_gvol_, c_cx_, c_cy_;
   DevBuf<unsigned char> c_flags_;
   DevBuf<R> c_wd_;
-  DevBuf<int> s_own_, s_nb_, s_meta_;
+  DevBuf<int> s_own_, s_nb_, s_meta_, s_item_;
   DevBuf<R> s_len_, s_geo_;
+  DevBuf<int> f_case_, f_own_, f_nb_, f_meta_, w_owner_;
+  DevBuf<R> f_len_, f_geo_, fval_, wval_;
   DevBuf<R> w_nx_, w_ny_, w_len_, w_dist_;
   DevBuf<double> w_xm_, w_ym_;
   DevBuf<int> w_donor_;

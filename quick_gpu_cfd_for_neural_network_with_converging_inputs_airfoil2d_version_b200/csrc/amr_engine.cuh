@@ -62,6 +62,11 @@ struct Tile {
   int cs, c0, c1, leader, s0, s1, t0, t1;
 };
 constexpr int SLOT_WALL = 1 << 9;  // s_meta flag: the slot is a wall fragment of its owner cell
+// A tile is processed by one warp: at most TILE_W slots and TILE_W gradient terms of whole cells,
+// synchronised by __syncwarp only, so the warps of a block never wait for one another.
+constexpr int TILE_W = 32;
+constexpr int SM_COLS = 12;  // shared-memory columns per slot
+constexpr unsigned FULL_MASK = 0xffffffffu;
 
 struct GridBarrier {
   unsigned int count, gen;
@@ -126,6 +131,18 @@ template <class R> struct Dev {
   R* srate;
   long long ncap;
   long long gcap;
+  // split mode: one record per face and per wall, and the slot -> record map
+  const int* f_case;
+  const int* f_own;
+  const int* f_nb;
+  const int* f_meta;
+  const R* f_len;
+  const R* f_geo;   // 6 per face
+  const int* w_owner;
+  const int* s_item;
+  R* fval;          // 12 per face
+  R* wval;          // 12 per wall
+  int n_faces, n_walls, n_cells;  // ends of the live face, wall and cell ranges
   GridBarrier* bar;
   unsigned long long barrier_cycles;
 };
@@ -220,81 +237,92 @@ template <class R> struct Smem {
 // G phase: velocity gradients, viscosity, eddy viscosity, SA gradients and point model of
 // every cell of a tile (reference src/static_amr2d_viscous.cpp:166-174, src/static_amr2d_sa.cpp:74-80).
 // ------------------------------------------------------------------------------------------
+// Cell part of the G phase from the summed LSQ contributions gr (velocity) and sg (SA phi and
+// density): viscosity, eddy viscosity, SA point model and source.  Returns false on failure.
+template <class R, int MODEL>
+__device__ __forceinline__ bool grad_finish(const Dev<R>& d, const CaseCfg<R>& cf, int k, const R* Uin, const R* gr,
+                                            const R* sg) {
+  const long long n = d.ncap;
+  const Prim<R> w = prim(Uin, n, k, cf.gamma);
+  const R mu = dyn_visc(cf.trn, w.p / (w.rho * cf.trn.gas_constant));
+  bool bad = !(mu > R(0)) || !isfinite(mu);
+  for (int v = 0; v < 4; ++v) d.grad[v * n + k] = gr[v];
+  d.mu[k] = mu;
+  R eddy = 0;
+  if (MODEL == MODEL_SA) {
+    const R ph = Uin[4 * n + k] / w.rho;
+    if (!isfinite(ph)) bad = true;
+    eddy = w.rho * sa_eddy(ph, mu / w.rho);
+    const SaPoint<R> pt = sa_neg(ph, mu / w.rho, d.c_wd[k], R(fabs(gr[2] - gr[1])));
+    const R src = sa_corrected_source(pt, w.rho, sg[0], sg[1], sg[2], sg[3]);
+    d.sgrad[k] = sg[0];
+    d.sgrad[n + k] = sg[1];
+    d.sdiff[k] = pt.diffusion;
+    d.ssrc[k] = src;
+    d.srate[k] = pt.source_rate;
+    if (!(pt.diffusion > R(0)) || !isfinite(src) || !isfinite(pt.source_rate)) bad = true;
+  }
+  d.eddy[k] = eddy;
+  return !bad;
+}
+
+// LSQ contribution of one gradient term of cell k (reference src/static_amr2d_viscous.cpp:170-173,
+// src/static_amr2d_sa.cpp:75-76): c[0..3] velocity, c[4..7] SA phi and density.
+template <class R, int MODEL>
+__device__ __forceinline__ void term_values(const Dev<R>& d, const CaseCfg<R>& cf, int q, int k, const R* Uin, R* c) {
+  const long long n = d.ncap;
+  const int src = __ldg(d.t_src + q);
+  const R x = __ldg(d.t_x + q), y = __ldg(d.t_y + q);
+  const R rk = Uin[k], uk = Uin[n + k] / rk, vk = Uin[2 * n + k] / rk;
+  R uu = 0, vv = 0;
+  if (src >= 0) {
+    const R rs = Uin[src];
+    uu = Uin[n + src] / rs;
+    vv = Uin[2 * n + src] / rs;
+  } else if (src <= -2) {
+    uu = cf.bnd[-2 - src].wall_velocity[0];
+    vv = cf.bnd[-2 - src].wall_velocity[1];
+  }
+  const R du = uu - uk, dv = vv - vk;
+  c[0] = x * du;
+  c[1] = y * du;
+  c[2] = x * dv;
+  c[3] = y * dv;
+  if (MODEL == MODEL_SA) {
+    const R phk = Uin[4 * n + k] / rk;
+    const R ph = src >= 0 ? Uin[4 * n + src] / Uin[src] : R(0);
+    const R rho = src >= 0 ? Uin[src] : rk;
+    c[4] = x * (ph - phk);
+    c[5] = y * (ph - phk);
+    c[6] = x * (rho - rk);
+    c[7] = y * (rho - rk);
+  }
+}
+
 template <class R, int MODEL>
 __device__ void phase_gradients(const Dev<R>& d, const Tile& t, const R* Uin, R* sm) {
-  const int B = blockDim.x, i = threadIdx.x;
-  const long long n = d.ncap;
+  const int B = TILE_W, i = threadIdx.x & 31;
   const CaseCfg<R>& cf = d.cfg[t.cs];
-  const R g = cf.gamma;
   const int t0 = t.t0, t1 = t.t1;
   if (i < t1 - t0) {
-    const int q = t0 + i, k = __ldg(d.t_own + q), src = __ldg(d.t_src + q);
-    const R x = __ldg(d.t_x + q), y = __ldg(d.t_y + q);
-    const R rk = Uin[k], uk = Uin[n + k] / rk, vk = Uin[2 * n + k] / rk;
-    R uu = 0, vv = 0;
-    if (src >= 0) {
-      const R rs = Uin[src];
-      uu = Uin[n + src] / rs;
-      vv = Uin[2 * n + src] / rs;
-    } else if (src <= -2) {
-      uu = cf.bnd[-2 - src].wall_velocity[0];
-      vv = cf.bnd[-2 - src].wall_velocity[1];
-    }
-    const R du = uu - uk, dv = vv - vk;
-    sm[0 * B + i] = x * du;
-    sm[1 * B + i] = y * du;
-    sm[2 * B + i] = x * dv;
-    sm[3 * B + i] = y * dv;
-    if (MODEL == MODEL_SA) {
-      const R phk = Uin[4 * n + k] / rk;
-      const R ph = src >= 0 ? Uin[4 * n + src] / Uin[src] : R(0);
-      const R rho = src >= 0 ? Uin[src] : rk;
-      sm[4 * B + i] = x * (ph - phk);
-      sm[5 * B + i] = y * (ph - phk);
-      sm[6 * B + i] = x * (rho - rk);
-      sm[7 * B + i] = y * (rho - rk);
-    }
+    const int q = t0 + i;
+    R c[8];
+    term_values<R, MODEL>(d, cf, q, __ldg(d.t_own + q), Uin, c);
+    for (int v = 0; v < (MODEL == MODEL_SA ? 8 : 4); ++v) sm[v * B + i] = c[v];
   }
-  __syncthreads();
+  __syncwarp();
   if (i < t.c1 - t.c0) {
     const int k = t.c0 + i;
-    const Prim<R> w = prim(Uin, n, k, g);
-    const R mu = dyn_visc(cf.trn, w.p / (w.rho * cf.trn.gas_constant));
-    bool bad = !(mu > R(0)) || !isfinite(mu);
     R gr[4] = {0, 0, 0, 0}, sg[4] = {0, 0, 0, 0};
     const int a = d.c_term[k] - t0, b = d.c_term[k + 1] - t0;
-    for (int q = a; q < b; ++q) {
-      gr[0] += sm[0 * B + q];
-      gr[1] += sm[1 * B + q];
-      gr[2] += sm[2 * B + q];
-      gr[3] += sm[3 * B + q];
-    }
-    for (int v = 0; v < 4; ++v) d.grad[v * n + k] = gr[v];
-    d.mu[k] = mu;
-    R eddy = 0;
-    if (MODEL == MODEL_SA) {
-      const R ph = Uin[4 * n + k] / w.rho;
-      if (!isfinite(ph)) bad = true;
-      eddy = w.rho * sa_eddy(ph, mu / w.rho);
-      for (int q = a; q < b; ++q) {
-        sg[0] += sm[4 * B + q];
-        sg[1] += sm[5 * B + q];
-        sg[2] += sm[6 * B + q];
-        sg[3] += sm[7 * B + q];
-      }
-      const SaPoint<R> pt = sa_neg(ph, mu / w.rho, d.c_wd[k], R(fabs(gr[2] - gr[1])));
-      const R src = sa_corrected_source(pt, w.rho, sg[0], sg[1], sg[2], sg[3]);
-      d.sgrad[k] = sg[0];
-      d.sgrad[n + k] = sg[1];
-      d.sdiff[k] = pt.diffusion;
-      d.ssrc[k] = src;
-      d.srate[k] = pt.source_rate;
-      if (!(pt.diffusion > R(0)) || !isfinite(src) || !isfinite(pt.source_rate)) bad = true;
-    }
-    d.eddy[k] = eddy;
-    if (bad) atomicOr(&d.ctl[t.cs].bad, 1);
+    for (int q = a; q < b; ++q)
+      for (int v = 0; v < 4; ++v) gr[v] += sm[v * B + q];
+    if (MODEL == MODEL_SA)
+      for (int q = a; q < b; ++q)
+        for (int v = 0; v < 4; ++v) sg[v] += sm[(4 + v) * B + q];
+    if (!grad_finish<R, MODEL>(d, cf, k, Uin, gr, sg)) atomicOr(&d.ctl[t.cs].bad, 1);
   }
-  __syncthreads();
+  __syncwarp();
 }
 
 // ------------------------------------------------------------------------------------------
@@ -302,9 +330,14 @@ __device__ void phase_gradients(const Dev<R>& d, const Tile& t, const R* Uin, R*
 // residual, cell dt and the stage update (reference src/static_amr2d.cpp:163-204,
 // src/static_amr2d_viscous.cpp:177-206, src/static_amr2d_sa.cpp:81-96, 395-426).
 // ------------------------------------------------------------------------------------------
+// Fluxes of one face seen from cell k (nb: the other cell, -1 outside).  Writes the 12 values
+// dst[c*stride]: conserved flux (4), viscous flux (4), speed*length, viscous spectral coefficient,
+// SA flux, SA spectral coefficient.  With signed = true the flux columns carry the orientation
+// sign of cell k (slot form); otherwise they are in face orientation (item form).
 template <class R, int MODEL, int FLUX>
-__device__ __forceinline__ void slot_face(const Dev<R>& d, const CaseCfg<R>& cf, int s, int k, int nb, int meta,
-                                          const R* Uin, bool base, R* sm, int B, int i, bool& bad) {
+__device__ __forceinline__ void slot_face(const Dev<R>& d, const CaseCfg<R>& cf, const R* gp, R len, int k, int nb,
+                                          int meta, const R* Uin, bool base, R* dst, int stride, bool signed_out,
+                                          bool& bad) {
   const long long n = d.ncap;
   const R g = cf.gamma;
   const bool own_left = meta & 1;
@@ -312,7 +345,6 @@ __device__ __forceinline__ void slot_face(const Dev<R>& d, const CaseCfg<R>& cf,
   // Every load of this slot is issued up front and unconditionally (an exterior face reads its
   // own cell twice), so the whole neighbourhood arrives in one memory round trip.
   const int m = nb >= 0 ? nb : k;
-  const R len = __ldg(d.s_len + s);
   R uk[5], um[5];
   for (int v = 0; v < 4; ++v) { uk[v] = Uin[v * n + k]; um[v] = Uin[v * n + m]; }
   if (MODEL == MODEL_SA) { uk[4] = Uin[4 * n + k]; um[4] = Uin[4 * n + m]; }
@@ -320,7 +352,6 @@ __device__ __forceinline__ void slot_face(const Dev<R>& d, const CaseCfg<R>& cf,
   if (MODEL >= MODEL_LAMINAR) {
     for (int v = 0; v < 4; ++v) { gk[v] = d.grad[v * n + k]; gm[v] = d.grad[v * n + m]; }
     mk = d.mu[k]; mm = d.mu[m]; ek = d.eddy[k]; em = d.eddy[m];
-    const R* gp = d.s_geo + 6 * (long long)s;
     for (int v = 0; v < 6; ++v) geo[v] = __ldg(gp + v);
     if (MODEL == MODEL_SA) {
       sgk[0] = d.sgrad[k]; sgk[1] = d.sgrad[n + k]; sgm[0] = d.sgrad[m]; sgm[1] = d.sgrad[n + m];
@@ -354,14 +385,14 @@ __device__ __forceinline__ void slot_face(const Dev<R>& d, const CaseCfg<R>& cf,
   // conserved components: normal momentum goes to 1+axis, tangential to 2-axis
   const R f0 = F[0] * len, fn = F[1] * len, ft = F[2] * len, f3 = F[3] * len;
   for (int v = 0; v < 4; ++v) if (!isfinite(F[v])) bad = true;
-  const R sg = own_left ? R(1) : R(-1);
-  sm[0 * B + i] = sg * f0;
-  sm[1 * B + i] = sg * (axis ? ft : fn);
-  sm[2 * B + i] = sg * (axis ? fn : ft);
-  sm[3 * B + i] = sg * f3;
+  const R sg = signed_out ? (own_left ? R(1) : R(-1)) : R(1);
+  dst[0 * stride] = sg * f0;
+  dst[1 * stride] = sg * (axis ? ft : fn);
+  dst[2 * stride] = sg * (axis ? fn : ft);
+  dst[3 * stride] = sg * f3;
   if (base) {
     const R speed = rmax(R(fabs(an)) + sqrt(g * a[3] / a[0]), R(fabs(bn)) + sqrt(g * b[3] / b[0]));
-    sm[8 * B + i] = speed * len;
+    dst[8 * stride] = speed * len;
   }
   if (MODEL >= MODEL_LAMINAR) {
     R gv[4], mu, uf, vf, nu, distance;
@@ -405,9 +436,9 @@ __device__ __forceinline__ void slot_face(const Dev<R>& d, const CaseCfg<R>& cf,
     visc_flux(mu, gv, axis == 0 ? R(1) : R(0), axis == 1 ? R(1) : R(0), uf, vf, fv);
     for (int v = 0; v < 4; ++v) {
       if (!isfinite(fv[v])) bad = true;
-      sm[(4 + v) * B + i] = sg * (fv[v] * len);
+      dst[(4 + v) * stride] = sg * (fv[v] * len);
     }
-    if (base) sm[9 * B + i] = R(4.0 / 3) * nu / distance * len;
+    if (base) dst[9 * stride] = R(4.0 / 3) * nu / distance * len;
     if (MODEL == MODEL_SA) {
       const R mass = f0 - fv[0] * len;
       const R phk = uk[4] / wk.rho;
@@ -434,8 +465,8 @@ __device__ __forceinline__ void slot_face(const Dev<R>& d, const CaseCfg<R>& cf,
           fc = coefficient / distance * len;
         }
       }
-      sm[10 * B + i] = sg * (mass * (mass >= R(0) ? left : right) - diff);
-      if (base) sm[11 * B + i] = fc;
+      dst[10 * stride] = sg * (mass * (mass >= R(0) ? left : right) - diff);
+      if (base) dst[11 * stride] = fc;
     }
   }
 }
@@ -444,21 +475,17 @@ __device__ __forceinline__ void slot_face(const Dev<R>& d, const CaseCfg<R>& cf,
 // flux from the visible donor (src/static_amr2d_viscous.cpp:192-196) and the SA wall flux
 // (src/static_amr2d_sa.cpp:91), with their spectral-radius contributions.
 template <class R, int MODEL>
-__device__ __forceinline__ void slot_wall(const Dev<R>& d, const CaseCfg<R>& cf, int s, int k, int dn,
-                                          const R* Uin, bool base, R* sm, int B, int i, bool& bad) {
+__device__ __forceinline__ void slot_wall(const Dev<R>& d, const CaseCfg<R>& cf, R nx, R ny, R wdist, R wl, int k, int dn,
+                                          const R* Uin, bool base, R* dst, int stride, bool& bad) {
   const long long n = d.ncap;
   const R g = cf.gamma;
-  const R wl = __ldg(d.s_len + s);
-  const R* geo = d.s_geo + 6 * (long long)s;
-  const R nx = __ldg(geo + 0), ny = __ldg(geo + 1);
   const Prim<R> wk = prim(Uin, n, k, g);
-  sm[0 * B + i] = 0;
-  sm[1 * B + i] = wk.p * nx * wl;
-  sm[2 * B + i] = wk.p * ny * wl;
-  sm[3 * B + i] = 0;
-  if (base) sm[8 * B + i] = sqrt(g * wk.p / wk.rho) * wl;
+  dst[0 * stride] = 0;
+  dst[1 * stride] = wk.p * nx * wl;
+  dst[2 * stride] = wk.p * ny * wl;
+  dst[3 * stride] = 0;
+  if (base) dst[8 * stride] = sqrt(g * wk.p / wk.rho) * wl;
   if (MODEL >= MODEL_LAMINAR) {
-    const R wdist = __ldg(geo + 2);
     const R rd = Uin[dn], ud = Uin[n + dn] / rd, vd = Uin[2 * n + dn] / rd;
     const R md = d.mu[dn];
     R gw[4], fw[4];
@@ -466,126 +493,139 @@ __device__ __forceinline__ void slot_wall(const Dev<R>& d, const CaseCfg<R>& cf,
     visc_flux(md, gw, nx, ny, R(0), R(0), fw);
     for (int v = 0; v < 4; ++v) {
       if (!isfinite(fw[v])) bad = true;
-      sm[(4 + v) * B + i] = fw[v] * wl;
+      dst[(4 + v) * stride] = fw[v] * wl;
     }
-    if (base) sm[9 * B + i] = R(4.0 / 3) * rmax(md / rd, d.mu[k] / wk.rho) / wdist * wl;
+    if (base) dst[9 * stride] = R(4.0 / 3) * rmax(md / rd, d.mu[k] / wk.rho) / wdist * wl;
     if (MODEL == MODEL_SA) {
       const R swc = md / R(AMRB_SIG) / wdist * wl;
-      sm[10 * B + i] = -swc * (Uin[4 * n + dn] / rd);
-      if (base) sm[11 * B + i] = swc;
+      dst[10 * stride] = -swc * (Uin[4 * n + dn] / rd);
+      if (base) dst[11 * stride] = swc;
     }
   }
 }
 
+// Per-cell end of the F phase: in-order sums of the cell's slot values (faces [a, e) in CSR order,
+// then walls [e, b)), residual, cell dt (base stage) and the stage update.  get(q, col) yields
+// the 12 values of slot q with the flux columns signed for cell k.  Returns the cell dt.
+template <class R, int MODEL, class Get>
+__device__ __forceinline__ double finish_cell(const Dev<R>& d, const CaseCfg<R>& cf, int cs, int k, int stage, int a,
+                                              int e, int b, const Get& get, const R* Uin, R* Ub, R* Un, bool& bad) {
+  const long long n = d.ncap;
+  const R g = cf.gamma;
+  const bool base = stage == STAGE_BASE;
+  double cell_dt = __longlong_as_double(0x7FF0000000000000ll);
+  const double V = d.c_vol[k];
+  const Prim<R> wk = prim(Uin, n, k, g);
+  if (!prim_ok(Uin, n, k, wk)) bad = true;
+  R sum[4] = {0, 0, 0, 0}, vs[4] = {0, 0, 0, 0}, spectral = 0, vspec = 0, snet = 0, sspec = 0;
+  for (int q = a; q < b; ++q) {
+    const bool wall = q >= e;
+    R col[SM_COLS];
+    get(q, wall, col);
+    if (!wall) {
+      for (int v = 0; v < 4; ++v) sum[v] += col[v];
+    } else {
+      sum[1] += col[1];
+      sum[2] += col[2];
+    }
+    if (base) spectral += col[8];
+    if (MODEL >= MODEL_LAMINAR) {
+      for (int v = 0; v < 4; ++v) vs[v] += col[4 + v];
+      if (base) vspec += col[9];
+    }
+    if (MODEL == MODEL_SA) {
+      if (!wall) snet += col[10]; else snet -= col[10];
+      if (base) sspec += col[11];
+    }
+  }
+  R res[5];
+  for (int v = 0; v < 4; ++v) res[v] = (R)(-sum[v] / V);
+  if (MODEL >= MODEL_LAMINAR) {
+    for (int v = 0; v < 4; ++v) res[v] += (R)(vs[v] / V);
+    if (MODEL == MODEL_SA) {
+      res[4] = (R)(-snet / V) + d.ssrc[k];
+      if (!isfinite(res[4])) bad = true;
+    }
+  }
+  const int nv = MODEL == MODEL_SA ? 5 : 4;
+  if (base) {
+    if (spectral > R(0)) cell_dt = cf.cfl * d.c_area[k] / (double)spectral;
+    if (MODEL >= MODEL_LAMINAR) {
+      const double vdt = vspec > R(0) ? cf.viscous_cfl * V / (double)vspec : __longlong_as_double(0x7FF0000000000000ll);
+      double sdt = __longlong_as_double(0x7FF0000000000000ll);
+      if (MODEL == MODEL_SA) {
+        const double rate = 2 * (double)sspec / ((double)wk.rho * V) + (double)d.srate[k];
+        sdt = rate > 0 ? cf.sa_cfl / rate : sdt;
+      }
+      cell_dt = rmin(cell_dt, rmin(vdt, sdt));
+    }
+    for (int v = 0; v < nv; ++v) d.R0[v * n + k] = res[v];
+  } else if (stage == STAGE_DIAG) {
+    for (int v = 0; v < nv; ++v) d.R0[v * n + k] = res[v];
+  } else {
+    const R dt = (R)d.ctl[cs].dt_trial;
+    const bool simple = cf.has_srd && (d.c_flags[k] & 1);
+    const bool check = stage == STAGE_2 && (!cf.has_srd || simple);
+    R out[5];
+    for (int v = 0; v < nv; ++v) {
+      if (stage == STAGE_1)
+        out[v] = R(0.75) * Ub[v * n + k] + R(0.25) * (Uin[v * n + k] + dt * res[v]);
+      else
+        out[v] = Ub[v * n + k] / R(3) + R(2.0 / 3) * (Uin[v * n + k] + dt * res[v]);
+    }
+    if (simple)
+      for (int v = 0; v < 4; ++v) out[v] = srd_self(out[v], V, d.c_gvol[k]);
+    R* dst = stage == STAGE_1 ? d.U2 : Un;
+    for (int v = 0; v < nv; ++v) dst[v * n + k] = out[v];
+    if (check) {
+      const R rho = out[0], mx = out[1], my = out[2], e = out[3];
+      const R vx = mx / rho, vy = my / rho, p = (g - R(1)) * (e - R(0.5) * (mx * vx + my * vy));
+      if (!isfinite(rho) || !(rho > R(0)) || !isfinite(mx) || !isfinite(my) || !isfinite(e) || !isfinite(p) || !(p > R(0)))
+        bad = true;
+      if (MODEL == MODEL_SA && !isfinite(out[4])) bad = true;
+    }
+  }
+  return cell_dt;
+}
+
+template <class R> struct SmemSlots {
+  const R* sm;
+  __device__ __forceinline__ void operator()(int q, bool, R* col) const {
+    for (int c = 0; c < SM_COLS; ++c) col[c] = sm[c * TILE_W + q];
+  }
+};
+
 template <class R, int MODEL, int FLUX>
 __device__ void phase_flux(const Dev<R>& d, const Tile& t, int stage, const R* Uin, R* Ub, R* Un, R* sm,
-                           bool* tile_bad, double* tile_dt) {
-  const int B = blockDim.x, i = threadIdx.x;
-  const long long n = d.ncap;
+                           bool* warp_bad, double* warp_dt) {
+  const int B = TILE_W, i = threadIdx.x & 31;
   const CaseCfg<R>& cf = d.cfg[t.cs];
-  const R g = cf.gamma;
   const int s0 = t.s0, s1 = t.s1;
   const bool base = stage == STAGE_BASE;
   bool bad = false;
   if (i < s1 - s0) {
     const int s = s0 + i;
     const int k = __ldg(d.s_own + s), nb = __ldg(d.s_nb + s), meta = __ldg(d.s_meta + s);
+    const R* gp = d.s_geo + 6 * (long long)s;
+    const R len = __ldg(d.s_len + s);
     if (meta & SLOT_WALL)
-      slot_wall<R, MODEL>(d, cf, s, k, nb, Uin, base, sm, B, i, bad);
+      slot_wall<R, MODEL>(d, cf, __ldg(gp + 0), __ldg(gp + 1), __ldg(gp + 2), len, k, nb, Uin, base, sm + i, B, bad);
     else
-      slot_face<R, MODEL, FLUX>(d, cf, s, k, nb, meta, Uin, base, sm, B, i, bad);
+      slot_face<R, MODEL, FLUX>(d, cf, gp, len, k, nb, meta, Uin, base, sm + i, B, true, bad);
   }
-  __syncthreads();
+  __syncwarp();
   double cell_dt = __longlong_as_double(0x7FF0000000000000ll);
   if (i < t.c1 - t.c0) {
     const int k = t.c0 + i;
-    const double V = d.c_vol[k];
-    const Prim<R> wk = prim(Uin, n, k, g);
-    if (!prim_ok(Uin, n, k, wk)) bad = true;
-    // slots of cell k: faces [a, e) in CSR order, then walls [e, b)
     const int a = d.c_slot[k] - s0, b = d.c_slot[k + 1] - s0;
     const int e = b - (d.c_wall[k + 1] - d.c_wall[k]);
-    R sum[4] = {0, 0, 0, 0};
-    for (int q = a; q < e; ++q)
-      for (int v = 0; v < 4; ++v) sum[v] += sm[v * B + q];
-    for (int q = e; q < b; ++q) {
-      sum[1] += sm[1 * B + q];
-      sum[2] += sm[2 * B + q];
-    }
-    R res[5];
-    for (int v = 0; v < 4; ++v) res[v] = (R)(-sum[v] / V);
-    R vspec = 0, sspec = 0;
-    if (MODEL >= MODEL_LAMINAR) {
-      R vs[4] = {0, 0, 0, 0};
-      for (int q = a; q < b; ++q) {
-        for (int v = 0; v < 4; ++v) vs[v] += sm[(4 + v) * B + q];
-        if (base) vspec += sm[9 * B + q];
-      }
-      for (int v = 0; v < 4; ++v) res[v] += (R)(vs[v] / V);
-      if (MODEL == MODEL_SA) {
-        R snet = 0;
-        for (int q = a; q < e; ++q) {
-          snet += sm[10 * B + q];
-          if (base) sspec += sm[11 * B + q];
-        }
-        for (int q = e; q < b; ++q) {
-          snet -= sm[10 * B + q];
-          if (base) sspec += sm[11 * B + q];
-        }
-        res[4] = (R)(-snet / V) + d.ssrc[k];
-        if (!isfinite(res[4])) bad = true;
-      }
-    }
-    const int nv = MODEL == MODEL_SA ? 5 : 4;
-    if (base) {
-      R spectral = 0;
-      for (int q = a; q < b; ++q) spectral += sm[8 * B + q];
-      if (spectral > R(0)) cell_dt = cf.cfl * d.c_area[k] / (double)spectral;
-      if (MODEL >= MODEL_LAMINAR) {
-        const double vdt = vspec > R(0) ? cf.viscous_cfl * V / (double)vspec : __longlong_as_double(0x7FF0000000000000ll);
-        double sdt = __longlong_as_double(0x7FF0000000000000ll);
-        if (MODEL == MODEL_SA) {
-          const double rate = 2 * (double)sspec / ((double)wk.rho * V) + (double)d.srate[k];
-          sdt = rate > 0 ? cf.sa_cfl / rate : sdt;
-        }
-        cell_dt = rmin(cell_dt, rmin(vdt, sdt));
-      }
-      for (int v = 0; v < nv; ++v) d.R0[v * n + k] = res[v];
-    } else if (stage == STAGE_DIAG) {
-      for (int v = 0; v < nv; ++v) d.R0[v * n + k] = res[v];
-    } else {
-      const R dt = (R)d.ctl[t.cs].dt_trial;
-      const bool simple = cf.has_srd && (d.c_flags[k] & 1);
-      const bool check = stage == STAGE_2 && (!cf.has_srd || simple);
-      R out[5];
-      for (int v = 0; v < nv; ++v) {
-        if (stage == STAGE_1)
-          out[v] = R(0.75) * Ub[v * n + k] + R(0.25) * (Uin[v * n + k] + dt * res[v]);
-        else
-          out[v] = Ub[v * n + k] / R(3) + R(2.0 / 3) * (Uin[v * n + k] + dt * res[v]);
-      }
-      if (simple)
-        for (int v = 0; v < 4; ++v) out[v] = srd_self(out[v], V, d.c_gvol[k]);
-      R* dst = stage == STAGE_1 ? d.U2 : Un;
-      for (int v = 0; v < nv; ++v) dst[v * n + k] = out[v];
-      if (check) {
-        const R rho = out[0], mx = out[1], my = out[2], e = out[3];
-        const R vx = mx / rho, vy = my / rho, p = (g - R(1)) * (e - R(0.5) * (mx * vx + my * vy));
-        if (!isfinite(rho) || !(rho > R(0)) || !isfinite(mx) || !isfinite(my) || !isfinite(e) || !isfinite(p) || !(p > R(0)))
-          bad = true;
-        if (MODEL == MODEL_SA && !isfinite(out[4])) bad = true;
-      }
-    }
+    cell_dt = finish_cell<R, MODEL>(d, cf, t.cs, k, stage, a, e, b, SmemSlots<R>{sm}, Uin, Ub, Un, bad);
   }
-  if (bad) *tile_bad = true;
-  if (base) {
-    // block minimum of the cell dt (exact; order-free)
-    for (int o = 16; o > 0; o >>= 1) cell_dt = rmin(cell_dt, __shfl_xor_sync(0xffffffffu, cell_dt, o));
-    if ((i & 31) == 0 && cell_dt < *tile_dt) {
-      atomicMin((unsigned long long*)tile_dt, (unsigned long long)__double_as_longlong(cell_dt));
-    }
-  }
-  __syncthreads();
+  *warp_bad = __any_sync(FULL_MASK, bad);
+  if (base)  // warp minimum of the cell dt (exact; order-free)
+    for (int o = 16; o > 0; o >>= 1) cell_dt = rmin(cell_dt, __shfl_xor_sync(FULL_MASK, cell_dt, o));
+  *warp_dt = cell_dt;
+  __syncwarp();  // the warp's shared memory is reused by its next tile
 }
 
 // Per-case step size of the current trial (reference src/static_amr2d.cpp:395-411 and the
@@ -618,7 +658,8 @@ __device__ void phase_first_update(const Dev<R>& d, const Tile& t, const R* Ub, 
   double dt;
   int fatal;
   const bool ok = choose_dt(c, cf.dt_fixed, &dt, &fatal);
-  if (threadIdx.x == 0 && t.leader) {
+  const int lane = threadIdx.x & 31;
+  if (lane == 0 && t.leader) {
     if (ok) {
       d.ctl[t.cs].dt_trial = dt;
       if (!c.retrying) d.ctl[t.cs].attempt = 0;
@@ -629,7 +670,7 @@ __device__ void phase_first_update(const Dev<R>& d, const Tile& t, const R* Ub, 
   if (!ok) return;
   const int nv = MODEL == MODEL_SA ? 5 : 4;
   const R dtr = (R)dt;
-  for (int j = threadIdx.x; j < t.c1 - t.c0; j += blockDim.x) {
+  for (int j = lane; j < t.c1 - t.c0; j += 32) {
     const int k = t.c0 + j;
     const bool simple = cf.has_srd && (d.c_flags[k] & 1);
     for (int v = 0; v < nv; ++v) {
@@ -716,9 +757,9 @@ template <class R> __device__ __forceinline__ R* state_buf(const Dev<R>& d, int 
 
 // ------------------------------------------------------------------------------------------
 // The persistent kernel.  MODE_TRIALS runs up to `trials` trials; MODE_RESIDUAL evaluates
-// the residual of every live case's accepted state into R0 (no update).
-// Every skip decision is taken by thread 0 from the control word and broadcast through
-// shared memory, so all threads of a block pass the same __syncthreads().
+// the residual of every live case's accepted state into R0 (no update).  Tiles are processed
+// one per warp; a warp's skip decision is taken by lane 0 from the control word and broadcast,
+// so every lane of a warp follows the same path through __syncwarp().
 // ------------------------------------------------------------------------------------------
 enum { SKIP_LIVE = 0, SKIP_ACTIVE = 1, SKIP_STAGE = 2 };
 
@@ -735,19 +776,20 @@ struct TileView {
 };
 
 __device__ __forceinline__ TileView read_tile(const Tile* tiles, const CaseCtl* ctl, int ti, int rule) {
-  __shared__ TileView s;
-  if (threadIdx.x == 0) {
-    s.t = tiles[ti];
-    const CaseCtl& c = ctl[s.t.cs];
-    s.skip = skip_case(c, rule);
-    s.cur = c.cur;
+  TileView v;
+  v.t = tiles[ti];
+  int skip = 0, cur = 0;
+  if ((threadIdx.x & 31) == 0) {
+    const CaseCtl& c = ctl[v.t.cs];
+    skip = skip_case(c, rule);
+    cur = c.cur;
   }
-  __syncthreads();
-  const TileView v = s;
-  __syncthreads();
+  v.skip = __shfl_sync(FULL_MASK, skip, 0) != 0;
+  v.cur = __shfl_sync(FULL_MASK, cur, 0);
   return v;
 }
 
+// Block-level variant for the per-case SRD phase.
 __device__ __forceinline__ bool read_case_skip(const CaseCtl* ctl, int cs, int rule, bool extra, int* cur) {
   __shared__ int s[2];
   if (threadIdx.x == 0) {
@@ -761,34 +803,49 @@ __device__ __forceinline__ bool read_case_skip(const CaseCtl* ctl, int cs, int r
   return skip;
 }
 
+template <class R> __device__ __forceinline__ const R* stage_input(const Dev<R>& d, int stage, int cur) {
+  if (stage == STAGE_BASE || stage == STAGE_DIAG) return state_buf(d, cur);
+  return stage == STAGE_1 ? state_buf(d, cur ^ 1) : d.U2;
+}
+
+// One phase over all tiles, one tile per warp.
+template <class R, int MODEL, int FLUX, bool GRAD>
+__device__ __forceinline__ void tile_sweep(const Dev<R>& d, int stage, R* sm_block) {
+  const int wpb = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  R* sm = sm_block + warp * (SM_COLS * TILE_W);
+  const int rule = stage == STAGE_DIAG ? SKIP_LIVE : (stage == STAGE_BASE ? SKIP_ACTIVE : SKIP_STAGE);
+  for (int ti = blockIdx.x * wpb + warp; ti < d.n_tiles; ti += gridDim.x * wpb) {
+    const TileView v = read_tile(d.tiles, d.ctl, ti, rule);
+    if (v.skip) continue;
+    if (GRAD) {
+      phase_gradients<R, MODEL>(d, v.t, stage_input(d, stage, v.cur), sm);
+    } else {
+      bool wbad;
+      double wdt;
+      phase_flux<R, MODEL, FLUX>(d, v.t, stage, stage_input(d, stage, v.cur), state_buf(d, v.cur),
+                                 state_buf(d, v.cur ^ 1), sm, &wbad, &wdt);
+      if (lane == 0 && stage != STAGE_DIAG) {
+        if (wbad) atomicOr(&d.ctl[v.t.cs].bad, 1);
+        if (stage == STAGE_BASE) atomic_min_dt(&d.ctl[v.t.cs].dtmin, wdt);
+      }
+    }
+  }
+}
+
 template <class R, int MODEL, int FLUX, bool SRD>
 __global__ void __launch_bounds__(MAX_BLOCK) trials_kernel(Dev<R> d, int trials, int mode) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* sm = reinterpret_cast<R*>(smem_raw);
-  __shared__ bool s_bad;
-  __shared__ double s_dt;
   GridBarrier* bar = d.bar;
   const unsigned long long lim = d.barrier_cycles;
   const int gsz = gridDim.x * blockDim.x, gid = blockIdx.x * blockDim.x + threadIdx.x;
-  const double inf = __longlong_as_double(0x7FF0000000000000ll);
 
   if (mode == MODE_RESIDUAL) {
     if (MODEL >= MODEL_LAMINAR) {
-      for (int ti = blockIdx.x; ti < d.n_tiles; ti += gridDim.x) {
-        const TileView v = read_tile(d.tiles, d.ctl, ti, SKIP_LIVE);
-        if (v.skip) continue;
-        phase_gradients<R, MODEL>(d, v.t, state_buf(d, v.cur), sm);
-      }
+      tile_sweep<R, MODEL, FLUX, true>(d, STAGE_DIAG, sm);
       if (!grid_barrier(bar, lim)) return;
     }
-    for (int ti = blockIdx.x; ti < d.n_tiles; ti += gridDim.x) {
-      const TileView v = read_tile(d.tiles, d.ctl, ti, SKIP_LIVE);
-      if (v.skip) continue;
-      if (threadIdx.x == 0) { s_bad = false; s_dt = 0; }
-      __syncthreads();
-      R* ub = state_buf(d, v.cur);
-      phase_flux<R, MODEL, FLUX>(d, v.t, STAGE_DIAG, ub, ub, ub, sm, &s_bad, &s_dt);
-    }
+    tile_sweep<R, MODEL, FLUX, false>(d, STAGE_DIAG, sm);
     return;
   }
 
@@ -801,31 +858,17 @@ __global__ void __launch_bounds__(MAX_BLOCK) trials_kernel(Dev<R> d, int trials,
   if (!grid_barrier(bar, lim)) return;
   if (ld_volatile(&bar->live[0]) == 0) return;
 
+  const int wpb = blockDim.x >> 5, warp = threadIdx.x >> 5;
   for (int trial = 0; trial < trials; ++trial) {
     // ---- stage 0: base residual and cell dt
     if (MODEL >= MODEL_LAMINAR) {
-      for (int ti = blockIdx.x; ti < d.n_tiles; ti += gridDim.x) {
-        const TileView v = read_tile(d.tiles, d.ctl, ti, SKIP_ACTIVE);
-        if (v.skip) continue;
-        phase_gradients<R, MODEL>(d, v.t, state_buf(d, v.cur), sm);
-      }
+      tile_sweep<R, MODEL, FLUX, true>(d, STAGE_BASE, sm);
       if (!grid_barrier(bar, lim)) return;
     }
-    for (int ti = blockIdx.x; ti < d.n_tiles; ti += gridDim.x) {
-      const TileView v = read_tile(d.tiles, d.ctl, ti, SKIP_ACTIVE);
-      if (v.skip) continue;
-      if (threadIdx.x == 0) { s_bad = false; s_dt = inf; }
-      __syncthreads();
-      R* ub = state_buf(d, v.cur);
-      phase_flux<R, MODEL, FLUX>(d, v.t, STAGE_BASE, ub, ub, ub, sm, &s_bad, &s_dt);
-      if (threadIdx.x == 0) {
-        if (s_bad) atomicOr(&d.ctl[v.t.cs].bad, 1);
-        atomic_min_dt(&d.ctl[v.t.cs].dtmin, s_dt);
-      }
-    }
+    tile_sweep<R, MODEL, FLUX, false>(d, STAGE_BASE, sm);
     if (!grid_barrier(bar, lim)) return;
     // ---- dt and U1
-    for (int ti = blockIdx.x; ti < d.n_tiles; ti += gridDim.x) {
+    for (int ti = blockIdx.x * wpb + warp; ti < d.n_tiles; ti += gridDim.x * wpb) {
       const TileView v = read_tile(d.tiles, d.ctl, ti, SKIP_ACTIVE);
       if (v.skip) continue;
       phase_first_update<R, MODEL>(d, v.t, state_buf(d, v.cur), state_buf(d, v.cur ^ 1));
@@ -841,23 +884,10 @@ __global__ void __launch_bounds__(MAX_BLOCK) trials_kernel(Dev<R> d, int trials,
         if (!grid_barrier(bar, lim)) return;
       }
       if (MODEL >= MODEL_LAMINAR) {
-        for (int ti = blockIdx.x; ti < d.n_tiles; ti += gridDim.x) {
-          const TileView v = read_tile(d.tiles, d.ctl, ti, SKIP_STAGE);
-          if (v.skip) continue;
-          phase_gradients<R, MODEL>(d, v.t, stage == 1 ? state_buf(d, v.cur ^ 1) : d.U2, sm);
-        }
+        tile_sweep<R, MODEL, FLUX, true>(d, stage, sm);
         if (!grid_barrier(bar, lim)) return;
       }
-      for (int ti = blockIdx.x; ti < d.n_tiles; ti += gridDim.x) {
-        const TileView v = read_tile(d.tiles, d.ctl, ti, SKIP_STAGE);
-        if (v.skip) continue;
-        if (threadIdx.x == 0) { s_bad = false; s_dt = 0; }
-        __syncthreads();
-        R* ub = state_buf(d, v.cur);
-        R* un = state_buf(d, v.cur ^ 1);
-        phase_flux<R, MODEL, FLUX>(d, v.t, stage, stage == 1 ? un : d.U2, ub, un, sm, &s_bad, &s_dt);
-        if (threadIdx.x == 0 && s_bad) atomicOr(&d.ctl[v.t.cs].bad, 1);
-      }
+      tile_sweep<R, MODEL, FLUX, false>(d, stage, sm);
       if (!grid_barrier(bar, lim)) return;
     }
     if (SRD) {
@@ -883,10 +913,9 @@ __global__ void __launch_bounds__(MAX_BLOCK) trials_kernel(Dev<R> d, int trials,
 }
 
 // ------------------------------------------------------------------------------------------
-// Phase kernels: the same phases as trials_kernel, one kernel per phase and one block per tile,
-// for batches large enough to fill the GPU many times over.  A trial is the launch sequence
-//   [grad 0] flux 0, first_update, [srd 1], [grad 1], flux 1, [srd 2], [grad 2], flux 2,
-//   [srd 3], commit
+// Phase kernels: the same phases as trials_kernel, one kernel per phase, for batches large
+// enough to fill the GPU many times over.  A trial is the launch sequence
+//   [grad 0] flux 0, first, [srd 1], [grad 1], flux 1, [srd 2], [grad 2], flux 2, [srd 3], commit
 // and a CUDA graph replays `trials` such sequences.
 // ------------------------------------------------------------------------------------------
 // Phase kernels run 128-thread blocks; the occupancy target sets the register budget
@@ -899,52 +928,16 @@ template <class R> struct PhaseOcc;
 template <> struct PhaseOcc<float> { static constexpr int flux = AMRB_FLUX_MINB_F32, grad = 8; };
 template <> struct PhaseOcc<double> { static constexpr int flux = 3, grad = 4; };
 
-template <class R> __device__ __forceinline__ const R* stage_input(const Dev<R>& d, int stage, int cur) {
-  if (stage == STAGE_BASE || stage == STAGE_DIAG) return state_buf(d, cur);
-  return stage == STAGE_1 ? state_buf(d, cur ^ 1) : d.U2;
-}
-
 template <class R, int MODEL>
 __global__ void __launch_bounds__(PHASE_BLOCK, PhaseOcc<R>::grad) phase_grad_kernel(Dev<R> d, int stage) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R* sm = reinterpret_cast<R*>(smem_raw);
-  const int rule = stage == STAGE_DIAG ? SKIP_LIVE : (stage == STAGE_BASE ? SKIP_ACTIVE : SKIP_STAGE);
-  for (int ti = blockIdx.x; ti < d.n_tiles; ti += gridDim.x) {
-    const TileView v = read_tile(d.tiles, d.ctl, ti, rule);
-    if (v.skip) continue;
-    phase_gradients<R, MODEL>(d, v.t, stage_input(d, stage, v.cur), sm);
-  }
+  tile_sweep<R, MODEL, 0, true>(d, stage, reinterpret_cast<R*>(smem_raw));
 }
 
 template <class R, int MODEL, int FLUX>
 __global__ void __launch_bounds__(PHASE_BLOCK, PhaseOcc<R>::flux) phase_flux_kernel(Dev<R> d, int stage) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R* sm = reinterpret_cast<R*>(smem_raw);
-  __shared__ bool s_bad;
-  __shared__ double s_dt;
-  const int rule = stage == STAGE_DIAG ? SKIP_LIVE : (stage == STAGE_BASE ? SKIP_ACTIVE : SKIP_STAGE);
-  for (int ti = blockIdx.x; ti < d.n_tiles; ti += gridDim.x) {
-    const TileView v = read_tile(d.tiles, d.ctl, ti, rule);
-    if (v.skip) continue;
-    if (threadIdx.x == 0) { s_bad = false; s_dt = __longlong_as_double(0x7FF0000000000000ll); }
-    __syncthreads();
-    R* ub = state_buf(d, v.cur);
-    R* un = state_buf(d, v.cur ^ 1);
-    phase_flux<R, MODEL, FLUX>(d, v.t, stage, stage_input(d, stage, v.cur), ub, un, sm, &s_bad, &s_dt);
-    if (threadIdx.x == 0 && stage != STAGE_DIAG) {
-      if (s_bad) atomicOr(&d.ctl[v.t.cs].bad, 1);
-      if (stage == STAGE_BASE) atomic_min_dt(&d.ctl[v.t.cs].dtmin, s_dt);
-    }
-  }
-}
-
-template <class R, int MODEL>
-__global__ void __launch_bounds__(MAX_BLOCK, 4) phase_first_kernel(Dev<R> d) {
-  for (int ti = blockIdx.x; ti < d.n_tiles; ti += gridDim.x) {
-    const TileView v = read_tile(d.tiles, d.ctl, ti, SKIP_ACTIVE);
-    if (v.skip) continue;
-    phase_first_update<R, MODEL>(d, v.t, state_buf(d, v.cur), state_buf(d, v.cur ^ 1));
-  }
+  tile_sweep<R, MODEL, FLUX, false>(d, stage, reinterpret_cast<R*>(smem_raw));
 }
 
 // U1 = U + dt R0, one thread per cell (phase mode).  Every thread derives its case's step size
@@ -1003,6 +996,178 @@ static __global__ void phase_commit_kernel(CaseCtl* ctl, int n_cases, int begin_
   case_begin(c);
 }
 
+// ------------------------------------------------------------------------------------------
+// Split mode: gradients one thread per cell, fluxes one thread per face or wall record (each face
+// evaluated once, in face orientation), then one thread per cell gathering its records in the
+// reference's order with the stage update.  Same arithmetic as the other modes.
+// ------------------------------------------------------------------------------------------
+#ifndef AMRB_SPLIT_MINB_F32
+#define AMRB_SPLIT_MINB_F32 8
+#endif
+template <class R> struct SplitOcc;
+template <> struct SplitOcc<float> { static constexpr int item = AMRB_SPLIT_MINB_F32, cell = 8; };
+template <> struct SplitOcc<double> { static constexpr int item = 3, cell = 4; };
+
+__device__ __forceinline__ int stage_rule(int stage) {
+  return stage == STAGE_DIAG ? SKIP_LIVE : (stage == STAGE_BASE ? SKIP_ACTIVE : SKIP_STAGE);
+}
+
+// A face or wall record is 12 values: flux 0-3, viscous flux 4-7, convective and viscous
+// spectral radius 8-9, SA flux 10 and SA spectral term 11.  Records are 16-byte aligned and
+// moved as 16-byte vectors; a model moves only the groups it uses (columns 8-11 ride with
+// the spectral radius, which only the base stage needs beyond column 10).
+template <class R> struct Vec16;
+template <> struct Vec16<float> { using T = float4; static constexpr int n = 4; };
+template <> struct Vec16<double> { using T = double2; static constexpr int n = 2; };
+
+template <class R> __device__ __forceinline__ void store_group(R* dst, const R* src) {
+  using V = typename Vec16<R>::T;
+  constexpr int m = Vec16<R>::n;
+#pragma unroll
+  for (int j = 0; j < 4 / m; ++j) {
+    V v;
+    R* e = reinterpret_cast<R*>(&v);
+#pragma unroll
+    for (int i = 0; i < m; ++i) e[i] = src[j * m + i];
+    reinterpret_cast<V*>(dst)[j] = v;
+  }
+}
+
+template <class R> __device__ __forceinline__ void load_group(const R* src, R* dst) {
+  using V = typename Vec16<R>::T;
+  constexpr int m = Vec16<R>::n;
+#pragma unroll
+  for (int j = 0; j < 4 / m; ++j) {
+    const V v = __ldg(reinterpret_cast<const V*>(src) + j);
+    const R* e = reinterpret_cast<const R*>(&v);
+#pragma unroll
+    for (int i = 0; i < m; ++i) dst[j * m + i] = e[i];
+  }
+}
+
+template <class R, int MODEL> __device__ __forceinline__ void store_record(R* dst, R* rec, bool base) {
+  if (!base) rec[8] = rec[9] = rec[11] = R(0);
+  if (MODEL < MODEL_SA) rec[10] = rec[11] = R(0);
+  if (MODEL < MODEL_LAMINAR) rec[9] = R(0);
+  store_group(dst, rec);
+  if (MODEL >= MODEL_LAMINAR) store_group(dst + 4, rec + 4);
+  if (base || MODEL == MODEL_SA) store_group(dst + 8, rec + 8);
+}
+
+template <class R, int MODEL> __device__ __forceinline__ void load_record(const R* src, R* col, bool base) {
+  load_group(src, col);
+  if (MODEL >= MODEL_LAMINAR) load_group(src + 4, col + 4);
+  if (base || MODEL == MODEL_SA) load_group(src + 8, col + 8);
+}
+
+template <class R, int MODEL>
+__global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::cell) grad_cells_kernel(Dev<R> d, int stage, int ncells) {
+  const int rule = stage_rule(stage);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ncells; k += gridDim.x * blockDim.x) {
+    const int cs = d.c_case[k];
+    if (cs < 0) continue;
+    const CaseCtl& c = d.ctl[cs];
+    if (skip_case(c, rule)) continue;
+    const CaseCfg<R>& cf = d.cfg[cs];
+    const R* Uin = stage_input(d, stage, c.cur);
+    R gr[4] = {0, 0, 0, 0}, sg[4] = {0, 0, 0, 0};
+    for (int q = d.c_term[k]; q < d.c_term[k + 1]; ++q) {
+      R t[8];
+      term_values<R, MODEL>(d, cf, q, k, Uin, t);
+      for (int v = 0; v < 4; ++v) gr[v] += t[v];
+      if (MODEL == MODEL_SA)
+        for (int v = 0; v < 4; ++v) sg[v] += t[4 + v];
+    }
+    if (!grad_finish<R, MODEL>(d, cf, k, Uin, gr, sg)) atomicOr(&d.ctl[cs].bad, 1);
+  }
+}
+
+template <class R, int MODEL, int FLUX>
+__global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::item) item_kernel(Dev<R> d, int stage) {
+  const int rule = stage_rule(stage);
+  const bool base = stage == STAGE_BASE;
+  const int total = d.n_faces + d.n_walls;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    bool bad = false;
+    int cs;
+    if (idx < d.n_faces) {
+      const int f = idx;
+      cs = d.f_case[f];
+      if (cs < 0) continue;
+      const CaseCtl& c = d.ctl[cs];
+      if (skip_case(c, rule)) continue;
+      R rec[SM_COLS];
+      slot_face<R, MODEL, FLUX>(d, d.cfg[cs], d.f_geo + 6 * (long long)f, __ldg(d.f_len + f), __ldg(d.f_own + f),
+                                __ldg(d.f_nb + f), __ldg(d.f_meta + f), stage_input(d, stage, c.cur), base, rec, 1,
+                                false, bad);
+      store_record<R, MODEL>(d.fval + SM_COLS * (long long)f, rec, base);
+    } else {
+      const int w = idx - d.n_faces;
+      const int owner = d.w_owner[w];
+      if (owner < 0) continue;
+      cs = d.c_case[owner];
+      const CaseCtl& c = d.ctl[cs];
+      if (skip_case(c, rule)) continue;
+      R rec[SM_COLS];
+      slot_wall<R, MODEL>(d, d.cfg[cs], __ldg(d.w_nx + w), __ldg(d.w_ny + w), __ldg(d.w_dist + w), __ldg(d.w_len + w),
+                          owner, __ldg(d.w_donor + w), stage_input(d, stage, c.cur), base, rec, 1, bad);
+      store_record<R, MODEL>(d.wval + SM_COLS * (long long)w, rec, base);
+    }
+    if (bad && stage != STAGE_DIAG) atomicOr(&d.ctl[cs].bad, 1);
+  }
+}
+
+// The 12 values of a slot's face or wall record, flux columns signed for the slot's cell.
+template <class R, int MODEL> struct ItemSlots {
+  const Dev<R>* d;
+  bool base;
+  __device__ __forceinline__ void operator()(int q, bool wall, R* col) const {
+    const int id = __ldg(d->s_item + q);
+    const R* src = (wall ? d->wval : d->fval) + SM_COLS * (long long)id;
+    load_record<R, MODEL>(src, col, base);
+    const R sg = wall ? R(1) : ((__ldg(d->s_meta + q) & 1) ? R(1) : R(-1));
+    for (int v = 0; v < 4; ++v) col[v] = sg * col[v];
+    if (MODEL >= MODEL_LAMINAR)
+      for (int v = 4; v < 8; ++v) col[v] = sg * col[v];
+    if (MODEL == MODEL_SA) col[10] = sg * col[10];
+  }
+};
+
+template <class R, int MODEL>
+__global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::cell) gather_kernel(Dev<R> d, int stage, int ncells) {
+  const int rule = stage_rule(stage);
+  const bool base = stage == STAGE_BASE;
+  const int lane = threadIdx.x & 31;
+  // the loop bound is warp-uniform so the segmented shuffles below see full warps
+  for (int k0 = blockIdx.x * blockDim.x; k0 < ncells; k0 += gridDim.x * blockDim.x) {
+    const int k = k0 + threadIdx.x;
+    int cs = k < ncells ? d.c_case[k] : -1;
+    bool bad = false;
+    double cell_dt = __longlong_as_double(0x7FF0000000000000ll);
+    if (cs >= 0 && skip_case(d.ctl[cs], rule)) cs = -1;
+    if (cs >= 0) {
+      const CaseCtl& c = d.ctl[cs];
+      const int a = d.c_slot[k], b = d.c_slot[k + 1];
+      const int e = b - (d.c_wall[k + 1] - d.c_wall[k]);
+      cell_dt = finish_cell<R, MODEL>(d, d.cfg[cs], cs, k, stage, a, e, b, ItemSlots<R, MODEL>{&d, base},
+                                      stage_input(d, stage, c.cur), state_buf(d, c.cur), state_buf(d, c.cur ^ 1), bad);
+      if (bad && stage != STAGE_DIAG) atomicOr(&d.ctl[cs].bad, 1);
+    }
+    if (base) {
+      // per-case minimum over the warp: cells of a case are contiguous, so a segmented suffix
+      // minimum leaves each segment's first lane with its segment's minimum
+      unsigned long long bits = (unsigned long long)__double_as_longlong(cell_dt);
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long ob = __shfl_down_sync(FULL_MASK, bits, o);
+        const int oc = __shfl_down_sync(FULL_MASK, cs, o);
+        if (lane + o < 32 && oc == cs && ob < bits) bits = ob;
+      }
+      const int prev = __shfl_up_sync(FULL_MASK, cs, 1);
+      if (cs >= 0 && (lane == 0 || prev != cs)) atomicMin(&d.ctl[cs].dtmin, bits);
+    }
+  }
+}
+
 // Host-visible launch helpers (defined in amr_engine_f64.cu / amr_engine_f32.cu).
 template <class R> struct EngineOps {
   static cudaError_t launch(const Dev<R>& d, int model, int flux, bool srd, int trials, int mode, int grid, int block,
@@ -1010,6 +1175,9 @@ template <class R> struct EngineOps {
   // One trial (or, with mode MODE_RESIDUAL, one residual evaluation) as a sequence of phase kernels.
   static cudaError_t launch_phases(const Dev<R>& d, int model, int flux, bool srd, int trials, int mode, int block,
                                    cudaStream_t stream);
+  // The same with the split kernels (gradients per cell, fluxes per face record, gather per cell).
+  static cudaError_t launch_split(const Dev<R>& d, int model, int flux, bool srd, int trials, int mode,
+                                  cudaStream_t stream);
   static cudaError_t occupancy(int model, int flux, bool srd, int block, int* blocks_per_sm);
   static size_t smem_bytes(int block) { return size_t(12) * block * sizeof(R); }
 };

@@ -36,7 +36,7 @@ cudaError_t EngineOps<R>::launch(const Dev<R>& d, int model, int flux, bool srd,
 
 template <class R, int MODEL, int FLUX>
 static cudaError_t launch_phases_t(const Dev<R>& d, bool srd, int trials, int mode, int block, cudaStream_t st) {
-  const int tiles = d.n_tiles > 0 ? d.n_tiles : 1;
+  const int tiles = d.n_tiles > 0 ? (d.n_tiles + block / 32 - 1) / (block / 32) : 1;  // blocks of block/32 tile-warps
   const size_t sm = EngineOps<R>::smem_bytes(block);
   const int cases = d.n_cases;
   const int cblocks = (cases + 127) / 128;
@@ -49,7 +49,7 @@ static cudaError_t launch_phases_t(const Dev<R>& d, bool srd, int trials, int mo
   for (int t = 0; t < trials; ++t) {
     if (MODEL >= MODEL_LAMINAR) phase_grad_kernel<R, MODEL><<<tiles, block, sm, st>>>(d, STAGE_BASE);
     phase_flux_kernel<R, MODEL, FLUX><<<tiles, block, sm, st>>>(d, STAGE_BASE);
-    phase_first_cells_kernel<R, MODEL><<<(int)((d.ncap + 255) / 256), 256, 0, st>>>(d, (int)d.ncap);
+    phase_first_cells_kernel<R, MODEL><<<(d.n_cells + 255) / 256 + 1, 256, 0, st>>>(d, d.n_cells);
     for (int stage = 1; stage <= 2; ++stage) {
       if (srd) phase_srd_kernel<R, MODEL><<<cases, block, 0, st>>>(d, stage);
       if (MODEL >= MODEL_LAMINAR) phase_grad_kernel<R, MODEL><<<tiles, block, sm, st>>>(d, stage);
@@ -72,6 +72,50 @@ cudaError_t EngineOps<R>::launch_phases(const Dev<R>& d, int model, int flux, bo
                              : launch_phases_t<R, MODEL_LAMINAR, FLUX_AUSM>(d, srd, trials, mode, block, stream);
   return flux == FLUX_HLLC ? launch_phases_t<R, MODEL_SA, FLUX_HLLC>(d, srd, trials, mode, block, stream)
                            : launch_phases_t<R, MODEL_SA, FLUX_AUSM>(d, srd, trials, mode, block, stream);
+}
+
+template <class R, int MODEL, int FLUX>
+static cudaError_t launch_split_t(const Dev<R>& d, bool srd, int trials, int mode, cudaStream_t st) {
+  const int B = PHASE_BLOCK;
+  const int ncells = d.n_cells;
+  const int cblocks = (ncells + B - 1) / B + (ncells == 0);
+  const int iblocks = (d.n_faces + d.n_walls + B - 1) / B + (d.n_faces + d.n_walls == 0);
+  const int cases = d.n_cases;
+  const int kblocks = (cases + 127) / 128;
+  auto stage_seq = [&](int stage) {
+    if (MODEL >= MODEL_LAMINAR) grad_cells_kernel<R, MODEL><<<cblocks, B, 0, st>>>(d, stage, ncells);
+    item_kernel<R, MODEL, FLUX><<<iblocks, B, 0, st>>>(d, stage);
+    gather_kernel<R, MODEL><<<cblocks, B, 0, st>>>(d, stage, ncells);
+  };
+  if (mode == MODE_RESIDUAL) {
+    stage_seq(STAGE_DIAG);
+    return cudaGetLastError();
+  }
+  phase_commit_kernel<<<kblocks, 128, 0, st>>>(d.ctl, cases, 1);
+  for (int t = 0; t < trials; ++t) {
+    stage_seq(STAGE_BASE);
+    phase_first_cells_kernel<R, MODEL><<<(ncells + 255) / 256, 256, 0, st>>>(d, ncells);
+    for (int stage = 1; stage <= 2; ++stage) {
+      if (srd) phase_srd_kernel<R, MODEL><<<cases, MAX_BLOCK, 0, st>>>(d, stage);
+      stage_seq(stage);
+    }
+    if (srd) phase_srd_kernel<R, MODEL><<<cases, MAX_BLOCK, 0, st>>>(d, 3);
+    phase_commit_kernel<<<kblocks, 128, 0, st>>>(d.ctl, cases, 0);
+  }
+  return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t EngineOps<R>::launch_split(const Dev<R>& d, int model, int flux, bool srd, int trials, int mode,
+                                       cudaStream_t stream) {
+  if (model == MODEL_EULER)
+    return flux == FLUX_HLLC ? launch_split_t<R, MODEL_EULER, FLUX_HLLC>(d, srd, trials, mode, stream)
+                             : launch_split_t<R, MODEL_EULER, FLUX_AUSM>(d, srd, trials, mode, stream);
+  if (model == MODEL_LAMINAR)
+    return flux == FLUX_HLLC ? launch_split_t<R, MODEL_LAMINAR, FLUX_HLLC>(d, srd, trials, mode, stream)
+                             : launch_split_t<R, MODEL_LAMINAR, FLUX_AUSM>(d, srd, trials, mode, stream);
+  return flux == FLUX_HLLC ? launch_split_t<R, MODEL_SA, FLUX_HLLC>(d, srd, trials, mode, stream)
+                           : launch_split_t<R, MODEL_SA, FLUX_AUSM>(d, srd, trials, mode, stream);
 }
 
 template <class R> cudaError_t EngineOps<R>::occupancy(int model, int flux, bool srd, int block, int* blocks_per_sm) {
@@ -195,13 +239,13 @@ template <class R> int Batch<R>::autotune(int trials, std::string* error) {
   cudaMemcpyAsync(s1.p, U1_.p, nbytes, cudaMemcpyDeviceToDevice, stream_);
   double best = 1e30;
   int best_block = block_, best_grid = grid_request_;
-  bool best_phases = phases_;
+  int best_mode = mode_;
   const bool graph_save = use_graph_;
   use_graph_ = false;
-  for (int phases = 0; phases <= 1; ++phases) {
+  for (int mode : {AMR_B200_LAUNCH_PERSISTENT, AMR_B200_LAUNCH_PHASES, AMR_B200_LAUNCH_SPLIT}) {
     for (int block : {128, 256}) {
-      if (phases && block != PHASE_BLOCK) continue;
-      phases_ = phases != 0;
+      if (mode != AMR_B200_LAUNCH_PERSISTENT && block != PHASE_BLOCK) continue;
+      mode_ = mode;
       block_ = block;
       grid_request_ = 0;
       if (!configure_grid(error)) continue;
@@ -212,9 +256,10 @@ template <class R> int Batch<R>::autotune(int trials, std::string* error) {
       tiles_dirty_ = true;
       if (!sync_tiles(error)) return 1;
       std::vector<int> grids = {max_grid_};
-      if (!phases_) {
-        if (n_tiles_ < max_grid_) grids.push_back(std::max(1, n_tiles_));
-        if (n_tiles_ / 2 < max_grid_ && n_tiles_ / 2 >= 8) grids.push_back(n_tiles_ / 2);
+      if (mode_ == AMR_B200_LAUNCH_PERSISTENT) {
+        const int need = (n_tiles_ + block / 32 - 1) / (block / 32);  // one tile per warp
+        if (need < max_grid_) grids.push_back(std::max(1, need));
+        if (need / 2 < max_grid_ && need / 2 >= 8) grids.push_back(need / 2);
       }
       for (int grid : grids) {
         grid_request_ = grid;
@@ -230,12 +275,12 @@ template <class R> int Batch<R>::autotune(int trials, std::string* error) {
           best = t;
           best_block = block;
           best_grid = grid;
-          best_phases = phases_;
+          best_mode = mode_;
         }
       }
     }
   }
-  phases_ = best_phases;
+  mode_ = best_mode;
   block_ = best_block;
   grid_request_ = best_grid;
   configure_grid(error);

@@ -27,8 +27,8 @@ def write_inputs(golden, folder, mode, backend, profile='LF1'):
     z = np.load(golden / 'examples.npz')
     i = list(z['names']).index('G0001')
     a, b = z['offsets'][i], z['offsets'][i + 1]
-    (folder / 'airfoil.csv').write_text('x,y\n' + ''.join(f'{x!r},{y!r}\n' for x, y in zip(z['x'][a:b], z['y'][a:b])))
-    (folder / 'patches.csv').write_text('edge,patch\n' + ''.join(f'{j},{p}\n' for j, p in enumerate(z['patches'][a:b])))
+    (folder / 'airfoil.csv').write_text('x,y\n' + ''.join(f'{float(x)!r},{float(y)!r}\n' for x, y in zip(z['x'][a:b], z['y'][a:b])))
+    (folder / 'patches.csv').write_text('edge,patch\n' + ''.join(f'{j},{int(p)}\n' for j, p in enumerate(z['patches'][a:b])))
 
 
 def run(golden, tmp_path, mode, backend):
