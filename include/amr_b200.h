@@ -319,6 +319,63 @@ int amr_batch_autotune(amr_batch* batch, int32_t trials, char* error, uint64_t e
 uint64_t amr_batch_kernel_launches(const amr_batch* batch);
 void amr_batch_destroy(amr_batch* batch);
 
+/* ----------------------------------------------------------------------------------
+ * Host mesh builder.
+ *
+ * amr_mesh_build replaces the reference's two host calls that turn a body polygon into a
+ * solver-ready mesh: static_amr2d_build (src/static_amr2d.h:80-82, src/static_amr2d.cpp:229)
+ * followed by static_amr2d_prepare_viscous (src/static_amr2d_viscous.h, defined at
+ * src/static_amr2d_viscous.cpp:40, which also runs static_amr2d_prepare_sa).  The tables it
+ * returns are bit-identical to the reference's; the build is faster and amr_mesh_build_many
+ * runs many builds on a pool of host threads (no reference counterpart), so that mesh
+ * generation keeps up with a serving batch.
+ * ---------------------------------------------------------------------------------- */
+typedef struct amr_mesh_box_t {
+  double x0, x1, y0, y1;
+  int32_t level;
+} amr_mesh_box_t;
+
+/* StaticAmrOptions2D (src/static_amr2d.h:29-35). */
+typedef struct amr_mesh_options_t {
+  int32_t nx, ny, levels, buffer;
+  double xmin, xmax, ymin, ymax;
+  uint64_t max_cells;
+  int32_t agglomerate_small;
+  int32_t n_boxes;
+  const amr_mesh_box_t* boxes;
+} amr_mesh_options_t;
+
+/* One build: options, the closed body polygon (no repeated closing vertex) with optional
+ * per-edge patch ids, and the physics the tables depend on (boundary kinds, transport). */
+typedef struct amr_mesh_request_t {
+  const amr_mesh_options_t* options;
+  const double* px;
+  const double* py;
+  const int32_t* patches; /* n_points or NULL */
+  uint64_t n_points;
+  const amr_boundary_t* boundaries; /* 4: xmin, xmax, ymin, ymax */
+  const amr_transport_t* transport;
+  const amr_params_t* params;       /* bc[] of sides whose kind is INHERIT */
+} amr_mesh_request_t;
+
+typedef struct amr_mesh_counts_t {
+  uint64_t background_leaves, split_leaves, coarse_fine_faces, small_cells, n_terms;
+} amr_mesh_counts_t;
+
+typedef struct amr_mesh_t amr_mesh_t; /* opaque; owns every table of one mesh */
+
+int amr_mesh_build(const amr_mesh_request_t* request, amr_mesh_t** out, char* error, uint64_t error_size);
+/* Builds count meshes on `threads` host threads (0 = all cores).  out[i] and status[i] (0 or
+ * 1) are set per request; a failed request's message goes to errors + i * error_stride.
+ * Returns 1 if any request failed. */
+int amr_mesh_build_many(uint64_t count, const amr_mesh_request_t* requests, int32_t threads, amr_mesh_t** out,
+                        int32_t* status, char* errors, uint64_t error_stride);
+/* A view of the mesh's tables, valid until amr_mesh_destroy; pass it to amr_gpu_create or
+ * amr_batch_admit. */
+int amr_mesh_view(const amr_mesh_t* mesh, amr_mesh_view_t* view);
+int amr_mesh_get_counts(const amr_mesh_t* mesh, amr_mesh_counts_t* counts);
+void amr_mesh_destroy(amr_mesh_t* mesh);
+
 #ifdef __cplusplus
 }
 #endif

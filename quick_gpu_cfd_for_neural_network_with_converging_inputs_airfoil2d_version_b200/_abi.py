@@ -80,6 +80,26 @@ class MeshView(C.Structure):
                 ('face_geometry', _P), ('wall_distance', _P)]
 
 
+class MeshBox(C.Structure):
+    _fields_ = [('x0', C.c_double), ('x1', C.c_double), ('y0', C.c_double), ('y1', C.c_double), ('level', C.c_int32)]
+
+
+class MeshOptions(C.Structure):
+    _fields_ = [('nx', C.c_int32), ('ny', C.c_int32), ('levels', C.c_int32), ('buffer', C.c_int32),
+                ('xmin', C.c_double), ('xmax', C.c_double), ('ymin', C.c_double), ('ymax', C.c_double),
+                ('max_cells', C.c_uint64), ('agglomerate_small', C.c_int32), ('n_boxes', C.c_int32), ('boxes', _P)]
+
+
+class MeshRequest(C.Structure):
+    _fields_ = [('options', _P), ('px', _P), ('py', _P), ('patches', _P), ('n_points', C.c_uint64),
+                ('boundaries', _P), ('transport', _P), ('params', _P)]
+
+
+class MeshCounts(C.Structure):
+    _fields_ = [('background_leaves', C.c_uint64), ('split_leaves', C.c_uint64), ('coarse_fine_faces', C.c_uint64),
+                ('small_cells', C.c_uint64), ('n_terms', C.c_uint64)]
+
+
 class GpuOptions(C.Structure):
     _fields_ = [('batch_trials', C.c_int32), ('graph', C.c_int32), ('fused', C.c_int32), ('event_timing', C.c_int32),
                 ('sa_fused', C.c_int32), ('device', C.c_int32), ('block_threads', C.c_int32), ('grid_blocks', C.c_int32),

@@ -35,6 +35,11 @@ SIGNATURES = {
     'amr_batch_last_advance_seconds': (C.c_double, [_P]),
     'amr_batch_kernel_launches': (C.c_uint64, [_P]),
     'amr_batch_destroy': (None, [_P]),
+    'amr_mesh_build': (C.c_int, [_P, _P, _S, C.c_uint64]),
+    'amr_mesh_build_many': (C.c_int, [C.c_uint64, _P, C.c_int32, _P, _P, _P, C.c_uint64]),
+    'amr_mesh_view': (C.c_int, [_P, _P]),
+    'amr_mesh_get_counts': (C.c_int, [_P, _P]),
+    'amr_mesh_destroy': (None, [_P]),
     # extras used by the host mirror
     'amr_batch_autotune': (C.c_int, [_P, C.c_int32, _S, C.c_uint64]),
     'amr_batch_launch_config': (C.c_int, [_P, _S, C.c_uint64]),

@@ -25,6 +25,12 @@ UNITS = {
     'amr_capi.cu': [],
     'amr_static.cu': ['-fmad=false'],
 }
+# Host-only units, compiled by the system g++ (the compiler, libstdc++ and libm the reference
+# CPU core is built with) without floating-point contraction.
+HOST_UNITS = {
+    'amr_mesh.cpp': ['-O2', '-ffp-contract=off', '-fno-fast-math'],
+}
+HOST_CXX = '/usr/bin/g++' if os.path.exists('/usr/bin/g++') else (shutil.which('g++') or 'g++')
 
 
 def nvcc():
@@ -35,7 +41,8 @@ def nvcc():
 
 
 def _sources():
-    return sorted(CSRC.glob('*.cu')) + sorted(CSRC.glob('*.cuh')) + sorted(CSRC.glob('*.h')) + [PKG.parent / 'include' / 'amr_b200.h']
+    return (sorted(CSRC.glob('*.cu')) + sorted(CSRC.glob('*.cuh')) + sorted(CSRC.glob('*.h')) + sorted(CSRC.glob('*.cpp')) +
+            [PKG.parent / 'include' / 'amr_b200.h'])
 
 
 def up_to_date():
@@ -54,7 +61,11 @@ def build(force=False, verbose=False):
     def compile_unit(item):
         name, extra = item
         obj = BUILD / (name + '.o')
-        cmd = [cc, *ARCH, *COMMON, *extra, '-c', str(CSRC / name), '-o', str(obj)]
+        if name in HOST_UNITS:
+            cmd = [HOST_CXX, '-std=c++17', '-fPIC', '-g', '-I', str(PKG.parent / 'include'), *extra, '-c', str(CSRC / name),
+                   '-o', str(obj)]
+        else:
+            cmd = [cc, *ARCH, *COMMON, *extra, '-c', str(CSRC / name), '-o', str(obj)]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode:
             raise RuntimeError(f'nvcc failed for {name}:\n{r.stderr[-4000:]}')
@@ -62,10 +73,12 @@ def build(force=False, verbose=False):
             print(r.stderr)
         return obj
 
-    with concurrent.futures.ThreadPoolExecutor(max_workers=len(UNITS)) as ex:
-        objs = list(ex.map(compile_unit, UNITS.items()))
+    units = {**UNITS, **HOST_UNITS}
+    with concurrent.futures.ThreadPoolExecutor(max_workers=len(units)) as ex:
+        objs = list(ex.map(compile_unit, units.items()))
     tmp = LIB.with_suffix('.so.tmp')
-    r = subprocess.run([cc, *ARCH, '-shared', '-o', str(tmp), *map(str, objs), '-lcudart'], capture_output=True, text=True)
+    r = subprocess.run([cc, *ARCH, '-shared', '-o', str(tmp), *map(str, objs), '-lcudart', '-lpthread'], capture_output=True,
+                       text=True)
     if r.returncode:
         raise RuntimeError('link failed:\n' + r.stderr[-4000:])
     os.replace(tmp, LIB)
