@@ -135,6 +135,7 @@ template <class R> class Batch final : public BatchBase {
     cap_slots_ = slots;
     cap_faces_ = slots;  // every face is listed by at least one cell
     cap_walls_ = walls;
+    if (cap_faces_ >= (1ll << 30) || cap_walls_ >= (1ll << 30)) return fail(error, "arena too large for 32-bit record indices");
     cap_terms_ = std::max<long long>(terms, 1);
     cap_groups_ = srd;
     cap_gmem_ = 8 * srd;
@@ -323,6 +324,20 @@ template <class R> class Batch final : public BatchBase {
     const int fb = (int)hc.faces.b;
     std::vector<int> s_item(ns), f_case(nf, slot), f_own(nf), f_nb(nf), f_meta(nf), w_owner(nw);
     std::vector<R> f_len(nf), f_geo(6 * nf, R(0));
+    // face records go in order of first reference by a cell, in slot order, so that the
+    // records of neighbouring cells are neighbours in memory (the reference's face order runs
+    // along grid lines)
+    std::vector<int> rec(nf, -1);
+    {
+      int next = 0;
+      for (long long k = 0; k < n; ++k)
+        for (uint64_t q = m->face_offsets[k]; q < m->face_offsets[k + 1]; ++q) {
+          const uint64_t fi = m->cell_faces[q];
+          if (fi < (uint64_t)nf && rec[fi] < 0) rec[fi] = next++;
+        }
+      for (long long fi = 0; fi < nf; ++fi)
+        if (rec[fi] < 0) rec[fi] = next++;  // a face no cell lists (still evaluated, never gathered)
+    }
     int kinds[4];
     for (int side = 0; side < 4; ++side) kinds[side] = m->boundaries[side].kind < 0 ? p->bc[side] : m->boundaries[side].kind;
     long long wpos = 0, spos = 0;
@@ -352,7 +367,7 @@ template <class R> class Batch final : public BatchBase {
         s_nb[spos] = other >= 0 ? cb + other : -1;
         s_meta[spos] = (own_left ? 1 : 0) | ((f.axis & 1) << 1) | ((side + 1) << 2) | ((kind & 15) << 5);
         s_len[spos] = (R)f.length;
-        s_item[spos] = fb + (int)fi;
+        s_item[spos] = 2 * (fb + rec[fi]) + (own_left ? 1 : 0);  // record index and orientation
         if (model_ >= MODEL_LAMINAR) {
           const amr_face_geometry_t& g = m->face_geometry[fi];
           s_geo[6 * spos + 0] = (R)g.dx;
@@ -413,18 +428,19 @@ template <class R> class Batch final : public BatchBase {
         return fail_release(hc, error, "face cells or boundary marker inconsistent");
       const int side = f.boundary;
       const int kind = side >= 0 ? kinds[side] : 0;
-      f_own[fi] = cb + own;
-      f_nb[fi] = other >= 0 ? cb + other : -1;
-      f_meta[fi] = (own_left ? 1 : 0) | ((f.axis & 1) << 1) | ((side + 1) << 2) | ((kind & 15) << 5);
-      f_len[fi] = (R)f.length;
+      const long long r = rec[fi];
+      f_own[r] = cb + own;
+      f_nb[r] = other >= 0 ? cb + other : -1;
+      f_meta[r] = (own_left ? 1 : 0) | ((f.axis & 1) << 1) | ((side + 1) << 2) | ((kind & 15) << 5);
+      f_len[r] = (R)f.length;
       if (model_ >= MODEL_LAMINAR) {
         const amr_face_geometry_t& g = m->face_geometry[fi];
-        f_geo[6 * fi + 0] = (R)g.dx;
-        f_geo[6 * fi + 1] = (R)g.dy;
-        f_geo[6 * fi + 2] = (R)g.ex;
-        f_geo[6 * fi + 3] = (R)g.ey;
-        f_geo[6 * fi + 4] = (R)g.distance;
-        f_geo[6 * fi + 5] = (R)m->face_samples[fi].distance;
+        f_geo[6 * r + 0] = (R)g.dx;
+        f_geo[6 * r + 1] = (R)g.dy;
+        f_geo[6 * r + 2] = (R)g.ex;
+        f_geo[6 * r + 3] = (R)g.ey;
+        f_geo[6 * r + 4] = (R)g.distance;
+        f_geo[6 * r + 5] = (R)m->face_samples[fi].distance;
       }
     }
     c_slot[n] = sb + (int)ns;

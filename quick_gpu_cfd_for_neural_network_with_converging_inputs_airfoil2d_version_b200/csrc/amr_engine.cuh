@@ -1122,10 +1122,10 @@ template <class R, int MODEL> struct ItemSlots {
   const Dev<R>* d;
   bool base;
   __device__ __forceinline__ void operator()(int q, bool wall, R* col) const {
-    const int id = __ldg(d->s_item + q);
-    const R* src = (wall ? d->wval : d->fval) + SM_COLS * (long long)id;
+    const int id = __ldg(d->s_item + q);  // wall index, or 2 * face record + (cell is the face's left)
+    const R* src = wall ? d->wval + SM_COLS * (long long)id : d->fval + SM_COLS * (long long)(id >> 1);
     load_record<R, MODEL>(src, col, base);
-    const R sg = wall ? R(1) : ((__ldg(d->s_meta + q) & 1) ? R(1) : R(-1));
+    const R sg = (wall || (id & 1)) ? R(1) : R(-1);
     for (int v = 0; v < 4; ++v) col[v] = sg * col[v];
     if (MODEL >= MODEL_LAMINAR)
       for (int v = 4; v < 8; ++v) col[v] = sg * col[v];
