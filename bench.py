@@ -322,6 +322,45 @@ def reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_serving(args, rank, world, local):
+    """--serve: the served form.  Poisson request arrivals (seeded), host mesh builds on a thread
+    pool, admission while the arena has room, device steady-rule retirement or the step cap.
+    Each rank serves its shard on its own GPU; rank 0 prints one JSON line."""
+    from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200 import serve
+    reqs = serve.poisson_requests(args.requests, args.rate, args.seed)
+    mine = serve.shard(reqs, rank, world)
+    batch = Batch(precision=32, model=_abi.MODEL_LAMINAR, sa=True, max_cases=args.serve_cases,
+                  max_cells=args.serve_cases * 9800, device=local, launch_mode=_abi.LAUNCH_SPLIT, block_threads=128)
+    server = serve.Server(batch, max_steps=args.max_steps, trials=32, builder_threads=max(1, (os.cpu_count() or 2) - 1))
+    dist_barrier(world)
+    with ClockSampler(local) as clk:
+        results = server.run(mine)
+    wall = dist_max(server.wall_seconds, world)
+    cell_steps = dist_sum(server.cell_steps, world)
+    merged = serve.gather_results(results, world)
+    if rank == 0:
+        summary = serve.summarize(merged, wall, cell_steps)
+        line = dict(metric='served solves/s and p50/p99 latency (converged and capped apart)', impl='ours',
+                    value=summary['completed_per_s'], unit='solves/s', n_gpus=world, higher_is_better=True,
+                    scaling='weak', dtype='f32', data='synthetic',
+                    config=dict(workload='served-sa-fp32', requests=args.requests, rate_per_s=args.rate, seed=args.seed,
+                                max_steps=args.max_steps, profiles='LF1:LF2 1:1', arena_cases=args.serve_cases,
+                                meshes='native host builder, seeded NACA 4-digit draws'),
+                    serving=summary, polls=server.polls, clocks=clk.summary())
+        print(json.dumps(line), flush=True)
+    dist_barrier(world)
+
+
+def dist_sum(value, world):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -334,11 +373,20 @@ def main():
                     help='only the timed batched loop, with this launch mode and --block (for ncu)')
     ap.add_argument('--block', type=int, default=128)
     ap.add_argument('--precision', type=int, default=32, choices=[32, 64])
+    ap.add_argument('--serve', action='store_true', help='the served form: Poisson arrivals, p50/p99 latency')
+    ap.add_argument('--requests', type=int, default=200)
+    ap.add_argument('--rate', type=float, default=50.0)
+    ap.add_argument('--max-steps', type=int, default=3000)
+    ap.add_argument('--serve-cases', type=int, default=512)
+    ap.add_argument('--seed', type=int, default=20261203)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank, world, local = dist_setup(args.gpus)
     if args.impl == 'reference':
         reference_arm(args, rank, world)
+        return
+    if args.serve:
+        run_serving(args, rank, world, local)
         return
     case_list = batched_cases(args.cases, seed=20261203 + rank)
     if args.profile:

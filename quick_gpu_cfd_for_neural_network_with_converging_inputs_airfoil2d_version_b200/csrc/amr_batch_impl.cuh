@@ -186,10 +186,11 @@ template <class R> class Batch final : public BatchBase {
          f_own_.alloc(cap_faces_, A, error, "faces") && f_nb_.alloc(cap_faces_, A, error, "faces") &&
          f_meta_.alloc(cap_faces_, A, error, "faces") && f_len_.alloc(cap_faces_, A, error, "faces") &&
          f_geo_.alloc(6 * cap_faces_, A, error, "faces") && fval_.alloc(SM_COLS * cap_faces_, A, error, "faces") &&
-         w_owner_.alloc(cap_walls_, A, error, "walls") && wval_.alloc(SM_COLS * cap_walls_, A, error, "walls");
+         w_owner_.alloc(cap_walls_, A, error, "walls") && wval_.alloc(SM_COLS * cap_walls_, A, error, "walls") &&
+         live_end_.alloc(4, A, error, "ranges");
     if (!ok) return false;
     if (model_ >= MODEL_LAMINAR) {
-      ok = t_own_.alloc(cap_terms_, A, error, "terms") &&
+      ok = crec_.alloc(CREC * nc, A, error, "scratch") && t_own_.alloc(cap_terms_, A, error, "terms") &&
            t_src_.alloc(cap_terms_, A, error, "terms") && t_x_.alloc(cap_terms_, A, error, "terms") &&
            t_y_.alloc(cap_terms_, A, error, "terms") && grad_.alloc(4 * nc, A, error, "scratch") &&
            mu_.alloc(nc, A, error, "scratch") && eddy_.alloc(nc, A, error, "scratch");
@@ -205,6 +206,7 @@ template <class R> class Batch final : public BatchBase {
     cudaMemsetAsync(c_case_.p, 0xff, sizeof(int) * nc, stream_);
     cudaMemsetAsync(f_case_.p, 0xff, sizeof(int) * cap_faces_, stream_);
     cudaMemsetAsync(w_owner_.p, 0xff, sizeof(int) * cap_walls_, stream_);
+    cudaMemsetAsync(live_end_.p, 0, sizeof(int) * 4, stream_);
     if (!cuda_ok(cudaHostAlloc(reinterpret_cast<void**>(&h_ctl_), sizeof(CaseCtl) * c.max_cases, cudaHostAllocDefault), error,
                  "pinned control") ||
         !cuda_ok(cudaHostAlloc(reinterpret_cast<void**>(&h_bar_), sizeof(GridBarrier), cudaHostAllocDefault), error,
@@ -903,6 +905,13 @@ template <class R> class Batch final : public BatchBase {
         hw_faces_ = std::max(hw_faces_, c.faces.b + c.faces.n);
         hw_walls_ = std::max(hw_walls_, c.walls.b + c.walls.n);
       }
+    h_live_end_[0] = (int)hw_cells_;
+    h_live_end_[1] = (int)hw_faces_;
+    h_live_end_[2] = (int)hw_walls_;
+    h_live_end_[3] = 0;
+    if (!cuda_ok(cudaMemcpyAsync(live_end_.p, h_live_end_, sizeof(h_live_end_), cudaMemcpyHostToDevice, stream_), error,
+                 "live ranges"))
+      return false;
     if (!all.empty() && !cuda_ok(cudaMemcpyAsync(tiles_.p, all.data(), sizeof(Tile) * all.size(), cudaMemcpyHostToDevice,
                                                  stream_), error, "tiles"))
       return false;
@@ -911,7 +920,9 @@ template <class R> class Batch final : public BatchBase {
       return false;
     case_tile_ranges_ = ranges;
     tiles_dirty_ = false;
-    graph_dirty_ = true;
+    // a split-mode graph reads the live ranges from the device and keeps its grids; it is
+    // recaptured only when the set of kernels changes (SRD launches appear or vanish)
+    if (mode_ != AMR_B200_LAUNCH_SPLIT || any_srd() != graph_srd_) graph_dirty_ = true;
     return cuda_ok(cudaStreamSynchronize(stream_), error, "tiles sync");
   }
 
@@ -976,6 +987,10 @@ template <class R> class Batch final : public BatchBase {
     d.s_item = s_item_.p;
     d.fval = fval_.p;
     d.wval = wval_.p;
+    d.crec = crec_.p;
+    d.live_end = live_end_.p;
+    d.cap_faces = (int)cap_faces_;
+    d.cap_walls = (int)cap_walls_;
     d.n_faces = (int)hw_faces_;
     d.n_walls = (int)hw_walls_;
     d.n_cells = (int)hw_cells_;
@@ -1023,7 +1038,7 @@ template <class R> class Batch final : public BatchBase {
       ok = ok && cuda_ok(EngineOps<R>::launch_phases(dev(), model_, flux_, any_srd(), trials, mode, block_, stream_), error,
                          "phase kernel launch");
     } else if (mode_ == AMR_B200_LAUNCH_SPLIT) {
-      ok = ok && cuda_ok(EngineOps<R>::launch_split(dev(), model_, flux_, any_srd(), trials, mode, stream_), error,
+      ok = ok && cuda_ok(EngineOps<R>::launch_split(dev(), model_, flux_, any_srd(), trials, mode, stream_, sms_), error,
                          "split kernel launch");
     } else {
       const int grid = mode == MODE_RESIDUAL ? std::min(grid_, std::max(1, (n_tiles_ + block_ / 32 - 1) / (block_ / 32))) : grid_;
@@ -1067,6 +1082,7 @@ template <class R> class Batch final : public BatchBase {
     cudaGraphGetNodes(graph_, nullptr, &nodes);
     graph_nodes_ = nodes;
     graph_trials_ = trials;
+    graph_srd_ = any_srd();
     graph_dirty_ = false;
     return true;
   }
@@ -1095,7 +1111,7 @@ template <class R> class Batch final : public BatchBase {
     c_term_.free(); c_cx_.free(); c_cy_.free(); c_wd_.free();
     s_own_.free(); s_nb_.free(); s_meta_.free(); s_len_.free(); s_geo_.free(); s_item_.free();
     f_case_.free(); f_own_.free(); f_nb_.free(); f_meta_.free(); f_len_.free(); f_geo_.free(); fval_.free();
-    w_owner_.free(); wval_.free();
+    w_owner_.free(); wval_.free(); crec_.free(); live_end_.free();
     w_nx_.free(); w_ny_.free(); w_len_.free(); w_dist_.free(); w_donor_.free(); w_xm_.free(); w_ym_.free();
     t_own_.free(); t_src_.free(); t_x_.free(); t_y_.free();
     g_mem_.free(); g_cell_.free(); g_cnt_.free(); g_vol_.free(); q_cell_.free(); q_grp_.free(); q_list_.free(); q_cnt_.free();
@@ -1109,6 +1125,9 @@ template <class R> class Batch final : public BatchBase {
   int block_ = 256, grid_ = 0, max_grid_ = 0, grid_request_ = 0;
   int mode_ = AMR_B200_LAUNCH_PERSISTENT;  // persistent cooperative kernel, one kernel per phase, or split
   long long hw_cells_ = 0, hw_faces_ = 0, hw_walls_ = 0;
+  int h_live_end_[4] = {0, 0, 0, 0};
+  bool graph_srd_ = false;
+  DevBuf<int> live_end_;
   long long cap_faces_ = 0;
   RangeAlloc a_faces_;
   long long cap_cells_ = 0, cap_slots_ = 0, cap_walls_ = 0, cap_terms_ = 0, cap_groups_ = 0, cap_gmem_ = 0, cap_q_ = 0,
@@ -1140,7 +1159,7 @@ template <class R> class Batch final : public BatchBase {
   DevBuf<int> s_own_, s_nb_, s_meta_, s_item_;
   DevBuf<R> s_len_, s_geo_;
   DevBuf<int> f_case_, f_own_, f_nb_, f_meta_, w_owner_;
-  DevBuf<R> f_len_, f_geo_, fval_, wval_;
+  DevBuf<R> f_len_, f_geo_, fval_, wval_, crec_;
   DevBuf<R> w_nx_, w_ny_, w_len_, w_dist_;
   DevBuf<double> w_xm_, w_ym_;
   DevBuf<int> w_donor_;

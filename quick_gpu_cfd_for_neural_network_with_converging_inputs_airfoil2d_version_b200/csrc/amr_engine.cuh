@@ -65,7 +65,8 @@ constexpr int SLOT_WALL = 1 << 9;  // s_meta flag: the slot is a wall fragment o
 // A tile is processed by one warp: at most TILE_W slots and TILE_W gradient terms of whole cells,
 // synchronised by __syncwarp only, so the warps of a block never wait for one another.
 constexpr int TILE_W = 32;
-constexpr int SM_COLS = 12;  // shared-memory columns per slot
+constexpr int SM_COLS = 12;
+constexpr int CREC = 16;  // values in a packed cell record  // shared-memory columns per slot
 constexpr unsigned FULL_MASK = 0xffffffffu;
 
 struct GridBarrier {
@@ -142,7 +143,11 @@ template <class R> struct Dev {
   const int* s_item;
   R* fval;          // 12 per face
   R* wval;          // 12 per wall
-  int n_faces, n_walls, n_cells;  // ends of the live face, wall and cell ranges
+  R* crec;          // CREC per cell: packed state and gradient-phase fields (viscous models)
+  int n_faces, n_walls, n_cells;  // ends of the live face, wall and cell ranges (host copy)
+  int cap_faces, cap_walls;       // record capacities
+  const int* live_end;            // the same on the device: cells, faces, walls (read by the
+                                  // graph-replayed kernels, so a graph outlives case changes)
   GridBarrier* bar;
   unsigned long long barrier_cycles;
 };
@@ -233,36 +238,113 @@ template <class R> struct Smem {
   R* a;  // [12][blockDim]
 };
 
+// A face or wall record is 12 values: flux 0-3, viscous flux 4-7, convective and viscous
+// spectral radius 8-9, SA flux 10 and SA spectral term 11.  Records are 16-byte aligned and
+// moved as 16-byte vectors; a model moves only the groups it uses (columns 8-11 ride with
+// the spectral radius, which only the base stage needs beyond column 10).
+template <class R> struct Vec16;
+template <> struct Vec16<float> { using T = float4; static constexpr int n = 4; };
+template <> struct Vec16<double> { using T = double2; static constexpr int n = 2; };
+
+template <class R> __device__ __forceinline__ void store_group(R* dst, const R* src) {
+  using V = typename Vec16<R>::T;
+  constexpr int m = Vec16<R>::n;
+#pragma unroll
+  for (int j = 0; j < 4 / m; ++j) {
+    V v;
+    R* e = reinterpret_cast<R*>(&v);
+#pragma unroll
+    for (int i = 0; i < m; ++i) e[i] = src[j * m + i];
+    reinterpret_cast<V*>(dst)[j] = v;
+  }
+}
+
+template <class R> __device__ __forceinline__ void load_group(const R* src, R* dst) {
+  using V = typename Vec16<R>::T;
+  constexpr int m = Vec16<R>::n;
+#pragma unroll
+  for (int j = 0; j < 4 / m; ++j) {
+    const V v = __ldg(reinterpret_cast<const V*>(src) + j);
+    const R* e = reinterpret_cast<const R*>(&v);
+#pragma unroll
+    for (int i = 0; i < m; ++i) dst[j * m + i] = e[i];
+  }
+}
+
+
+// A packed cell record (split mode, viscous models) is CREC values, 16-byte aligned, moved as
+// 16-byte vectors: state 0-4, gradient 5-8, mu 9, eddy 10, SA phi gradient 11-12, SA diffusion
+// 13.  A laminar model uses the first twelve only.
+template <class R, int MODEL> __device__ __forceinline__ void store_cell_record(R* dst, const R* c) {
+  store_group(dst, c);
+  store_group(dst + 4, c + 4);
+  store_group(dst + 8, c + 8);
+  if (MODEL == MODEL_SA) store_group(dst + 12, c + 12);
+}
+
+template <class R, int MODEL> __device__ __forceinline__ void load_cell_record(const R* src, R* c) {
+  load_group(src, c);
+  load_group(src + 4, c + 4);
+  load_group(src + 8, c + 8);
+  if (MODEL == MODEL_SA) {
+    load_group(src + 12, c + 12);
+  } else {
+    c[4] = c[11] = c[12] = c[13] = R(0);
+  }
+}
+
+
 // ------------------------------------------------------------------------------------------
 // G phase: velocity gradients, viscosity, eddy viscosity, SA gradients and point model of
 // every cell of a tile (reference src/static_amr2d_viscous.cpp:166-174, src/static_amr2d_sa.cpp:74-80).
 // ------------------------------------------------------------------------------------------
 // Cell part of the G phase from the summed LSQ contributions gr (velocity) and sg (SA phi and
 // density): viscosity, eddy viscosity, SA point model and source.  Returns false on failure.
+// With soa the per-cell fields go to the SoA scratch arrays; with rec (split mode) they also go
+// to the cell's packed record: state 0-4, gradient 5-8, mu 9, eddy 10, SA phi gradient 11-12,
+// SA diffusion 13.
 template <class R, int MODEL>
 __device__ __forceinline__ bool grad_finish(const Dev<R>& d, const CaseCfg<R>& cf, int k, const R* Uin, const R* gr,
-                                            const R* sg) {
+                                            const R* sg, bool soa = true, R* rec = nullptr) {
   const long long n = d.ncap;
   const Prim<R> w = prim(Uin, n, k, cf.gamma);
   const R mu = dyn_visc(cf.trn, w.p / (w.rho * cf.trn.gas_constant));
   bool bad = !(mu > R(0)) || !isfinite(mu);
-  for (int v = 0; v < 4; ++v) d.grad[v * n + k] = gr[v];
-  d.mu[k] = mu;
-  R eddy = 0;
+  if (soa) {
+    for (int v = 0; v < 4; ++v) d.grad[v * n + k] = gr[v];
+    d.mu[k] = mu;
+  }
+  R eddy = 0, sdiff = 0;
   if (MODEL == MODEL_SA) {
     const R ph = Uin[4 * n + k] / w.rho;
     if (!isfinite(ph)) bad = true;
     eddy = w.rho * sa_eddy(ph, mu / w.rho);
     const SaPoint<R> pt = sa_neg(ph, mu / w.rho, d.c_wd[k], R(fabs(gr[2] - gr[1])));
     const R src = sa_corrected_source(pt, w.rho, sg[0], sg[1], sg[2], sg[3]);
-    d.sgrad[k] = sg[0];
-    d.sgrad[n + k] = sg[1];
-    d.sdiff[k] = pt.diffusion;
+    if (soa) {
+      d.sgrad[k] = sg[0];
+      d.sgrad[n + k] = sg[1];
+      d.sdiff[k] = pt.diffusion;
+    }
+    sdiff = pt.diffusion;
     d.ssrc[k] = src;
     d.srate[k] = pt.source_rate;
     if (!(pt.diffusion > R(0)) || !isfinite(src) || !isfinite(pt.source_rate)) bad = true;
   }
-  d.eddy[k] = eddy;
+  if (soa) d.eddy[k] = eddy;
+  if (rec) {
+    R c[CREC];
+    for (int v = 0; v < 4; ++v) c[v] = Uin[v * n + k];
+    c[4] = MODEL == MODEL_SA ? Uin[4 * n + k] : R(0);
+    for (int v = 0; v < 4; ++v) c[5 + v] = gr[v];
+    c[9] = mu;
+    c[10] = eddy;
+    c[11] = MODEL == MODEL_SA ? sg[0] : R(0);
+    c[12] = MODEL == MODEL_SA ? sg[1] : R(0);
+    c[13] = sdiff;
+    c[14] = c[15] = R(0);
+    store_cell_record<R, MODEL>(rec, c);
+  }
   return !bad;
 }
 
@@ -334,30 +416,76 @@ __device__ void phase_gradients(const Dev<R>& d, const Tile& t, const R* Uin, R*
 // dst[c*stride]: conserved flux (4), viscous flux (4), speed*length, viscous spectral coefficient,
 // SA flux, SA spectral coefficient.  With signed = true the flux columns carry the orientation
 // sign of cell k (slot form); otherwise they are in face orientation (item form).
+// Everything one face's fluxes read: both cells' states and (viscous) gradients, viscosities,
+// SA fields and the fixed face geometry.  k is the slot's cell, m the other cell (k itself
+// outside the domain).
+template <class R> struct FaceIn {
+  R uk[5], um[5], gk[4], gm[4], geo[6];
+  R mk, mm, ek, em, sgk[2], sgm[2], sdk, sdm;
+};
+
+// Loads a FaceIn from the SoA state and scratch arrays.  Every load is issued up front and
+// unconditionally (an exterior face reads its own cell twice), so the whole neighbourhood
+// arrives in one memory round trip.
+template <class R, int MODEL>
+__device__ __forceinline__ void face_in_soa(const Dev<R>& d, const R* gp, int k, int m, const R* Uin, FaceIn<R>& f) {
+  const long long n = d.ncap;
+  for (int v = 0; v < 4; ++v) { f.uk[v] = Uin[v * n + k]; f.um[v] = Uin[v * n + m]; }
+  if (MODEL == MODEL_SA) { f.uk[4] = Uin[4 * n + k]; f.um[4] = Uin[4 * n + m]; }
+  f.mk = f.mm = f.ek = f.em = f.sdk = f.sdm = 0;
+  f.sgk[0] = f.sgk[1] = f.sgm[0] = f.sgm[1] = 0;
+  if (MODEL >= MODEL_LAMINAR) {
+    for (int v = 0; v < 4; ++v) { f.gk[v] = d.grad[v * n + k]; f.gm[v] = d.grad[v * n + m]; }
+    f.mk = d.mu[k]; f.mm = d.mu[m]; f.ek = d.eddy[k]; f.em = d.eddy[m];
+    for (int v = 0; v < 6; ++v) f.geo[v] = __ldg(gp + v);
+    if (MODEL == MODEL_SA) {
+      f.sgk[0] = d.sgrad[k]; f.sgk[1] = d.sgrad[n + k]; f.sgm[0] = d.sgrad[m]; f.sgm[1] = d.sgrad[n + m];
+      f.sdk = d.sdiff[k]; f.sdm = d.sdiff[m];
+    }
+  }
+}
+
+// Loads a FaceIn from the two cells' packed records (split mode, viscous models).
+template <class R, int MODEL>
+__device__ __forceinline__ void face_in_records(const Dev<R>& d, const R* gp, int k, int m, FaceIn<R>& f) {
+  R a[CREC], b[CREC];
+  load_cell_record<R, MODEL>(d.crec + CREC * (long long)k, a);
+  load_cell_record<R, MODEL>(d.crec + CREC * (long long)m, b);
+  for (int v = 0; v < 5; ++v) { f.uk[v] = a[v]; f.um[v] = b[v]; }
+  for (int v = 0; v < 4; ++v) { f.gk[v] = a[5 + v]; f.gm[v] = b[5 + v]; }
+  f.mk = a[9]; f.mm = b[9]; f.ek = a[10]; f.em = b[10];
+  f.sgk[0] = a[11]; f.sgk[1] = a[12]; f.sgm[0] = b[11]; f.sgm[1] = b[12];
+  f.sdk = a[13]; f.sdm = b[13];
+  for (int v = 0; v < 6; ++v) f.geo[v] = __ldg(gp + v);
+}
+
+template <class R, int MODEL, int FLUX>
+__device__ __forceinline__ void face_fluxes(const CaseCfg<R>& cf, const FaceIn<R>& f, R len, int nb, int meta, bool base,
+                                            R* dst, int stride, bool signed_out, bool& bad);
+
 template <class R, int MODEL, int FLUX>
 __device__ __forceinline__ void slot_face(const Dev<R>& d, const CaseCfg<R>& cf, const R* gp, R len, int k, int nb,
                                           int meta, const R* Uin, bool base, R* dst, int stride, bool signed_out,
                                           bool& bad) {
-  const long long n = d.ncap;
+  FaceIn<R> f;
+  face_in_soa<R, MODEL>(d, gp, k, nb >= 0 ? nb : k, Uin, f);
+  face_fluxes<R, MODEL, FLUX>(cf, f, len, nb, meta, base, dst, stride, signed_out, bad);
+}
+
+template <class R, int MODEL, int FLUX>
+__device__ __forceinline__ void face_fluxes(const CaseCfg<R>& cf, const FaceIn<R>& f, R len, int nb, int meta, bool base,
+                                            R* dst, int stride, bool signed_out, bool& bad) {
   const R g = cf.gamma;
   const bool own_left = meta & 1;
   const int axis = (meta >> 1) & 1, side = ((meta >> 2) & 7) - 1, kind = (meta >> 5) & 15;
-  // Every load of this slot is issued up front and unconditionally (an exterior face reads its
-  // own cell twice), so the whole neighbourhood arrives in one memory round trip.
-  const int m = nb >= 0 ? nb : k;
-  R uk[5], um[5];
-  for (int v = 0; v < 4; ++v) { uk[v] = Uin[v * n + k]; um[v] = Uin[v * n + m]; }
-  if (MODEL == MODEL_SA) { uk[4] = Uin[4 * n + k]; um[4] = Uin[4 * n + m]; }
-  R gk[4], gm[4], geo[6], mk = 0, mm = 0, ek = 0, em = 0, sgk[2] = {0, 0}, sgm[2] = {0, 0}, sdk = 0, sdm = 0;
-  if (MODEL >= MODEL_LAMINAR) {
-    for (int v = 0; v < 4; ++v) { gk[v] = d.grad[v * n + k]; gm[v] = d.grad[v * n + m]; }
-    mk = d.mu[k]; mm = d.mu[m]; ek = d.eddy[k]; em = d.eddy[m];
-    for (int v = 0; v < 6; ++v) geo[v] = __ldg(gp + v);
-    if (MODEL == MODEL_SA) {
-      sgk[0] = d.sgrad[k]; sgk[1] = d.sgrad[n + k]; sgm[0] = d.sgrad[m]; sgm[1] = d.sgrad[n + m];
-      sdk = d.sdiff[k]; sdm = d.sdiff[m];
-    }
-  }
+  const R* uk = f.uk;
+  const R* um = f.um;
+  const R* gk = f.gk;
+  const R* gm = f.gm;
+  const R* geo = f.geo;
+  const R mk = f.mk, mm = f.mm, ek = f.ek, em = f.em, sdk = f.sdk, sdm = f.sdm;
+  const R* sgk = f.sgk;
+  const R* sgm = f.sgm;
   Prim<R> wk, wn;
   wk.rho = uk[0]; wk.u = uk[1] / uk[0]; wk.v = uk[2] / uk[0]; wk.p = (g - R(1)) * (uk[3] - R(0.5) * (uk[1] * wk.u + uk[2] * wk.v));
   wn.rho = um[0]; wn.u = um[1] / um[0]; wn.v = um[2] / um[0]; wn.p = (g - R(1)) * (um[3] - R(0.5) * (um[1] * wn.u + um[2] * wn.v));
@@ -474,20 +602,64 @@ __device__ __forceinline__ void slot_face(const Dev<R>& d, const CaseCfg<R>& cf,
 // A wall fragment of cell k: pressure force (reference src/static_amr2d.cpp:193-195), viscous wall
 // flux from the visible donor (src/static_amr2d_viscous.cpp:192-196) and the SA wall flux
 // (src/static_amr2d_sa.cpp:91), with their spectral-radius contributions.
+// The owner's conserved state and viscosity, the donor's state and viscosity.
+template <class R> struct WallIn {
+  R uk[4], ud[5], mk, md;
+};
+
+template <class R, int MODEL>
+__device__ __forceinline__ void wall_fluxes(const CaseCfg<R>& cf, const WallIn<R>& w, R nx, R ny, R wdist, R wl, bool base,
+                                            R* dst, int stride, bool& bad);
+
 template <class R, int MODEL>
 __device__ __forceinline__ void slot_wall(const Dev<R>& d, const CaseCfg<R>& cf, R nx, R ny, R wdist, R wl, int k, int dn,
                                           const R* Uin, bool base, R* dst, int stride, bool& bad) {
   const long long n = d.ncap;
+  WallIn<R> w;
+  for (int v = 0; v < 4; ++v) w.uk[v] = Uin[v * n + k];
+  w.mk = w.md = 0;
+  w.ud[0] = w.ud[1] = w.ud[2] = w.ud[3] = w.ud[4] = 0;
+  if (MODEL >= MODEL_LAMINAR) {
+    for (int v = 0; v < 3; ++v) w.ud[v] = Uin[v * n + dn];
+    if (MODEL == MODEL_SA) w.ud[4] = Uin[4 * n + dn];
+    w.md = d.mu[dn];
+    w.mk = d.mu[k];
+  }
+  wall_fluxes<R, MODEL>(cf, w, nx, ny, wdist, wl, base, dst, stride, bad);
+}
+
+// The same from the packed cell records of the owner and the donor (split mode, viscous models).
+template <class R, int MODEL>
+__device__ __forceinline__ void slot_wall_records(const Dev<R>& d, const CaseCfg<R>& cf, R nx, R ny, R wdist, R wl, int k,
+                                                  int dn, bool base, R* dst, int stride, bool& bad) {
+  R a[CREC], b[CREC];
+  load_cell_record<R, MODEL>(d.crec + CREC * (long long)k, a);
+  load_cell_record<R, MODEL>(d.crec + CREC * (long long)dn, b);
+  WallIn<R> w;
+  for (int v = 0; v < 4; ++v) w.uk[v] = a[v];
+  for (int v = 0; v < 5; ++v) w.ud[v] = b[v];
+  w.mk = a[9];
+  w.md = b[9];
+  wall_fluxes<R, MODEL>(cf, w, nx, ny, wdist, wl, base, dst, stride, bad);
+}
+
+template <class R, int MODEL>
+__device__ __forceinline__ void wall_fluxes(const CaseCfg<R>& cf, const WallIn<R>& w, R nx, R ny, R wdist, R wl, bool base,
+                                            R* dst, int stride, bool& bad) {
   const R g = cf.gamma;
-  const Prim<R> wk = prim(Uin, n, k, g);
+  Prim<R> wk;
+  wk.rho = w.uk[0];
+  wk.u = w.uk[1] / w.uk[0];
+  wk.v = w.uk[2] / w.uk[0];
+  wk.p = (g - R(1)) * (w.uk[3] - R(0.5) * (w.uk[1] * wk.u + w.uk[2] * wk.v));
   dst[0 * stride] = 0;
   dst[1 * stride] = wk.p * nx * wl;
   dst[2 * stride] = wk.p * ny * wl;
   dst[3 * stride] = 0;
   if (base) dst[8 * stride] = sqrt(g * wk.p / wk.rho) * wl;
   if (MODEL >= MODEL_LAMINAR) {
-    const R rd = Uin[dn], ud = Uin[n + dn] / rd, vd = Uin[2 * n + dn] / rd;
-    const R md = d.mu[dn];
+    const R rd = w.ud[0], ud = w.ud[1] / rd, vd = w.ud[2] / rd;
+    const R md = w.md;
     R gw[4], fw[4];
     wall_gradient(nx, ny, wdist, -ud, -vd, gw);
     visc_flux(md, gw, nx, ny, R(0), R(0), fw);
@@ -495,10 +667,10 @@ __device__ __forceinline__ void slot_wall(const Dev<R>& d, const CaseCfg<R>& cf,
       if (!isfinite(fw[v])) bad = true;
       dst[(4 + v) * stride] = fw[v] * wl;
     }
-    if (base) dst[9 * stride] = R(4.0 / 3) * rmax(md / rd, d.mu[k] / wk.rho) / wdist * wl;
+    if (base) dst[9 * stride] = R(4.0 / 3) * rmax(md / rd, w.mk / wk.rho) / wdist * wl;
     if (MODEL == MODEL_SA) {
       const R swc = md / R(AMRB_SIG) / wdist * wl;
-      dst[10 * stride] = -swc * (Uin[4 * n + dn] / rd);
+      dst[10 * stride] = -swc * (w.ud[4] / rd);
       if (base) dst[11 * stride] = swc;
     }
   }
@@ -943,8 +1115,9 @@ __global__ void __launch_bounds__(PHASE_BLOCK, PhaseOcc<R>::flux) phase_flux_ker
 // U1 = U + dt R0, one thread per cell (phase mode).  Every thread derives its case's step size
 // from the control record; the first cell of each case records it.
 template <class R, int MODEL>
-__global__ void __launch_bounds__(MAX_BLOCK) phase_first_cells_kernel(Dev<R> d, int ncells) {
+__global__ void __launch_bounds__(MAX_BLOCK) phase_first_cells_kernel(Dev<R> d) {
   const long long n = d.ncap;
+  const int ncells = d.live_end[0];
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ncells; k += gridDim.x * blockDim.x) {
     const int cs = d.c_case[k];
     if (cs < 0) continue;
@@ -1004,45 +1177,15 @@ static __global__ void phase_commit_kernel(CaseCtl* ctl, int n_cases, int begin_
 #ifndef AMRB_SPLIT_MINB_F32
 #define AMRB_SPLIT_MINB_F32 8
 #endif
+#ifndef AMRB_SPLIT_CELL_MINB_F32
+#define AMRB_SPLIT_CELL_MINB_F32 12
+#endif
 template <class R> struct SplitOcc;
-template <> struct SplitOcc<float> { static constexpr int item = AMRB_SPLIT_MINB_F32, cell = 8; };
+template <> struct SplitOcc<float> { static constexpr int item = AMRB_SPLIT_MINB_F32, cell = AMRB_SPLIT_CELL_MINB_F32; };
 template <> struct SplitOcc<double> { static constexpr int item = 3, cell = 4; };
 
 __device__ __forceinline__ int stage_rule(int stage) {
   return stage == STAGE_DIAG ? SKIP_LIVE : (stage == STAGE_BASE ? SKIP_ACTIVE : SKIP_STAGE);
-}
-
-// A face or wall record is 12 values: flux 0-3, viscous flux 4-7, convective and viscous
-// spectral radius 8-9, SA flux 10 and SA spectral term 11.  Records are 16-byte aligned and
-// moved as 16-byte vectors; a model moves only the groups it uses (columns 8-11 ride with
-// the spectral radius, which only the base stage needs beyond column 10).
-template <class R> struct Vec16;
-template <> struct Vec16<float> { using T = float4; static constexpr int n = 4; };
-template <> struct Vec16<double> { using T = double2; static constexpr int n = 2; };
-
-template <class R> __device__ __forceinline__ void store_group(R* dst, const R* src) {
-  using V = typename Vec16<R>::T;
-  constexpr int m = Vec16<R>::n;
-#pragma unroll
-  for (int j = 0; j < 4 / m; ++j) {
-    V v;
-    R* e = reinterpret_cast<R*>(&v);
-#pragma unroll
-    for (int i = 0; i < m; ++i) e[i] = src[j * m + i];
-    reinterpret_cast<V*>(dst)[j] = v;
-  }
-}
-
-template <class R> __device__ __forceinline__ void load_group(const R* src, R* dst) {
-  using V = typename Vec16<R>::T;
-  constexpr int m = Vec16<R>::n;
-#pragma unroll
-  for (int j = 0; j < 4 / m; ++j) {
-    const V v = __ldg(reinterpret_cast<const V*>(src) + j);
-    const R* e = reinterpret_cast<const R*>(&v);
-#pragma unroll
-    for (int i = 0; i < m; ++i) dst[j * m + i] = e[i];
-  }
 }
 
 template <class R, int MODEL> __device__ __forceinline__ void store_record(R* dst, R* rec, bool base) {
@@ -1061,8 +1204,9 @@ template <class R, int MODEL> __device__ __forceinline__ void load_record(const 
 }
 
 template <class R, int MODEL>
-__global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::cell) grad_cells_kernel(Dev<R> d, int stage, int ncells) {
+__global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::cell) grad_cells_kernel(Dev<R> d, int stage) {
   const int rule = stage_rule(stage);
+  const int ncells = d.live_end[0];
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ncells; k += gridDim.x * blockDim.x) {
     const int cs = d.c_case[k];
     if (cs < 0) continue;
@@ -1078,7 +1222,9 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::cell) grad_cells_ker
       if (MODEL == MODEL_SA)
         for (int v = 0; v < 4; ++v) sg[v] += t[4 + v];
     }
-    if (!grad_finish<R, MODEL>(d, cf, k, Uin, gr, sg)) atomicOr(&d.ctl[cs].bad, 1);
+    // the packed record feeds the item kernel; the SoA copies only the residual-mode loads
+    if (!grad_finish<R, MODEL>(d, cf, k, Uin, gr, sg, stage == STAGE_DIAG, d.crec + CREC * (long long)k))
+      atomicOr(&d.ctl[cs].bad, 1);
   }
 }
 
@@ -1086,31 +1232,41 @@ template <class R, int MODEL, int FLUX>
 __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::item) item_kernel(Dev<R> d, int stage) {
   const int rule = stage_rule(stage);
   const bool base = stage == STAGE_BASE;
-  const int total = d.n_faces + d.n_walls;
+  const int nf = d.live_end[1], total = nf + d.live_end[2];
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
     bool bad = false;
     int cs;
-    if (idx < d.n_faces) {
+    if (idx < nf) {
       const int f = idx;
       cs = d.f_case[f];
       if (cs < 0) continue;
       const CaseCtl& c = d.ctl[cs];
       if (skip_case(c, rule)) continue;
       R rec[SM_COLS];
-      slot_face<R, MODEL, FLUX>(d, d.cfg[cs], d.f_geo + 6 * (long long)f, __ldg(d.f_len + f), __ldg(d.f_own + f),
-                                __ldg(d.f_nb + f), __ldg(d.f_meta + f), stage_input(d, stage, c.cur), base, rec, 1,
-                                false, bad);
+      const int own = __ldg(d.f_own + f), nb = __ldg(d.f_nb + f);
+      if (MODEL >= MODEL_LAMINAR) {
+        FaceIn<R> in;
+        face_in_records<R, MODEL>(d, d.f_geo + 6 * (long long)f, own, nb >= 0 ? nb : own, in);
+        face_fluxes<R, MODEL, FLUX>(d.cfg[cs], in, __ldg(d.f_len + f), nb, __ldg(d.f_meta + f), base, rec, 1, false, bad);
+      } else {
+        slot_face<R, MODEL, FLUX>(d, d.cfg[cs], d.f_geo + 6 * (long long)f, __ldg(d.f_len + f), own, nb,
+                                  __ldg(d.f_meta + f), stage_input(d, stage, c.cur), base, rec, 1, false, bad);
+      }
       store_record<R, MODEL>(d.fval + SM_COLS * (long long)f, rec, base);
     } else {
-      const int w = idx - d.n_faces;
+      const int w = idx - nf;
       const int owner = d.w_owner[w];
       if (owner < 0) continue;
       cs = d.c_case[owner];
       const CaseCtl& c = d.ctl[cs];
       if (skip_case(c, rule)) continue;
       R rec[SM_COLS];
-      slot_wall<R, MODEL>(d, d.cfg[cs], __ldg(d.w_nx + w), __ldg(d.w_ny + w), __ldg(d.w_dist + w), __ldg(d.w_len + w),
-                          owner, __ldg(d.w_donor + w), stage_input(d, stage, c.cur), base, rec, 1, bad);
+      if (MODEL >= MODEL_LAMINAR)
+        slot_wall_records<R, MODEL>(d, d.cfg[cs], __ldg(d.w_nx + w), __ldg(d.w_ny + w), __ldg(d.w_dist + w),
+                                    __ldg(d.w_len + w), owner, __ldg(d.w_donor + w), base, rec, 1, bad);
+      else
+        slot_wall<R, MODEL>(d, d.cfg[cs], __ldg(d.w_nx + w), __ldg(d.w_ny + w), __ldg(d.w_dist + w), __ldg(d.w_len + w),
+                            owner, __ldg(d.w_donor + w), stage_input(d, stage, c.cur), base, rec, 1, bad);
       store_record<R, MODEL>(d.wval + SM_COLS * (long long)w, rec, base);
     }
     if (bad && stage != STAGE_DIAG) atomicOr(&d.ctl[cs].bad, 1);
@@ -1134,8 +1290,9 @@ template <class R, int MODEL> struct ItemSlots {
 };
 
 template <class R, int MODEL>
-__global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::cell) gather_kernel(Dev<R> d, int stage, int ncells) {
+__global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::cell) gather_kernel(Dev<R> d, int stage) {
   const int rule = stage_rule(stage);
+  const int ncells = d.live_end[0];
   const bool base = stage == STAGE_BASE;
   const int lane = threadIdx.x & 31;
   // the loop bound is warp-uniform so the segmented shuffles below see full warps
@@ -1177,7 +1334,7 @@ template <class R> struct EngineOps {
                                    cudaStream_t stream);
   // The same with the split kernels (gradients per cell, fluxes per face record, gather per cell).
   static cudaError_t launch_split(const Dev<R>& d, int model, int flux, bool srd, int trials, int mode,
-                                  cudaStream_t stream);
+                                  cudaStream_t stream, int sms);
   static cudaError_t occupancy(int model, int flux, bool srd, int block, int* blocks_per_sm);
   static size_t smem_bytes(int block) { return size_t(12) * block * sizeof(R); }
 };

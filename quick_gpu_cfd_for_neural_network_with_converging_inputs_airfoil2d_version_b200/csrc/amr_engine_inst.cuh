@@ -49,7 +49,7 @@ static cudaError_t launch_phases_t(const Dev<R>& d, bool srd, int trials, int mo
   for (int t = 0; t < trials; ++t) {
     if (MODEL >= MODEL_LAMINAR) phase_grad_kernel<R, MODEL><<<tiles, block, sm, st>>>(d, STAGE_BASE);
     phase_flux_kernel<R, MODEL, FLUX><<<tiles, block, sm, st>>>(d, STAGE_BASE);
-    phase_first_cells_kernel<R, MODEL><<<(d.n_cells + 255) / 256 + 1, 256, 0, st>>>(d, d.n_cells);
+    phase_first_cells_kernel<R, MODEL><<<(d.n_cells + 255) / 256 + 1, 256, 0, st>>>(d);
     for (int stage = 1; stage <= 2; ++stage) {
       if (srd) phase_srd_kernel<R, MODEL><<<cases, block, 0, st>>>(d, stage);
       if (MODEL >= MODEL_LAMINAR) phase_grad_kernel<R, MODEL><<<tiles, block, sm, st>>>(d, stage);
@@ -74,18 +74,21 @@ cudaError_t EngineOps<R>::launch_phases(const Dev<R>& d, int model, int flux, bo
                            : launch_phases_t<R, MODEL_SA, FLUX_AUSM>(d, srd, trials, mode, block, stream);
 }
 
+// Grids are fixed by the arena's capacity (grid-stride loops over the live ranges, which the
+// kernels read from the device), so a captured graph stays valid when cases come and go.
 template <class R, int MODEL, int FLUX>
-static cudaError_t launch_split_t(const Dev<R>& d, bool srd, int trials, int mode, cudaStream_t st) {
+static cudaError_t launch_split_t(const Dev<R>& d, bool srd, int trials, int mode, cudaStream_t st, int sms) {
   const int B = PHASE_BLOCK;
-  const int ncells = d.n_cells;
-  const int cblocks = (ncells + B - 1) / B + (ncells == 0);
-  const int iblocks = (d.n_faces + d.n_walls + B - 1) / B + (d.n_faces + d.n_walls == 0);
+  const long long ncap = d.ncap, icap = (long long)d.cap_faces + d.cap_walls;
+  const int cblocks = (int)std::min<long long>((ncap + B - 1) / B, (long long)sms * SplitOcc<R>::cell);
+  const int iblocks = (int)std::min<long long>((icap + B - 1) / B, (long long)sms * SplitOcc<R>::item);
+  const int fblocks = (int)std::min<long long>((ncap + 255) / 256, (long long)sms * 8);
   const int cases = d.n_cases;
   const int kblocks = (cases + 127) / 128;
   auto stage_seq = [&](int stage) {
-    if (MODEL >= MODEL_LAMINAR) grad_cells_kernel<R, MODEL><<<cblocks, B, 0, st>>>(d, stage, ncells);
+    if (MODEL >= MODEL_LAMINAR) grad_cells_kernel<R, MODEL><<<cblocks, B, 0, st>>>(d, stage);
     item_kernel<R, MODEL, FLUX><<<iblocks, B, 0, st>>>(d, stage);
-    gather_kernel<R, MODEL><<<cblocks, B, 0, st>>>(d, stage, ncells);
+    gather_kernel<R, MODEL><<<cblocks, B, 0, st>>>(d, stage);
   };
   if (mode == MODE_RESIDUAL) {
     stage_seq(STAGE_DIAG);
@@ -94,7 +97,7 @@ static cudaError_t launch_split_t(const Dev<R>& d, bool srd, int trials, int mod
   phase_commit_kernel<<<kblocks, 128, 0, st>>>(d.ctl, cases, 1);
   for (int t = 0; t < trials; ++t) {
     stage_seq(STAGE_BASE);
-    phase_first_cells_kernel<R, MODEL><<<(ncells + 255) / 256, 256, 0, st>>>(d, ncells);
+    phase_first_cells_kernel<R, MODEL><<<fblocks, 256, 0, st>>>(d);
     for (int stage = 1; stage <= 2; ++stage) {
       if (srd) phase_srd_kernel<R, MODEL><<<cases, MAX_BLOCK, 0, st>>>(d, stage);
       stage_seq(stage);
@@ -107,15 +110,15 @@ static cudaError_t launch_split_t(const Dev<R>& d, bool srd, int trials, int mod
 
 template <class R>
 cudaError_t EngineOps<R>::launch_split(const Dev<R>& d, int model, int flux, bool srd, int trials, int mode,
-                                       cudaStream_t stream) {
+                                       cudaStream_t stream, int sms) {
   if (model == MODEL_EULER)
-    return flux == FLUX_HLLC ? launch_split_t<R, MODEL_EULER, FLUX_HLLC>(d, srd, trials, mode, stream)
-                             : launch_split_t<R, MODEL_EULER, FLUX_AUSM>(d, srd, trials, mode, stream);
+    return flux == FLUX_HLLC ? launch_split_t<R, MODEL_EULER, FLUX_HLLC>(d, srd, trials, mode, stream, sms)
+                             : launch_split_t<R, MODEL_EULER, FLUX_AUSM>(d, srd, trials, mode, stream, sms);
   if (model == MODEL_LAMINAR)
-    return flux == FLUX_HLLC ? launch_split_t<R, MODEL_LAMINAR, FLUX_HLLC>(d, srd, trials, mode, stream)
-                             : launch_split_t<R, MODEL_LAMINAR, FLUX_AUSM>(d, srd, trials, mode, stream);
-  return flux == FLUX_HLLC ? launch_split_t<R, MODEL_SA, FLUX_HLLC>(d, srd, trials, mode, stream)
-                           : launch_split_t<R, MODEL_SA, FLUX_AUSM>(d, srd, trials, mode, stream);
+    return flux == FLUX_HLLC ? launch_split_t<R, MODEL_LAMINAR, FLUX_HLLC>(d, srd, trials, mode, stream, sms)
+                             : launch_split_t<R, MODEL_LAMINAR, FLUX_AUSM>(d, srd, trials, mode, stream, sms);
+  return flux == FLUX_HLLC ? launch_split_t<R, MODEL_SA, FLUX_HLLC>(d, srd, trials, mode, stream, sms)
+                           : launch_split_t<R, MODEL_SA, FLUX_AUSM>(d, srd, trials, mode, stream, sms);
 }
 
 template <class R> cudaError_t EngineOps<R>::occupancy(int model, int flux, bool srd, int block, int* blocks_per_sm) {
