@@ -247,6 +247,10 @@ int amr_euler_residual_static(const amr_cell_t* cells, uint64_t n_cells, const a
                               const uint64_t* cell_faces, const amr_boundary_t* boundaries, const amr_params_t* params,
                               const double* u, double* r, void* stream, char* error, uint64_t error_size);
 
+/* The same export for the single-case session (see amr_batch_export). */
+int amr_gpu_export(amr_gpu_session* session, double* wall_rows, uint64_t wall_count, double* sa_rows,
+                   uint64_t sa_count, double limits[2], char* error, uint64_t error_size);
+
 /* ----------------------------------------------------------------------------------
  * Batched form.
  * ---------------------------------------------------------------------------------- */
@@ -307,6 +311,15 @@ int amr_batch_check(amr_batch* batch, char* error, uint64_t error_size);
 int amr_batch_status(const amr_batch* batch, int32_t slot, amr_case_status_t* out);
 int amr_batch_download(amr_batch* batch, int32_t slot, double* u_out, uint64_t u_count,
                        char* error, uint64_t error_size);
+/* Compact results of one case, computed on the device from its accepted state, so a retired
+ * case leaves the device without its full state: the wall-stress rows of the reference's viscous
+ * snapshot (src/static_amr2d_viscous.cpp:155-160; 14 doubles per wall fragment, viscous models
+ * only, else wall_count = 0), the SA cell rows (nutilde, eddy viscosity, wall distance; 3 per
+ * cell, SA only, else sa_count = 0) and limits = {smallest convective dt, smallest viscous dt}.
+ * Runs one residual pass of the live cases first.  No counterpart in the reference, which
+ * downloads the state and evaluates these on the host. */
+int amr_batch_export(amr_batch* batch, int32_t slot, double* wall_rows, uint64_t wall_count, double* sa_rows,
+                     uint64_t sa_count, double limits[2], char* error, uint64_t error_size);
 int amr_batch_release(amr_batch* batch, int32_t slot);
 int amr_batch_live_cases(const amr_batch* batch);
 uint64_t amr_batch_free_cells(const amr_batch* batch);
@@ -374,7 +387,51 @@ int amr_mesh_build_many(uint64_t count, const amr_mesh_request_t* requests, int3
  * amr_batch_admit. */
 int amr_mesh_view(const amr_mesh_t* mesh, amr_mesh_view_t* view);
 int amr_mesh_get_counts(const amr_mesh_t* mesh, amr_mesh_counts_t* counts);
+
+/* Build records the mesh files carry besides the tables: the agglomeration map (9 doubles per
+ * original control volume: old id, new id, x0, x1, y0, y1, volume, cx, cy) and the (background
+ * leaf, control volume) pairs of leaves split into several fluid loops. */
+typedef struct amr_mesh_extras_t {
+  uint64_t coarse_fine_faces, split_leaves;
+  const double* agglomeration;     /* n_agglomeration x 9 */
+  uint64_t n_agglomeration;
+  const uint64_t* leaf_components; /* n_leaf_components x 2 */
+  uint64_t n_leaf_components;
+} amr_mesh_extras_t;
+int amr_mesh_get_extras(const amr_mesh_t* mesh, amr_mesh_extras_t* extras);
 void amr_mesh_destroy(amr_mesh_t* mesh);
+
+/* ----------------------------------------------------------------------------------
+ * Result files in the reference's formats (read by its pipeline/export.py).
+ *
+ * amr_write_mesh_files   <- static_amr_binary_mesh (src/static_amr2d_binary.cpp:25-49):
+ *                           <prefix>.bc.json, .transport.json, .viscous_stabilization.json,
+ *                           .gradient_table.csv, .wall_samples.csv (viscous), .cells.npy,
+ *                           .faces.npy, .walls.npy, .leaf_components.npy, .agglomeration.npy,
+ *                           .mesh.json
+ * amr_write_snapshot_files <- static_amr_binary_snapshot (src/static_amr2d_binary.cpp:50-69):
+ *                           <prefix>.state.npy, .json and, for viscous models,
+ *                           .timestep_limits.json, .wall_stress.npy, .viscous_loads.json,
+ *                           .sa.npy, .sa.json; the rows come from amr_gpu_export /
+ *                           amr_batch_export.
+ * amr_write_npy          <- static_amr_write_npy (src/static_amr2d_binary.cpp:14-24).
+ * The files are byte-identical to the reference writer's for the same inputs.
+ * ---------------------------------------------------------------------------------- */
+typedef struct amr_export_rows_t {
+  const double* wall_rows; /* n_walls x 14 (viscous models) */
+  const double* sa_rows;   /* n_cells x 3 (SA) */
+  double convective_dt, viscous_dt;
+} amr_export_rows_t;
+
+int amr_write_npy(const char* path, const double* values, uint64_t rows, uint64_t cols, char* error,
+                  uint64_t error_size);
+int amr_write_mesh_files(const char* prefix, const amr_mesh_view_t* mesh, const amr_mesh_options_t* options,
+                         const amr_params_t* params, const amr_mesh_extras_t* extras, char* error,
+                         uint64_t error_size);
+int amr_write_snapshot_files(const char* prefix, const amr_mesh_view_t* mesh, const amr_mesh_options_t* options,
+                             const amr_params_t* params, const double* u, double time, int64_t steps,
+                             int64_t rejected, const char* backend, const amr_export_rows_t* rows, char* error,
+                             uint64_t error_size);
 
 #ifdef __cplusplus
 }

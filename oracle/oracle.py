@@ -58,6 +58,10 @@ def ref_lib(kind='serial'):
         lib.ref_case_counts.argtypes = [P, P]
         lib.ref_case_initialize.argtypes = [P, P, P]
         lib.ref_case_run.argtypes = [P, P, C.c_uint64, P, P, P, C.c_double, C.c_int64, C.c_char_p, C.c_uint64]
+        lib.ref_case_write_mesh.argtypes = [P, C.c_char_p, C.c_char_p, C.c_uint64]
+        lib.ref_case_write_snapshot.argtypes = [P, P, C.c_uint64, C.c_double, C.c_int64, C.c_int64, C.c_char_p,
+                                                C.c_char_p, C.c_char_p, C.c_uint64]
+        lib.ref_write_npy.argtypes = [C.c_char_p, P, C.c_uint64, C.c_uint64]
         lib.ref_case_run_timed.restype = C.c_double
         lib.ref_case_run_timed.argtypes = [P, P, C.c_uint64, P, P, P, C.c_double, C.c_int64, P]
         lib.ref_case_rhs.argtypes = [P, P, P]
@@ -158,6 +162,18 @@ class RefCase:
         u = np.ascontiguousarray(u, dtype=np.float64).copy()
         assert self.lib.ref_case_redistribute(C.c_void_p(self.h), u.ctypes.data) == 0
         return u
+
+    def write_mesh(self, prefix):
+        err = C.create_string_buffer(512)
+        if self.lib.ref_case_write_mesh(C.c_void_p(self.h), str(prefix).encode(), err, 512):
+            raise RuntimeError(err.value.decode())
+
+    def write_snapshot(self, prefix, u, time, steps, rejected, backend='cuda'):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        err = C.create_string_buffer(512)
+        if self.lib.ref_case_write_snapshot(C.c_void_p(self.h), u.ctypes.data, len(u), float(time), int(steps),
+                                            int(rejected), str(prefix).encode(), backend.encode(), err, 512):
+            raise RuntimeError(err.value.decode())
 
     def diagnostics(self, u, region=(-1.0, 3.0, -1.0, 1.0), moment=(0.25, 0.0)):
         u = np.ascontiguousarray(u, dtype=np.float64)

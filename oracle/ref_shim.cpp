@@ -11,6 +11,7 @@
 // (src/quick_airfoil.cpp:189-199).  With REF_WITH_CUDA it also wraps the reference CUDA
 // session (src/static_amr2d_cuda.cu:274-366) so its kernels can be timed on the same GPU.
 #include "static_amr2d.h"
+#include "static_amr2d_binary.h"
 #include "static_amr2d_gpu.h"
 #include "amr_b200.h"
 
@@ -207,6 +208,31 @@ int ref_case_run(const ref_case* c, double* u, uint64_t count, double* time, int
   *time = s.time; *steps = s.steps; *rejected = s.rejected;
   if (status) put_error(error, error_size, message);
   return status;
+}
+
+// The reference's own result writers, for byte-for-byte comparison of the files.
+int ref_case_write_mesh(const ref_case* c, const char* prefix, char* error, uint64_t error_size) {
+  std::string message;
+  const int st = static_amr_binary_mesh(c->mesh, c->params, prefix, &message);
+  if (st) put_error(error, error_size, message);
+  return st;
+}
+
+int ref_case_write_snapshot(const ref_case* c, const double* u, uint64_t count, double time, int64_t steps,
+                            int64_t rejected, const char* prefix, const char* backend, char* error,
+                            uint64_t error_size) {
+  StaticAmrState2D s;
+  s.u.assign(u, u + count);
+  s.time = time; s.steps = steps; s.rejected = rejected;
+  std::string message;
+  const int st = static_amr_binary_snapshot(c->mesh, c->params, s, prefix, backend, &message);
+  if (st) put_error(error, error_size, message);
+  return st;
+}
+
+int ref_write_npy(const char* path, const double* values, uint64_t rows, uint64_t cols) {
+  std::string message;
+  return static_amr_write_npy(path, values, rows, cols, &message);
 }
 
 // Wall-clock seconds of ref_case_run, measured around the reference call alone.

@@ -95,6 +95,15 @@ class MeshRequest(C.Structure):
                 ('boundaries', _P), ('transport', _P), ('params', _P)]
 
 
+class MeshExtras(C.Structure):
+    _fields_ = [('coarse_fine_faces', C.c_uint64), ('split_leaves', C.c_uint64), ('agglomeration', _P),
+                ('n_agglomeration', C.c_uint64), ('leaf_components', _P), ('n_leaf_components', C.c_uint64)]
+
+
+class ExportRows(C.Structure):
+    _fields_ = [('wall_rows', _P), ('sa_rows', _P), ('convective_dt', C.c_double), ('viscous_dt', C.c_double)]
+
+
 class MeshCounts(C.Structure):
     _fields_ = [('background_leaves', C.c_uint64), ('split_leaves', C.c_uint64), ('coarse_fine_faces', C.c_uint64),
                 ('small_cells', C.c_uint64), ('n_terms', C.c_uint64)]

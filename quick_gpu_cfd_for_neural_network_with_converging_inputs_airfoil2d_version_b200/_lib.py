@@ -40,6 +40,13 @@ SIGNATURES = {
     'amr_mesh_view': (C.c_int, [_P, _P]),
     'amr_mesh_get_counts': (C.c_int, [_P, _P]),
     'amr_mesh_destroy': (None, [_P]),
+    'amr_mesh_get_extras': (C.c_int, [_P, _P]),
+    'amr_gpu_export': (C.c_int, [_P, _P, C.c_uint64, _P, C.c_uint64, _P, _S, C.c_uint64]),
+    'amr_batch_export': (C.c_int, [_P, C.c_int32, _P, C.c_uint64, _P, C.c_uint64, _P, _S, C.c_uint64]),
+    'amr_write_npy': (C.c_int, [_S, _P, C.c_uint64, C.c_uint64, _S, C.c_uint64]),
+    'amr_write_mesh_files': (C.c_int, [_S, _P, _P, _P, _P, _S, C.c_uint64]),
+    'amr_write_snapshot_files': (C.c_int, [_S, _P, _P, _P, _P, C.c_double, C.c_int64, C.c_int64, _S, _P, _S,
+                                           C.c_uint64]),
     # extras used by the host mirror
     'amr_batch_autotune': (C.c_int, [_P, C.c_int32, _S, C.c_uint64]),
     'amr_batch_launch_config': (C.c_int, [_P, _S, C.c_uint64]),

@@ -87,6 +87,11 @@ class Batch:
             raise BatchError(err.value.decode())
         return u
 
+    def export(self, slot, mesh):
+        """Device-computed compact results of a case (see StaticAmrGpu.export)."""
+        from .snapshot import export_rows
+        return export_rows(lambda *a: lib().amr_batch_export(self._h, int(slot), *a), mesh)
+
     def residual(self, slot):
         r = np.empty(self.nv * self.ncells[slot])
         err = errbuf()

@@ -29,6 +29,7 @@ UNITS = {
 # CPU core is built with) without floating-point contraction.
 HOST_UNITS = {
     'amr_mesh.cpp': ['-O2', '-ffp-contract=off', '-fno-fast-math'],
+    'amr_export.cpp': ['-O2', '-ffp-contract=off', '-fno-fast-math'],
 }
 HOST_CXX = '/usr/bin/g++' if os.path.exists('/usr/bin/g++') else (shutil.which('g++') or 'g++')
 

@@ -54,6 +54,14 @@ def _take(handle, options):
     m = MeshArrays.from_view(v, options)
     m.options.update(background_leaves=counts.background_leaves, split_leaves=counts.split_leaves,
                      coarse_fine_faces=counts.coarse_fine_faces)
+    ex = _abi.MeshExtras()
+    lib().amr_mesh_get_extras(C.c_void_p(handle), C.byref(ex))
+    if ex.n_agglomeration:
+        buf = (C.c_double * (9 * ex.n_agglomeration)).from_address(ex.agglomeration)
+        m.agglomeration = np.frombuffer(buf, dtype=np.float64).reshape(-1, 9).copy()
+    if ex.n_leaf_components:
+        buf = (C.c_uint64 * (2 * ex.n_leaf_components)).from_address(ex.leaf_components)
+        m.leaf_components = np.frombuffer(buf, dtype=np.uint64).reshape(-1, 2).copy()
     lib().amr_mesh_destroy(C.c_void_p(handle))
     return m
 

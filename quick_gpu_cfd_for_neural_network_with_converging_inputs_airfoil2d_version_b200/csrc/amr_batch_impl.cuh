@@ -178,7 +178,8 @@ template <class R> class Batch final : public BatchBase {
               U0_.alloc(nv_ * nc, A, error, "state") && U1_.alloc(nv_ * nc, A, error, "state") &&
               U2_.alloc(nv_ * nc, A, error, "state") && R0_.alloc(nv_ * nc, A, error, "state") &&
               diag_part_.alloc(9 * cap_tiles_, A, error, "diag") && diag_out_.alloc(9 * c.max_cases, A, error, "diag") &&
-              diag_cfg_.alloc(7 * c.max_cases, A, error, "diag") && case_tiles_.alloc(2 * c.max_cases, A, error, "diag");
+              diag_cfg_.alloc(7 * c.max_cases, A, error, "diag") && case_tiles_.alloc(2 * c.max_cases, A, error, "diag") &&
+              ddt_.alloc(2 * nc, A, error, "diag");
     if (!ok) return false;
     if (!s_geo_.alloc(6 * cap_slots_, A, error, "slots")) return false;
     // face and wall records of the split launch mode
@@ -668,6 +669,10 @@ template <class R> class Batch final : public BatchBase {
     return copy_out(R0_.p, slot, out, count, error);
   }
 
+  int export_case(int slot, double* wall_rows, uint64_t wall_count, double* sa_rows, uint64_t sa_count, double* limits,
+                  std::string* error) override;
+  int n_walls(int slot) const override { return (int)cases_[slot].walls.n; }
+
   int download(int slot, double* u, uint64_t count, std::string* error) override {
     if (slot < 0 || slot >= config_.max_cases || !cases_[slot].live) return fail1(error, "no such case");
     const int ok = copy_out(h_ctl_[slot].cur ? U1_.p : U0_.p, slot, u, count, error);
@@ -988,6 +993,9 @@ template <class R> class Batch final : public BatchBase {
     d.fval = fval_.p;
     d.wval = wval_.p;
     d.crec = crec_.p;
+    d.ddt = ddt_.p;
+    d.w_xm = w_xm_.p;
+    d.w_ym = w_ym_.p;
     d.live_end = live_end_.p;
     d.cap_faces = (int)cap_faces_;
     d.cap_walls = (int)cap_walls_;
@@ -1111,7 +1119,7 @@ template <class R> class Batch final : public BatchBase {
     c_term_.free(); c_cx_.free(); c_cy_.free(); c_wd_.free();
     s_own_.free(); s_nb_.free(); s_meta_.free(); s_len_.free(); s_geo_.free(); s_item_.free();
     f_case_.free(); f_own_.free(); f_nb_.free(); f_meta_.free(); f_len_.free(); f_geo_.free(); fval_.free();
-    w_owner_.free(); wval_.free(); crec_.free(); live_end_.free();
+    w_owner_.free(); wval_.free(); crec_.free(); live_end_.free(); ddt_.free(); ex_buf_.free();
     w_nx_.free(); w_ny_.free(); w_len_.free(); w_dist_.free(); w_donor_.free(); w_xm_.free(); w_ym_.free();
     t_own_.free(); t_src_.free(); t_x_.free(); t_y_.free();
     g_mem_.free(); g_cell_.free(); g_cnt_.free(); g_vol_.free(); q_cell_.free(); q_grp_.free(); q_list_.free(); q_cnt_.free();
@@ -1168,7 +1176,7 @@ template <class R> class Batch final : public BatchBase {
   DevBuf<int> g_mem_, g_cell_, q_cell_, q_grp_, q_list_;
   DevBuf<double> g_cnt_, g_vol_, q_cnt_, qhat_;
   DevBuf<R> U0_, U1_, U2_, R0_, grad_, mu_, eddy_, sgrad_, sdiff_, ssrc_, srate_;
-  DevBuf<double> diag_part_, diag_out_, diag_cfg_;
+  DevBuf<double> diag_part_, diag_out_, diag_cfg_, ddt_, ex_buf_;
   DevBuf<int> case_tiles_;
 };
 

@@ -216,6 +216,20 @@ int amr_gpu_residual(amr_gpu_session* s, double* r, uint64_t count, char* error,
   return 0;
 }
 
+int amr_gpu_export(amr_gpu_session* s, double* wall_rows, uint64_t wall_count, double* sa_rows, uint64_t sa_count,
+                   double limits[2], char* error, uint64_t error_size) {
+  if (!s) {
+    put(error, error_size, "invalid AMR GPU export");
+    return 1;
+  }
+  std::string err;
+  if (s->batch->export_case(0, wall_rows, wall_count, sa_rows, sa_count, limits, &err)) {
+    put(error, error_size, err);
+    return 1;
+  }
+  return 0;
+}
+
 int amr_gpu_diagnostics(amr_gpu_session* s, const double region[4], double mx, double my, double out[8], char* error,
                         uint64_t error_size) {
   if (!s || !region || !out) {
@@ -405,6 +419,17 @@ int amr_batch_status(const amr_batch* b, int32_t slot, amr_case_status_t* out) {
   out->cl = cs.cl;
   out->cd = cs.cd;
   out->cm = cs.cm;
+  return 0;
+}
+
+int amr_batch_export(amr_batch* b, int32_t slot, double* wall_rows, uint64_t wall_count, double* sa_rows, uint64_t sa_count,
+                     double limits[2], char* error, uint64_t error_size) {
+  if (!b) return 1;
+  std::string err;
+  if (b->batch->export_case(slot, wall_rows, wall_count, sa_rows, sa_count, limits, &err)) {
+    put(error, error_size, err);
+    return 1;
+  }
   return 0;
 }
 

@@ -144,6 +144,9 @@ template <class R> struct Dev {
   R* fval;          // 12 per face
   R* wval;          // 12 per wall
   R* crec;          // CREC per cell: packed state and gradient-phase fields (viscous models)
+  double* ddt;      // 2 per cell: convective and viscous dt limits of the last residual pass
+  const double* w_xm;  // wall midpoints
+  const double* w_ym;
   int n_faces, n_walls, n_cells;  // ends of the live face, wall and cell ranges (host copy)
   int cap_faces, cap_walls;       // record capacities
   const int* live_end;            // the same on the device: cells, faces, walls (read by the
@@ -685,6 +688,7 @@ __device__ __forceinline__ double finish_cell(const Dev<R>& d, const CaseCfg<R>&
   const long long n = d.ncap;
   const R g = cf.gamma;
   const bool base = stage == STAGE_BASE;
+  const bool spec = base || stage == STAGE_DIAG;  // spectral sums wanted (dt, or the export's dt limits)
   double cell_dt = __longlong_as_double(0x7FF0000000000000ll);
   const double V = d.c_vol[k];
   const Prim<R> wk = prim(Uin, n, k, g);
@@ -700,14 +704,14 @@ __device__ __forceinline__ double finish_cell(const Dev<R>& d, const CaseCfg<R>&
       sum[1] += col[1];
       sum[2] += col[2];
     }
-    if (base) spectral += col[8];
+    if (spec) spectral += col[8];
     if (MODEL >= MODEL_LAMINAR) {
       for (int v = 0; v < 4; ++v) vs[v] += col[4 + v];
-      if (base) vspec += col[9];
+      if (spec) vspec += col[9];
     }
     if (MODEL == MODEL_SA) {
       if (!wall) snet += col[10]; else snet -= col[10];
-      if (base) sspec += col[11];
+      if (spec) sspec += col[11];
     }
   }
   R res[5];
@@ -734,6 +738,11 @@ __device__ __forceinline__ double finish_cell(const Dev<R>& d, const CaseCfg<R>&
     for (int v = 0; v < nv; ++v) d.R0[v * n + k] = res[v];
   } else if (stage == STAGE_DIAG) {
     for (int v = 0; v < nv; ++v) d.R0[v * n + k] = res[v];
+    // convective and viscous dt limits of the cell, for the export (reference
+    // src/static_amr2d_viscous.cpp:151-153 and :131)
+    const double inf = __longlong_as_double(0x7FF0000000000000ll);
+    d.ddt[k] = spectral > R(0) ? cf.cfl * d.c_area[k] / (double)spectral : inf;
+    d.ddt[n + k] = MODEL >= MODEL_LAMINAR && vspec > R(0) ? cf.viscous_cfl * V / (double)vspec : inf;
   } else {
     const R dt = (R)d.ctl[cs].dt_trial;
     const bool simple = cf.has_srd && (d.c_flags[k] & 1);
@@ -774,6 +783,7 @@ __device__ void phase_flux(const Dev<R>& d, const Tile& t, int stage, const R* U
   const CaseCfg<R>& cf = d.cfg[t.cs];
   const int s0 = t.s0, s1 = t.s1;
   const bool base = stage == STAGE_BASE;
+  const bool spec = base || stage == STAGE_DIAG;
   bool bad = false;
   if (i < s1 - s0) {
     const int s = s0 + i;
@@ -781,9 +791,9 @@ __device__ void phase_flux(const Dev<R>& d, const Tile& t, int stage, const R* U
     const R* gp = d.s_geo + 6 * (long long)s;
     const R len = __ldg(d.s_len + s);
     if (meta & SLOT_WALL)
-      slot_wall<R, MODEL>(d, cf, __ldg(gp + 0), __ldg(gp + 1), __ldg(gp + 2), len, k, nb, Uin, base, sm + i, B, bad);
+      slot_wall<R, MODEL>(d, cf, __ldg(gp + 0), __ldg(gp + 1), __ldg(gp + 2), len, k, nb, Uin, spec, sm + i, B, bad);
     else
-      slot_face<R, MODEL, FLUX>(d, cf, gp, len, k, nb, meta, Uin, base, sm + i, B, true, bad);
+      slot_face<R, MODEL, FLUX>(d, cf, gp, len, k, nb, meta, Uin, spec, sm + i, B, true, bad);
   }
   __syncwarp();
   double cell_dt = __longlong_as_double(0x7FF0000000000000ll);
@@ -1231,7 +1241,7 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::cell) grad_cells_ker
 template <class R, int MODEL, int FLUX>
 __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::item) item_kernel(Dev<R> d, int stage) {
   const int rule = stage_rule(stage);
-  const bool base = stage == STAGE_BASE;
+  const bool base = stage == STAGE_BASE || stage == STAGE_DIAG;  // spectral columns wanted
   const int nf = d.live_end[1], total = nf + d.live_end[2];
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
     bool bad = false;
@@ -1306,7 +1316,8 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::cell) gather_kernel(
       const CaseCtl& c = d.ctl[cs];
       const int a = d.c_slot[k], b = d.c_slot[k + 1];
       const int e = b - (d.c_wall[k + 1] - d.c_wall[k]);
-      cell_dt = finish_cell<R, MODEL>(d, d.cfg[cs], cs, k, stage, a, e, b, ItemSlots<R, MODEL>{&d, base},
+      cell_dt = finish_cell<R, MODEL>(d, d.cfg[cs], cs, k, stage, a, e, b,
+                                      ItemSlots<R, MODEL>{&d, base || stage == STAGE_DIAG},
                                       stage_input(d, stage, c.cur), state_buf(d, c.cur), state_buf(d, c.cur ^ 1), bad);
       if (bad && stage != STAGE_DIAG) atomicOr(&d.ctl[cs].bad, 1);
     }

@@ -298,6 +298,180 @@ template <class R> int Batch<R>::autotune(int trials, std::string* error) {
   return sync_tiles(error) ? 0 : 1;
 }
 
+// Wall-stress rows of one case (reference src/static_amr2d_viscous.cpp:155-160): wall index,
+// owner, donor, donor distance, donor viscosity, wall flux x and y per length, signed tangential
+// stress, owner pressure, pressure force x/y, viscous force x/y and its moment about the origin.
+// Evaluated in double from the accepted state and the viscosity of the last residual pass.
+template <class R>
+__global__ void export_walls_kernel(Dev<R> d, int cs, int w0, int nw, int cell0, double gamma, double* rows) {
+  const long long n = d.ncap;
+  const R* U = state_buf(d, d.ctl[cs].cur);
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nw; q += gridDim.x * blockDim.x) {
+    const int w = w0 + q;
+    const int k = d.w_owner[w], dn = d.w_donor[w];
+    const double u0 = U[k], u1 = U[n + k], u2 = U[2 * n + k], u3 = U[3 * n + k];
+    const double pressure = (gamma - 1) * (u3 - .5 * (u1 * u1 + u2 * u2) / u0);
+    const double nx = d.w_nx[w], ny = d.w_ny[w], len = d.w_len[w], dist = d.w_dist[w];
+    const double x = d.w_xm[w], y = d.w_ym[w];
+    const double mu = d.mu[dn];
+    const double rd = U[dn], ud = U[n + dn] / rd, vd = U[2 * n + dn] / rd;
+    double gw[4], fw[4];
+    wall_gradient(nx, ny, dist, -ud, -vd, gw);
+    visc_flux(mu, gw, nx, ny, 0.0, 0.0, fw);
+    const double fx = fw[1] * len, fy = fw[2] * len;
+    const double px = pressure * nx * len, py = pressure * ny * len, vx = -fx, vy = -fy;
+    double* r = rows + 14 * (long long)q;
+    r[0] = q;
+    r[1] = k - cell0;
+    r[2] = dn - cell0;
+    r[3] = dist;
+    r[4] = mu;
+    r[5] = fx / len;
+    r[6] = fy / len;
+    r[7] = (-ny * fx + nx * fy) / len;
+    r[8] = pressure;
+    r[9] = px;
+    r[10] = py;
+    r[11] = vx;
+    r[12] = vy;
+    r[13] = x * vy - y * vx;
+  }
+}
+
+// SA cell rows (reference src/static_amr2d_viscous.cpp:164): nutilde, eddy viscosity, wall distance.
+template <class R> __global__ void export_sa_kernel(Dev<R> d, int cs, int c0, int n_cells, double* rows) {
+  const long long n = d.ncap;
+  const R* U = state_buf(d, d.ctl[cs].cur);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_cells; i += gridDim.x * blockDim.x) {
+    const int k = c0 + i;
+    rows[3 * (long long)i + 0] = (double)U[4 * n + k] / (double)U[k];
+    rows[3 * (long long)i + 1] = d.eddy[k];
+    rows[3 * (long long)i + 2] = d.c_wd[k];
+  }
+}
+
+// Convective dt limit of each cell of a case as the reference's snapshot evaluates it
+// (src/static_amr2d_viscous.cpp:146-153): primitives p = (gamma-1)(E - rho|v|^2/2), boundary ghost
+// states, face rate max(|u_n| + c) * length summed in face order then walls, cfl * A / speed.
+// Overwrites the case's convective entries of the last residual pass.
+template <class R> __global__ void export_convective_kernel(Dev<R> d, int cs, int c0, int n_cells) {
+  const long long n = d.ncap;
+  const CaseCfg<R>& cf = d.cfg[cs];
+  const R* U = state_buf(d, d.ctl[cs].cur);
+  const double g = cf.gamma;
+  const auto prim_of = [&](int k, double* w) {
+    w[0] = U[k];
+    w[1] = (double)U[n + k] / w[0];
+    w[2] = (double)U[2 * n + k] / w[0];
+    w[3] = (g - 1) * ((double)U[3 * n + k] - .5 * w[0] * (w[1] * w[1] + w[2] * w[2]));
+  };
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_cells; i += gridDim.x * blockDim.x) {
+    const int k = c0 + i;
+    double speed = 0;
+    const int a = d.c_slot[k], b = d.c_slot[k + 1];
+    const int e = b - (d.c_wall[k + 1] - d.c_wall[k]);
+    double wk[4];
+    prim_of(k, wk);
+    for (int q = a; q < e; ++q) {
+      const int meta = d.s_meta[q], nb = d.s_nb[q];
+      const bool own_left = meta & 1;
+      const int axis = (meta >> 1) & 1, side = ((meta >> 2) & 7) - 1, kind = (meta >> 5) & 15;
+      double wn[4];
+      if (nb >= 0) {
+        prim_of(nb, wn);
+      } else {
+        Bnd<double> bd;
+        const Bnd<R>& br = cf.bnd[side];
+        bd.kind = br.kind;
+        for (int v = 0; v < 4; ++v) bd.ref[v] = br.ref[v];
+        bd.total_pressure = br.total_pressure;
+        bd.total_temperature = br.total_temperature;
+        bd.gas_constant = br.gas_constant;
+        bd.dir[0] = br.dir[0];
+        bd.dir[1] = br.dir[1];
+        bd.outlet_pressure = br.outlet_pressure;
+        bd.wall_velocity[0] = br.wall_velocity[0];
+        bd.wall_velocity[1] = br.wall_velocity[1];
+        bc_state(bd, kind, g, side, wk, wn);
+      }
+      const double* l = own_left ? wk : wn;
+      const double* r = own_left ? wn : wk;
+      const double ra = fabs(l[1 + axis]) + sqrt(g * l[3] / l[0]), rb = fabs(r[1 + axis]) + sqrt(g * r[3] / r[0]);
+      speed += (ra < rb ? rb : ra) * (double)d.s_len[q];
+    }
+    for (int q = e; q < b; ++q) speed += sqrt(g * wk[3] / wk[0]) * (double)d.s_len[q];
+    d.ddt[k] = speed > 0 ? cf.cfl * d.c_area[k] / speed : __longlong_as_double(0x7FF0000000000000ll);
+  }
+}
+
+// Smallest convective and viscous dt limit over a case's cells (min is order-free).
+template <class R> __global__ void export_limits_kernel(Dev<R> d, int c0, int n_cells, double* out) {
+  __shared__ double sc[256], sv[256];
+  const double inf = __longlong_as_double(0x7FF0000000000000ll);
+  double c = inf, v = inf;
+  for (int i = threadIdx.x; i < n_cells; i += blockDim.x) {
+    c = fmin(c, d.ddt[c0 + i]);
+    v = fmin(v, d.ddt[d.ncap + c0 + i]);
+  }
+  sc[threadIdx.x] = c;
+  sv[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+      sc[threadIdx.x] = fmin(sc[threadIdx.x], sc[threadIdx.x + s]);
+      sv[threadIdx.x] = fmin(sv[threadIdx.x], sv[threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = sc[0];
+    out[1] = sv[0];
+  }
+}
+
+template <class R>
+int Batch<R>::export_case(int slot, double* wall_rows, uint64_t wall_count, double* sa_rows, uint64_t sa_count,
+                          double* limits, std::string* error) {
+  if (slot < 0 || slot >= config_.max_cases || !cases_[slot].live) return fail1(error, "no such case");
+  const HostCase<R>& hc = cases_[slot];
+  const long long n = hc.n, nw = hc.walls.n;
+  const uint64_t want_walls = model_ >= MODEL_LAMINAR ? 14 * (uint64_t)nw : 0;
+  const uint64_t want_sa = model_ == MODEL_SA ? 3 * (uint64_t)n : 0;
+  if ((want_walls && !wall_rows) || wall_count != want_walls || (want_sa && !sa_rows) || sa_count != want_sa || !limits)
+    return fail1(error, "export buffer sizes do not match the case (14 per wall for viscous models, 3 per cell for SA)");
+  if (residual(error)) return 1;
+  const uint64_t need = want_walls + want_sa + 2;
+  if (ex_buf_.n < need) {
+    ex_buf_.free();
+    uint64_t dummy = 0;
+    if (!ex_buf_.alloc(need, &dummy, error, "export")) return 1;
+  }
+  const Dev<R> d = dev();
+  const int c0 = (int)hc.cells.b;
+  double* dev_walls = ex_buf_.p;
+  double* dev_sa = ex_buf_.p + want_walls;
+  double* dev_lim = ex_buf_.p + want_walls + want_sa;
+  if (want_walls && nw > 0)
+    export_walls_kernel<R><<<(int)((nw + 127) / 128), 128, 0, stream_>>>(d, slot, (int)hc.walls.b, (int)nw, c0,
+                                                                        (double)hc.cfg.gamma, dev_walls);
+  if (want_sa) export_sa_kernel<R><<<(int)((n + 255) / 256), 256, 0, stream_>>>(d, slot, c0, (int)n, dev_sa);
+  export_convective_kernel<R><<<(int)((n + 127) / 128), 128, 0, stream_>>>(d, slot, c0, (int)n);
+  export_limits_kernel<R><<<1, 256, 0, stream_>>>(d, c0, (int)n, dev_lim);
+  bool ok = cuda_ok(cudaGetLastError(), error, "export launch");
+  launches_ += (want_walls && nw > 0) + (want_sa ? 1 : 0) + 2;
+  if (ok && want_walls)
+    ok = cuda_ok(cudaMemcpyAsync(wall_rows, dev_walls, sizeof(double) * want_walls, cudaMemcpyDeviceToHost, stream_),
+                 error, "export copy");
+  if (ok && want_sa)
+    ok = cuda_ok(cudaMemcpyAsync(sa_rows, dev_sa, sizeof(double) * want_sa, cudaMemcpyDeviceToHost, stream_), error,
+                 "export copy");
+  ok = ok && cuda_ok(cudaMemcpyAsync(limits, dev_lim, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream_), error,
+                     "export copy") &&
+       cuda_ok(cudaStreamSynchronize(stream_), error, "export sync");
+  if (ok) stats_.state_d2h_bytes += sizeof(double) * need;
+  return ok ? 0 : 1;
+}
+
 template <class R>
 void Batch<R>::restore(const std::vector<CaseCtl>& ctl_save, const DevBuf<R>& s0, const DevBuf<R>& s1, long long nbytes) {
   std::copy(ctl_save.begin(), ctl_save.end(), h_ctl_);

@@ -32,6 +32,12 @@ class BatchBase {
   virtual int residual(std::string* error) = 0;
   virtual int download_residual(int slot, double* out, uint64_t count, std::string* error) = 0;
   virtual int download(int slot, double* u, uint64_t count, std::string* error) = 0;
+  // Compact results of one case from its accepted state, computed on the device: wall-stress
+  // rows (14 per wall, viscous models), SA cell rows (3 per cell) and the convective and viscous
+  // dt limits.  Runs one residual pass of the live cases first.
+  virtual int export_case(int slot, double* wall_rows, uint64_t wall_count, double* sa_rows, uint64_t sa_count,
+                          double* limits, std::string* error) = 0;
+  virtual int n_walls(int slot) const = 0;
   // Region residual norms (5), region volume, Fx, Fy, Mz per requested case (9 doubles each).
   virtual int diagnostics(const std::vector<int>& slots, const std::vector<double>& region_moment,
                           std::vector<double>* out, std::string* error) = 0;

@@ -38,6 +38,8 @@ class MeshArrays:
     face_geometry: np.ndarray = None
     wall_distance: np.ndarray = None
     options: dict = field(default_factory=dict)  # build options (bounds, base shape, levels, ...)
+    agglomeration: np.ndarray = None      # (n_original, 9) build record of agglomerated meshes
+    leaf_components: np.ndarray = None    # (m, 2) uint64 (background leaf, control volume)
 
     @property
     def n_cells(self):
@@ -119,6 +121,9 @@ class MeshArrays:
     def save(self, path):
         data = {k: getattr(self, k) for k in self._ARRAYS if getattr(self, k) is not None}
         data['scalars'] = np.array([self.small_cells, self.agglomerate_small], dtype=np.int64)
+        for k in ('agglomeration', 'leaf_components'):
+            if getattr(self, k) is not None:
+                data[k] = getattr(self, k)
         opts = dict(self.options)
         data['options_json'] = np.frombuffer(__import__('json').dumps(opts).encode(), dtype=np.uint8)
         np.savez_compressed(path, **data)
@@ -130,6 +135,9 @@ class MeshArrays:
         kw = {k: z[k] for k in cls._ARRAYS if k in z.files}
         small, agg = (int(x) for x in z['scalars'])
         opts = json.loads(bytes(z['options_json']).decode()) if 'options_json' in z.files else {}
+        for k in ('agglomeration', 'leaf_components'):
+            if k in z.files:
+                kw[k] = z[k]
         return cls(small_cells=small, agglomerate_small=agg, options=opts, **kw)
 
     def with_physics(self, boundaries=None, transport=None):

@@ -67,6 +67,12 @@ class StaticAmrGpu:
             raise AmrGpuError(err.value.decode())
         return u
 
+    def export(self):
+        """Device-computed compact results of the accepted state: wall-stress rows (n_walls x 14,
+        viscous models), SA cell rows (n_cells x 3) and the (convective, viscous) dt limits."""
+        from .snapshot import export_rows
+        return export_rows(lambda *a: lib().amr_gpu_export(self._h, *a), self.mesh)
+
     def residual(self):
         r = np.empty(self.nv * self.mesh.n_cells)
         err = errbuf()

@@ -212,3 +212,28 @@ def test_graph_and_direct_launch_agree(golden):
         s.advance(1e30, 40)
         outs.append(s.download())
     assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[1], outs[2])
+
+
+def test_total_inlet_parity():
+    """Total-pressure inlet (the 64-step bisection of the inflow state) with a pressure outlet."""
+    from tests.test_oracle import total_inlet_spec
+    spec = total_inlet_spec()
+    x, y, pt = airfoils.naca4(0.0, 0.4, 0.12)
+    mesh = RefCase.build(spec, x, y, pt).mesh()
+    run_pair(mesh, spec, [1, 20])
+
+
+@pytest.mark.parametrize('control', ['fixed_dt', 'cpu_ausm', 'subsonic_outlet'])
+def test_control_known_steps_on_gpu(golden, control):
+    """validation/controls_checks.json through the B200 path: steps to t*=0.01 on G0001 LF2."""
+    ka = json.loads((golden / 'known_answers.json').read_text())
+    s, boxes = parse_settings(ka['settings']['control_' + control])
+    spec = SettingsSpec(s, boxes, 'LF2')
+    z = np.load(golden / 'examples.npz')
+    i = list(z['names']).index('G0001')
+    a, b = z['offsets'][i], z['offsets'][i + 1]
+    mesh = RefCase.build(spec, z['x'][a:b], z['y'][a:b], z['patches'][a:b]).mesh()
+    u0 = cases.initial_state(mesh, spec.initial_primitive())
+    g = StaticAmrGpu.create(mesh, spec.params(), u0)
+    assert g.advance(0.01, 50000000) == 0
+    assert g.steps == ka['controls'][control] and g.rejected == 0 and g.time == 0.01

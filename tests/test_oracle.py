@@ -104,3 +104,59 @@ def test_oracle_rejection_and_fatal_paths(golden):
     assert (o['status'], o['steps'], o['rejected'], o['time']) == (ref['status'], ref['steps'], ref['rejected'], ref['time'])
     assert o['error'] == ref['error']
     assert np.array_equal(o['u'], ref['u'])
+
+
+def total_inlet_spec():
+    """Subsonic channel-like case: total-pressure inlet on xmin (direction +x), static-pressure
+    outlet on xmax, farfield top and bottom; NACA 0012, LF1, agglomerated, inviscid."""
+    spec = cases.CaseSpec(naca=(0.0, 0.4, 0.12), profile='LF1', physics='euler', mach=0.5, aoa=0.0, agglomerate=True,
+                          kinds=('total-inlet', 'pressure-outlet', 'farfield', 'farfield'))
+    base = spec.boundary_records
+    gamma, mach = 1.4, 0.5
+
+    def records(g=1.4):
+        b = base(g)
+        w = cases.freestream(mach, 0.0, gamma)
+        t_static = w[3] / w[0]  # R = 1
+        b[0]['total_temperature'] = t_static * (1 + 0.5 * (gamma - 1) * mach * mach)
+        b[0]['total_pressure'] = w[3] * (1 + 0.5 * (gamma - 1) * mach * mach) ** (gamma / (gamma - 1))
+        b[0]['gas_constant'] = 1.0
+        b[0]['direction'] = (1.0, 0.0)
+        return b
+    spec.boundary_records = records
+    return spec
+
+
+def test_oracle_total_inlet_bitexact_against_reference():
+    spec = total_inlet_spec()
+    x, y, pt = airfoils.naca4(0.0, 0.4, 0.12)
+    rc = RefCase.build(spec, x, y, pt)
+    m = rc.mesh()
+    u0 = cases.initial_state(m, spec.initial_primitive())
+    ref = rc.run_steps(u0, 15)
+    o = Oracle(m, spec.params()).run_steps(u0, 15)
+    assert o['steps'] == ref['steps'] == 15 and o['time'] == ref['time']
+    assert np.array_equal(o['u'], ref['u'])
+
+
+def test_oracle_srd_rate_viscous_bitexact_against_reference():
+    """Laminar on an SRD (non-agglomerated) mesh with SRD-rate viscous stabilization."""
+    spec = cases.CaseSpec(naca=(0.02, 0.4, 0.12), profile='LF1', physics='laminar', agglomerate=False, mach=1.4,
+                          kinds=('farfield', 'pressure-outlet', 'farfield', 'farfield'))
+    base = spec.transport_record
+    spec.transport_record = lambda g=1.4: _with_stabilization(base(g))
+    x, y, pt = airfoils.naca4(0.02, 0.4, 0.12)
+    rc = RefCase.build(spec, x, y, pt)
+    m = rc.mesh()
+    assert m.small_cells > 0
+    u0 = cases.initial_state(m, spec.initial_primitive())
+    ref = rc.run_steps(u0, 10)
+    o = Oracle(m, spec.params()).run_steps(u0, 10)
+    assert o['steps'] == ref['steps'] == 10 and o['time'] == ref['time']
+    assert np.array_equal(o['u'], ref['u'])
+
+
+def _with_stabilization(t):
+    from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200 import _abi
+    t['stabilization'] = _abi.VISCOUS_SRD
+    return t
