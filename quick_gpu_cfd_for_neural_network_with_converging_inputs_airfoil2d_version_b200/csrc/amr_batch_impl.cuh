@@ -515,6 +515,10 @@ template <class R> class Batch final : public BatchBase {
     cf.srd_g1 = gb + (int)ng;
     cf.srd_q0 = qb;
     cf.srd_q1 = qb + (int)ng;
+    cf.srd_rate = model_ >= MODEL_LAMINAR && m->transport.stabilization == AMR_B200_VISCOUS_SRD && m->small_cells > 0 &&
+                  cf.has_srd;
+    cf.cell0 = cb;
+    cf.cell1 = cb + (int)n;
     // state
     const long long ncap = cap_cells_;
     std::vector<R> u(nv_ * (n + 1), R(1));
@@ -785,8 +789,6 @@ template <class R> class Batch final : public BatchBase {
       if (!m.visc_offsets || !m.visc_terms || (m.n_walls && !m.wall_samples) || !m.face_samples || !m.face_geometry)
         return fail(why, "viscous tables missing");
       if (t.sa_model && !m.wall_distance) return fail(why, "SA wall distance missing");
-      if (t.stabilization == AMR_B200_VISCOUS_SRD && m.small_cells)
-        return fail(why, "SRD-rate viscous stabilization is not supported by this engine");
     }
     if (m.small_cells && (!m.group_offsets || !m.group_members || !m.member_offsets || !m.member_groups || !m.group_volume))
       return fail(why, "SRD tables missing");
@@ -927,7 +929,7 @@ template <class R> class Batch final : public BatchBase {
     tiles_dirty_ = false;
     // a split-mode graph reads the live ranges from the device and keeps its grids; it is
     // recaptured only when the set of kernels changes (SRD launches appear or vanish)
-    if (mode_ != AMR_B200_LAUNCH_SPLIT || any_srd() != graph_srd_) graph_dirty_ = true;
+    if (mode_ != AMR_B200_LAUNCH_SPLIT || any_srd() != graph_srd_ || any_srd_rate() != graph_srd_rate_) graph_dirty_ = true;
     return cuda_ok(cudaStreamSynchronize(stream_), error, "tiles sync");
   }
 
@@ -994,6 +996,7 @@ template <class R> class Batch final : public BatchBase {
     d.wval = wval_.p;
     d.crec = crec_.p;
     d.ddt = ddt_.p;
+    d.any_srd_rate = any_srd_rate() ? 1 : 0;
     d.w_xm = w_xm_.p;
     d.w_ym = w_ym_.p;
     d.live_end = live_end_.p;
@@ -1014,13 +1017,20 @@ template <class R> class Batch final : public BatchBase {
     // per trial: three flux stages (one kernel, or item + gather), gradients per stage, the
     // first update, SRD after each stage and the commit; plus the opening commit
     const uint64_t flux = mode_ == AMR_B200_LAUNCH_SPLIT ? 2 : 1;
-    const uint64_t per_trial = 3 * flux + (model_ >= MODEL_LAMINAR ? 3 : 0) + 1 + (any_srd() ? 3 : 0) + 1;
+    const uint64_t per_trial = 3 * flux + (model_ >= MODEL_LAMINAR ? 3 : 0) + 1 + (any_srd() ? 3 : 0) + 1 +
+                               (any_srd_rate() ? 1 : 0);
     return 1 + per_trial * trials;
   }
 
   bool any_srd() const {
     for (auto& c : cases_)
       if (c.live && c.cfg.has_srd) return true;
+    return false;
+  }
+
+  bool any_srd_rate() const {
+    for (auto& c : cases_)
+      if (c.live && c.cfg.srd_rate) return true;
     return false;
   }
 
@@ -1091,6 +1101,7 @@ template <class R> class Batch final : public BatchBase {
     graph_nodes_ = nodes;
     graph_trials_ = trials;
     graph_srd_ = any_srd();
+    graph_srd_rate_ = any_srd_rate();
     graph_dirty_ = false;
     return true;
   }
@@ -1134,7 +1145,7 @@ template <class R> class Batch final : public BatchBase {
   int mode_ = AMR_B200_LAUNCH_PERSISTENT;  // persistent cooperative kernel, one kernel per phase, or split
   long long hw_cells_ = 0, hw_faces_ = 0, hw_walls_ = 0;
   int h_live_end_[4] = {0, 0, 0, 0};
-  bool graph_srd_ = false;
+  bool graph_srd_ = false, graph_srd_rate_ = false;
   DevBuf<int> live_end_;
   long long cap_faces_ = 0;
   RangeAlloc a_faces_;

@@ -55,6 +55,8 @@ template <class R> struct CaseCfg {
   Trn<R> trn;
   int agglomerated, has_srd;
   int srd_g0, srd_g1, srd_q0, srd_q1;  // SRD group / cell list ranges
+  int srd_rate;                        // viscous dt limited through the SRD map of the rates
+  int cell0, cell1;                    // the case's cell range
 };
 
 // A run of whole cells of one case: cells [c0, c1), their slots [s0, s1) and gradient terms [t0, t1).
@@ -65,8 +67,8 @@ constexpr int SLOT_WALL = 1 << 9;  // s_meta flag: the slot is a wall fragment o
 // A tile is processed by one warp: at most TILE_W slots and TILE_W gradient terms of whole cells,
 // synchronised by __syncwarp only, so the warps of a block never wait for one another.
 constexpr int TILE_W = 32;
-constexpr int SM_COLS = 12;
-constexpr int CREC = 16;  // values in a packed cell record  // shared-memory columns per slot
+constexpr int SM_COLS = 12;  // values per slot (shared-memory columns, face and wall records)
+constexpr int CREC = 16;     // values in a packed cell record
 constexpr unsigned FULL_MASK = 0xffffffffu;
 
 struct GridBarrier {
@@ -145,6 +147,7 @@ template <class R> struct Dev {
   R* wval;          // 12 per wall
   R* crec;          // CREC per cell: packed state and gradient-phase fields (viscous models)
   double* ddt;      // 2 per cell: convective and viscous dt limits of the last residual pass
+  int any_srd_rate; // some live case limits its viscous dt through the SRD map
   const double* w_xm;  // wall midpoints
   const double* w_ym;
   int n_faces, n_walls, n_cells;  // ends of the live face, wall and cell ranges (host copy)
@@ -733,7 +736,12 @@ __device__ __forceinline__ double finish_cell(const Dev<R>& d, const CaseCfg<R>&
         const double rate = 2 * (double)sspec / ((double)wk.rho * V) + (double)d.srate[k];
         sdt = rate > 0 ? cf.sa_cfl / rate : sdt;
       }
-      cell_dt = rmin(cell_dt, rmin(vdt, sdt));
+      if (cf.srd_rate) {
+        d.ddt[n + k] = vdt;  // mapped through the SRD neighbourhoods before it joins the minimum
+        cell_dt = rmin(cell_dt, sdt);
+      } else {
+        cell_dt = rmin(cell_dt, rmin(vdt, sdt));
+      }
     }
     for (int v = 0; v < nv; ++v) d.R0[v * n + k] = res[v];
   } else if (stage == STAGE_DIAG) {
@@ -904,6 +912,50 @@ __device__ void phase_srd(const Dev<R>& d, int cs, R* u, bool check) {
   __syncthreads();
 }
 
+// SRD-rate viscous stabilization of one case (reference src/static_amr2d_viscous.cpp:123-134):
+// the viscous rates r_k = viscous_cfl / dt_k go through the same redistribution map as the state,
+// R_g = sum_k V_k r_k / N_k / Vhat_g, then r'_k = sum_g R_g / N_k, and dt'_k = viscous_cfl / r'_k.
+// With store the mapped dt'_k replace dt_k in ddt (export); otherwise they join the case's dt
+// minimum.  One block per case; the non-trivial groups use the SRD lists, every other cell the
+// exact one-member form of the same sums.
+template <class R, int MODEL>
+__device__ void srd_rate_case(const Dev<R>& d, int cs, bool store) {
+  const long long n = d.ncap;
+  const CaseCfg<R>& cf = d.cfg[cs];
+  const double vcfl = cf.viscous_cfl, inf = __longlong_as_double(0x7FF0000000000000ll);
+  for (int gi = cf.srd_g0 + threadIdx.x; gi < cf.srd_g1; gi += blockDim.x) {
+    double sum = 0;
+    for (int q = d.g_mem[gi]; q < d.g_mem[gi + 1]; ++q) {
+      const int k = d.g_cell[q];
+      sum += d.c_vol[k] * (vcfl / d.ddt[n + k]) / d.g_cnt[q];
+    }
+    d.qhat[gi] = sum / d.g_vol[gi];
+  }
+  __syncthreads();
+  double best = inf;
+  for (int qi = cf.srd_q0 + threadIdx.x; qi < cf.srd_q1; qi += blockDim.x) {
+    double sum = 0;
+    for (int q = d.q_grp[qi]; q < d.q_grp[qi + 1]; ++q) sum += d.qhat[d.q_list[q]];
+    const double rate = sum / d.q_cnt[qi];
+    const double dt = rate > 0 ? vcfl / rate : inf;
+    if (store) d.ddt[n + d.q_cell[qi]] = dt;
+    best = rmin(best, dt);
+  }
+  for (int k = cf.cell0 + threadIdx.x; k < cf.cell1; k += blockDim.x) {
+    if (!(d.c_flags[k] & 1)) continue;  // non-trivial: done above
+    double s = 0.0;
+    s += d.c_vol[k] * (vcfl / d.ddt[n + k]) / 1.0;
+    double t = 0.0;
+    t += s / d.c_gvol[k];
+    const double rate = t / 1.0;
+    const double dt = rate > 0 ? vcfl / rate : inf;
+    if (store) d.ddt[n + k] = dt;
+    best = rmin(best, dt);
+  }
+  if (!store && best < inf) atomic_min_dt(&d.ctl[cs].dtmin, best);
+  __syncthreads();
+}
+
 // Case begin logic (reference src/static_amr2d_cuda.cu:54-59).
 __device__ __forceinline__ void case_begin(CaseCtl& c) {
   c.active = 0;
@@ -1049,6 +1101,14 @@ __global__ void __launch_bounds__(MAX_BLOCK) trials_kernel(Dev<R> d, int trials,
     }
     tile_sweep<R, MODEL, FLUX, false>(d, STAGE_BASE, sm);
     if (!grid_barrier(bar, lim)) return;
+    if (SRD && MODEL >= MODEL_LAMINAR && d.any_srd_rate) {
+      for (int cs = blockIdx.x; cs < d.n_cases; cs += gridDim.x) {
+        int cur;
+        if (read_case_skip(d.ctl, cs, SKIP_ACTIVE, !d.cfg[cs].srd_rate, &cur)) continue;
+        srd_rate_case<R, MODEL>(d, cs, false);
+      }
+      if (!grid_barrier(bar, lim)) return;
+    }
     // ---- dt and U1
     for (int ti = blockIdx.x * wpb + warp; ti < d.n_tiles; ti += gridDim.x * wpb) {
       const TileView v = read_tile(d.tiles, d.ctl, ti, SKIP_ACTIVE);
@@ -1333,6 +1393,20 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::cell) gather_kernel(
       const int prev = __shfl_up_sync(FULL_MASK, cs, 1);
       if (cs >= 0 && (lane == 0 || prev != cs)) atomicMin(&d.ctl[cs].dtmin, bits);
     }
+  }
+}
+
+template <class R, int MODEL>
+__global__ void __launch_bounds__(MAX_BLOCK) srd_rate_kernel(Dev<R> d, int store_only_case) {
+  for (int cs = blockIdx.x; cs < d.n_cases; cs += gridDim.x) {
+    int cur;
+    if (store_only_case >= 0) {
+      if (cs != store_only_case) continue;
+      srd_rate_case<R, MODEL>(d, cs, true);
+      continue;
+    }
+    if (read_case_skip(d.ctl, cs, SKIP_ACTIVE, !d.cfg[cs].srd_rate, &cur)) continue;
+    srd_rate_case<R, MODEL>(d, cs, false);
   }
 }
 

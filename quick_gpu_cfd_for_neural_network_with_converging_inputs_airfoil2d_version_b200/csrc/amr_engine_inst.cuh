@@ -49,6 +49,7 @@ static cudaError_t launch_phases_t(const Dev<R>& d, bool srd, int trials, int mo
   for (int t = 0; t < trials; ++t) {
     if (MODEL >= MODEL_LAMINAR) phase_grad_kernel<R, MODEL><<<tiles, block, sm, st>>>(d, STAGE_BASE);
     phase_flux_kernel<R, MODEL, FLUX><<<tiles, block, sm, st>>>(d, STAGE_BASE);
+    if (srd && MODEL >= MODEL_LAMINAR && d.any_srd_rate) srd_rate_kernel<R, MODEL><<<cases, MAX_BLOCK, 0, st>>>(d, -1);
     phase_first_cells_kernel<R, MODEL><<<(d.n_cells + 255) / 256 + 1, 256, 0, st>>>(d);
     for (int stage = 1; stage <= 2; ++stage) {
       if (srd) phase_srd_kernel<R, MODEL><<<cases, block, 0, st>>>(d, stage);
@@ -97,6 +98,7 @@ static cudaError_t launch_split_t(const Dev<R>& d, bool srd, int trials, int mod
   phase_commit_kernel<<<kblocks, 128, 0, st>>>(d.ctl, cases, 1);
   for (int t = 0; t < trials; ++t) {
     stage_seq(STAGE_BASE);
+    if (srd && MODEL >= MODEL_LAMINAR && d.any_srd_rate) srd_rate_kernel<R, MODEL><<<cases, MAX_BLOCK, 0, st>>>(d, -1);
     phase_first_cells_kernel<R, MODEL><<<fblocks, 256, 0, st>>>(d);
     for (int stage = 1; stage <= 2; ++stage) {
       if (srd) phase_srd_kernel<R, MODEL><<<cases, MAX_BLOCK, 0, st>>>(d, stage);
@@ -456,6 +458,10 @@ int Batch<R>::export_case(int slot, double* wall_rows, uint64_t wall_count, doub
                                                                         (double)hc.cfg.gamma, dev_walls);
   if (want_sa) export_sa_kernel<R><<<(int)((n + 255) / 256), 256, 0, stream_>>>(d, slot, c0, (int)n, dev_sa);
   export_convective_kernel<R><<<(int)((n + 127) / 128), 128, 0, stream_>>>(d, slot, c0, (int)n);
+  if (hc.cfg.srd_rate) {  // the snapshot's viscous dt is the SRD-mapped one
+    if (model_ == MODEL_LAMINAR) srd_rate_kernel<R, MODEL_LAMINAR><<<config_.max_cases, MAX_BLOCK, 0, stream_>>>(d, slot);
+    if (model_ == MODEL_SA) srd_rate_kernel<R, MODEL_SA><<<config_.max_cases, MAX_BLOCK, 0, stream_>>>(d, slot);
+  }
   export_limits_kernel<R><<<1, 256, 0, stream_>>>(d, c0, (int)n, dev_lim);
   bool ok = cuda_ok(cudaGetLastError(), error, "export launch");
   launches_ += (want_walls && nw > 0) + (want_sa ? 1 : 0) + 2;

@@ -17,10 +17,15 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize('physics,kinds,steps', [
     ('sa', ('farfield',) * 4, 12),
     ('laminar', ('farfield', 'pressure-outlet', 'no-slip', 'no-slip'), 8),
+    ('laminar-srd-rate', ('farfield', 'pressure-outlet', 'farfield', 'farfield'), 6),
 ])
 def test_viscous_snapshot_files_match_reference(tmp_path, physics, kinds, steps):
     naca = (0.02, 0.4, 0.12)
-    spec = cases.CaseSpec(naca=naca, profile='LF1', physics=physics, kinds=kinds)
+    if physics == 'laminar-srd-rate':
+        from tests.test_gpu_parity import srd_rate_spec
+        spec = srd_rate_spec()
+    else:
+        spec = cases.CaseSpec(naca=naca, profile='LF1', physics=physics, kinds=kinds)
     x, y, pt = airfoils.naca4(*naca)
     mesh = builder.build_mesh(spec, x, y, pt)
     rc = RefCase.build(spec, x, y, pt)
@@ -33,6 +38,7 @@ def test_viscous_snapshot_files_match_reference(tmp_path, physics, kinds, steps)
     rows = s.export()
     assert rows['wall_rows'].shape == (mesh.n_walls, 14)
     assert (rows['sa_rows'] is not None) == (physics == 'sa')
+    assert np.isfinite(rows['viscous_dt']) and np.isfinite(rows['convective_dt'])
     (tmp_path / 'ours').mkdir()
     (tmp_path / 'ref').mkdir()
     snapshot.write_snapshot_files(tmp_path / 'ours' / 'raw.final', mesh, spec.params(), u, s.time, s.steps, s.rejected,

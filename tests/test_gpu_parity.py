@@ -237,3 +237,23 @@ def test_control_known_steps_on_gpu(golden, control):
     g = StaticAmrGpu.create(mesh, spec.params(), u0)
     assert g.advance(0.01, 50000000) == 0
     assert g.steps == ka['controls'][control] and g.rejected == 0 and g.time == 0.01
+
+
+def srd_rate_spec():
+    from tests.test_oracle import _with_stabilization
+    spec = cases.CaseSpec(naca=(0.02, 0.4, 0.12), profile='LF1', physics='laminar', agglomerate=False, mach=1.4,
+                          kinds=('farfield', 'pressure-outlet', 'farfield', 'farfield'))
+    base = spec.transport_record
+    spec.transport_record = lambda g=1.4: _with_stabilization(base(g))
+    return spec
+
+
+@pytest.mark.parametrize('mode', ['persistent', 'phases', 'split'])
+def test_srd_rate_viscous_parity(mode):
+    """Laminar on an SRD mesh with the viscous dt limited through the SRD map of the rates."""
+    from tests.test_gpu_launch_modes import MODES
+    spec = srd_rate_spec()
+    x, y, pt = airfoils.naca4(0.02, 0.4, 0.12)
+    mesh = RefCase.build(spec, x, y, pt).mesh()
+    assert mesh.small_cells > 0
+    run_pair(mesh, spec, [1, 12], options=default_options(**MODES[mode]))
