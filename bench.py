@@ -34,6 +34,10 @@ METRIC = 'solves/s & cell-steps/s at |ΔCL|,|ΔCD|≤1e-4 vs plain FP64; p50/p99
 GOLDEN = ROOT / 'tests' / 'golden'
 MESHES = {'LF1': GOLDEN / 'mesh_naca2412_lf1_sa.npz', 'LF2': GOLDEN / 'mesh_naca2412_lf2_sa.npz'}
 SOLVE_STEPS = 5000  # steps per solve of the batched workload
+# DRAM bytes (read + write) of one split-mode trial of the 256-case workload, summed over its
+# kernels from one ncu capture (profiles/split_trial_f32_sa_256cases.md; cold cache, so an upper
+# bound of a warm trial).  Reported as roofline.traffic when the run matches that configuration.
+SPLIT_256_TRAFFIC_PER_STEP = 3.5563e9
 
 
 def peaks():
@@ -127,7 +131,7 @@ def parse_launch(cfg):
     block = int(cfg.split('block=')[1].split()[0])
     grid = int(cfg.split('grid=')[1].split()[0])
     mode = (_abi.LAUNCH_PHASES if 'mode=phases' in cfg else _abi.LAUNCH_SPLIT if 'mode=split' in cfg
-            else _abi.LAUNCH_PERSISTENT)
+            else _abi.LAUNCH_TILED if 'mode=tiled' in cfg else _abi.LAUNCH_PERSISTENT)
     return block, grid, mode
 
 
@@ -369,7 +373,7 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--cases', type=int, default=256)
     ap.add_argument('--no-cpu', action='store_true')
-    ap.add_argument('--profile', choices=['persistent', 'phases', 'split'], default=None,
+    ap.add_argument('--profile', choices=['persistent', 'phases', 'split', 'tiled'], default=None,
                     help='only the timed batched loop, with this launch mode and --block (for ncu)')
     ap.add_argument('--block', type=int, default=128)
     ap.add_argument('--precision', type=int, default=32, choices=[32, 64])
@@ -390,7 +394,8 @@ def main():
         return
     case_list = batched_cases(args.cases, seed=20261203 + rank)
     if args.profile:
-        mode = {'phases': _abi.LAUNCH_PHASES, 'split': _abi.LAUNCH_SPLIT}.get(args.profile, _abi.LAUNCH_PERSISTENT)
+        mode = {'phases': _abi.LAUNCH_PHASES, 'split': _abi.LAUNCH_SPLIT,
+                'tiled': _abi.LAUNCH_TILED}.get(args.profile, _abi.LAUNCH_PERSISTENT)
         b = Batch(precision=args.precision, model=_abi.MODEL_LAMINAR, sa=True, max_cases=len(case_list),
                   max_cells=sum(m.n_cells for _, m in case_list) + 64, device=local, block_threads=args.block,
                   launch_mode=mode)
@@ -434,7 +439,11 @@ def main():
                             solves_per_s=value / mean_cells / SOLVE_STEPS,
                             l2='working set > L2 (no flush needed)', launch=cfg, parallelism='replicas'),
                 roofline=dict(bound='hbm', achieved=achieved, peak=hbm, unit='GB/s', frac=achieved / hbm,
-                              peak_kind=peak_kind, traffic=None, bytes_per_step=bytes_per_step,
+                              peak_kind=peak_kind,
+                              traffic=(SPLIT_256_TRAFFIC_PER_STEP * args.steps / r['advances']
+                                       if 'mode=split' in cfg and args.cases == 256 else None),
+                              traffic_scope='DRAM bytes per launch (a graph of steps_per_launch steps), ncu, cold cache',
+                              bytes_per_step=bytes_per_step,
                               launch_ms=1e3 * per_launch, steps_per_launch=args.steps / r['advances']),
                 e2e=dict(value=e2e_value, unit='cell-steps/s', h2d_bytes_per_step=e2e['h2d'] / args.steps,
                          d2h_bytes_per_step=e2e['d2h'] / args.steps, seconds=e2e['seconds']),

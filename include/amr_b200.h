@@ -258,8 +258,16 @@ enum { AMR_B200_PRECISION_FP64 = 64, AMR_B200_PRECISION_FP32 = 32 };
 /* Launch modes: one persistent cooperative kernel per poll with grid barriers between phases;
  * one kernel per phase (a warp per tile of whole cells) replayed from a CUDA graph; or split,
  * also graph-replayed: gradients one thread per cell, each face flux once (one thread per face
- * or wall record), then one thread per cell gathering its records in order with the update. */
-enum { AMR_B200_LAUNCH_AUTO = 0, AMR_B200_LAUNCH_PERSISTENT = 1, AMR_B200_LAUNCH_PHASES = 2, AMR_B200_LAUNCH_SPLIT = 3 };
+ * or wall record), then one thread per cell gathering its records in order with the update; or
+ * tiled, graph-replayed: one kernel per stage, each block working through block tiles of up to
+ * 128 cells with the cell records and face fluxes of a tile kept in shared memory. */
+enum {
+  AMR_B200_LAUNCH_AUTO = 0,
+  AMR_B200_LAUNCH_PERSISTENT = 1,
+  AMR_B200_LAUNCH_PHASES = 2,
+  AMR_B200_LAUNCH_SPLIT = 3,
+  AMR_B200_LAUNCH_TILED = 4
+};
 
 typedef struct amr_batch_config_t {
   int32_t precision;      /* AMR_B200_PRECISION_FP32 or _FP64 */

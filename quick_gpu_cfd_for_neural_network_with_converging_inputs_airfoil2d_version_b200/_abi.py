@@ -19,7 +19,7 @@ LIMITER_FIRST_ORDER = 3
 TIME_SSP_RK3 = 0
 STATUS_OK, STATUS_NONPHYSICAL_BASE, STATUS_MAXSTEPS, STATUS_DT_UNDERFLOW, STATUS_REJECTIONS, STATUS_BARRIER_TIMEOUT = 0, 2, 3, 4, 5, 9
 PRECISION_FP64, PRECISION_FP32 = 64, 32
-LAUNCH_AUTO, LAUNCH_PERSISTENT, LAUNCH_PHASES, LAUNCH_SPLIT = 0, 1, 2, 3
+LAUNCH_AUTO, LAUNCH_PERSISTENT, LAUNCH_PHASES, LAUNCH_SPLIT, LAUNCH_TILED = 0, 1, 2, 3, 4
 
 CELL_DTYPE = np.dtype([('ix', '<i4'), ('iy', '<i4'), ('span', '<i4'), ('level', '<i4'),
                        ('x0', '<f8'), ('x1', '<f8'), ('y0', '<f8'), ('y1', '<f8'),

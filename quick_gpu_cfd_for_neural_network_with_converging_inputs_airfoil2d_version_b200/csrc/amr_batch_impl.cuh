@@ -93,11 +93,12 @@ struct Range {
 template <class R> struct HostCase {
   bool live = false;
   int n = 0;
-  Range cells, slots, walls, terms, groups, gmembers, qcells, qlist, faces;
+  Range cells, slots, walls, terms, groups, gmembers, qcells, qlist, faces, halo, tfaces;
   int slot = -1;
   std::vector<int> nslot, nterm;  // per-cell slot and gradient-term counts (for tiling)
   std::vector<int> slot_prefix, term_prefix;  // n+1 running sums of nslot / nterm
   std::vector<Tile> tiles;
+  std::vector<BTile> btiles;  // block tiles (tiled mode), global indices
   CaseCfg<R> cfg;
 };
 
@@ -145,6 +146,11 @@ template <class R> class Batch final : public BatchBase {
     a_cells_ = RangeAlloc(cap_cells_);
     a_slots_ = RangeAlloc(cap_slots_);
     a_faces_ = RangeAlloc(cap_faces_);
+    cap_halo_ = 2 * cap_cells_;
+    cap_tface_ = 2 * cap_faces_ + 64;
+    cap_btiles_ = cap_cells_ / 16 + 4 * (long long)c.max_cases;
+    a_halo_ = RangeAlloc(cap_halo_);
+    a_tface_ = RangeAlloc(cap_tface_);
     a_walls_ = RangeAlloc(cap_walls_);
     a_terms_ = RangeAlloc(cap_terms_);
     a_groups_ = RangeAlloc(cap_groups_ + c.max_cases);
@@ -188,7 +194,10 @@ template <class R> class Batch final : public BatchBase {
          f_meta_.alloc(cap_faces_, A, error, "faces") && f_len_.alloc(cap_faces_, A, error, "faces") &&
          f_geo_.alloc(6 * cap_faces_, A, error, "faces") && fval_.alloc(SM_COLS * cap_faces_, A, error, "faces") &&
          w_owner_.alloc(cap_walls_, A, error, "walls") && wval_.alloc(SM_COLS * cap_walls_, A, error, "walls") &&
-         live_end_.alloc(4, A, error, "ranges");
+         live_end_.alloc(4, A, error, "ranges") && btiles_.alloc(cap_btiles_, A, error, "block tiles") &&
+         bt_halo_.alloc(cap_halo_, A, error, "block tiles") && bt_face_.alloc(cap_tface_, A, error, "block tiles") &&
+         bt_floc_.alloc(cap_tface_, A, error, "block tiles") && s_loc_.alloc(cap_slots_, A, error, "slots") &&
+         w_ldon_.alloc(cap_walls_, A, error, "walls");
     if (!ok) return false;
     if (model_ >= MODEL_LAMINAR) {
       ok = crec_.alloc(CREC * nc, A, error, "scratch") && t_own_.alloc(cap_terms_, A, error, "terms") &&
@@ -220,11 +229,12 @@ template <class R> class Batch final : public BatchBase {
     block_ = c.block_threads > 0 ? c.block_threads : 256;
     if (block_ % 32 || block_ < 64 || block_ > MAX_BLOCK) return fail(error, "block_threads must be 64..256, a multiple of 32");
     grid_request_ = c.grid_blocks;
-    if (c.launch_mode < AMR_B200_LAUNCH_AUTO || c.launch_mode > AMR_B200_LAUNCH_SPLIT)
+    if (c.launch_mode < AMR_B200_LAUNCH_AUTO || c.launch_mode > AMR_B200_LAUNCH_TILED)
       return fail(error, "unknown launch mode");
+    if (!cuda_ok(EngineOps<R>::tiled_setup(model_, flux_), error, "tiled kernel shared memory")) return false;
     mode_ = c.launch_mode == AMR_B200_LAUNCH_AUTO ? AMR_B200_LAUNCH_PERSISTENT : c.launch_mode;
     if (mode_ != AMR_B200_LAUNCH_PERSISTENT && block_ != PHASE_BLOCK)
-      return fail(error, "the phase and split launch modes run 128-thread blocks");
+      return fail(error, "the phase, split and tiled launch modes take block_threads 128");
     if (!configure_grid(error)) return false;
     return cuda_ok(cudaStreamSynchronize(stream_), error, "batch init");
   }
@@ -449,6 +459,31 @@ template <class R> class Batch final : public BatchBase {
     c_slot[n] = sb + (int)ns;
     c_wall[n] = wb + (int)nw;
     c_term[n] = tb + (int)nt;
+    // block tiles (tiled mode)
+    std::vector<int> bt_halo, bt_face, s_loc(ns, 0), w_ldon(nw, 0);
+    std::vector<int2> bt_floc;
+    std::vector<BTile> btiles;
+    if (!make_block_tiles(m, n, rec, slot, &btiles, &bt_halo, &bt_face, &bt_floc, &s_loc, &w_ldon, &why))
+      return fail_release(hc, error, why);
+    hc.halo = {a_halo_.alloc((long long)bt_halo.size()), (long long)bt_halo.size()};
+    hc.tfaces = {a_tface_.alloc((long long)bt_face.size()), (long long)bt_face.size()};
+    if (hc.halo.b < 0 || hc.tfaces.b < 0 || n_btiles_total() + (long long)btiles.size() > cap_btiles_) {
+      release_ranges(hc);
+      return 3;
+    }
+    for (BTile& t : btiles) {
+      t.c0 += cb;
+      t.c1 += cb;
+      t.h0 += (int)hc.halo.b;
+      t.h1 += (int)hc.halo.b;
+      t.f0 += (int)hc.tfaces.b;
+      t.f1 += (int)hc.tfaces.b;
+      t.w0 += wb;
+      t.w1 += wb;
+    }
+    for (int& h : bt_halo) h += cb;
+    for (int& f : bt_face) f += fb;
+    hc.btiles = std::move(btiles);
     // SRD arrays
     const int gb = (int)hc.groups.b, gmb = (int)hc.gmembers.b, qb = (int)hc.qcells.b, qlb = (int)hc.qlist.b;
     std::vector<int> g_mem(ng + 1), g_cell(gmem), q_cell(ng + 1, cb + (int)n), q_grp(ng + 1), q_list(qlist);
@@ -551,7 +586,9 @@ template <class R> class Batch final : public BatchBase {
     ok = ok && up(s_geo_.p + 6 * (long long)sb, s_geo, G) && up(s_item_.p + sb, s_item, G) &&
          up(f_case_.p + fb, f_case, G) && up(f_own_.p + fb, f_own, G) && up(f_nb_.p + fb, f_nb, G) &&
          up(f_meta_.p + fb, f_meta, G) && up(f_len_.p + fb, f_len, G) && up(f_geo_.p + 6 * (long long)fb, f_geo, G) &&
-         up(w_owner_.p + wb, w_owner, G);
+         up(w_owner_.p + wb, w_owner, G) && up(bt_halo_.p + hc.halo.b, bt_halo, G) &&
+         up(bt_face_.p + hc.tfaces.b, bt_face, G) && up(bt_floc_.p + hc.tfaces.b, bt_floc, G) &&
+         up(s_loc_.p + sb, s_loc, G) && up(w_ldon_.p + wb, w_ldon, G);
     if (ok && model_ >= MODEL_LAMINAR)
       ok = up(t_own_.p + tb, t_own, G) && up(t_src_.p + tb, t_src, G) &&
            up(t_x_.p + tb, t_x, G) && up(t_y_.p + tb, t_y, G);
@@ -665,7 +702,9 @@ template <class R> class Batch final : public BatchBase {
     if (!sync_tiles(error)) return 1;
     cudaGetLastError();
     if (!enqueue(1, MODE_RESIDUAL, error)) return 1;
-    launches_ += mode_ == AMR_B200_LAUNCH_PERSISTENT ? 1 : (model_ >= MODEL_LAMINAR ? 3 : 2) - (mode_ == AMR_B200_LAUNCH_PHASES);
+    launches_ += mode_ == AMR_B200_LAUNCH_PERSISTENT || mode_ == AMR_B200_LAUNCH_TILED
+                     ? 1
+                     : (model_ >= MODEL_LAMINAR ? 3 : 2) - (mode_ == AMR_B200_LAUNCH_PHASES);
     return cuda_ok(cudaStreamSynchronize(stream_), error, "residual") ? 0 : 1;
   }
 
@@ -708,10 +747,15 @@ template <class R> class Batch final : public BatchBase {
     use_graph_ = on;
     graph_dirty_ = true;
   }
+
   std::string launch_config() const override {
-    const char* name = mode_ == AMR_B200_LAUNCH_PHASES ? "mode=phases" : mode_ == AMR_B200_LAUNCH_SPLIT ? "mode=split" : "mode=persistent";
+    const char* name = mode_ == AMR_B200_LAUNCH_PHASES  ? "mode=phases"
+                       : mode_ == AMR_B200_LAUNCH_SPLIT ? "mode=split"
+                       : mode_ == AMR_B200_LAUNCH_TILED ? "mode=tiled"
+                                                        : "mode=persistent";
     const int grid = mode_ == AMR_B200_LAUNCH_PHASES  ? (n_tiles_ + block_ / 32 - 1) / (block_ / 32)
                      : mode_ == AMR_B200_LAUNCH_SPLIT ? (int)((hw_cells_ + PHASE_BLOCK - 1) / PHASE_BLOCK)
+                     : mode_ == AMR_B200_LAUNCH_TILED ? sms_ * TiledOcc<R>::blocks
                                                       : grid_;
     return std::string(name) + " block=" + std::to_string(block_) + " grid=" + std::to_string(grid) +
            (use_graph_ ? " graph" : " direct");
@@ -858,6 +902,103 @@ template <class R> class Batch final : public BatchBase {
     return make_tiles(hc, &why);
   }
 
+  long long n_btiles_total() const {
+    long long s = 0;
+    for (auto& c : cases_)
+      if (c.live) s += (long long)c.btiles.size();
+    return s;
+  }
+
+  // Block tiles of one case (case-local indices): runs of up to BT_CELLS consecutive cells whose
+  // halo (face neighbours and wall donors outside the run), face records and wall fragments fit
+  // the tiled kernel's shared memory.  Fills per slot its local record (2 * tile face + the cell
+  // is the face's left, or the tile wall index) and per wall the donor's local index.
+  bool make_block_tiles(const amr_mesh_view_t* m, long long n, const std::vector<int>& rec, int slot,
+                        std::vector<BTile>* tiles, std::vector<int>* halo_out, std::vector<int>* face_out,
+                        std::vector<int2>* floc_out, std::vector<int>* s_loc, std::vector<int>* w_ldon,
+                        std::string* why) const {
+    const long long nf = (long long)m->n_faces;
+    const bool viscous = model_ >= MODEL_LAMINAR;
+    std::vector<int> dstamp(n, -1), dloc(n, 0), fstamp(nf, -1), floc(nf, 0);
+    std::vector<int> halo, faces;
+    std::vector<long long> slot_base(n + 1, 0);  // case-local slot index of each cell's first slot
+    for (long long k = 0; k < n; ++k)
+      slot_base[k + 1] = slot_base[k] + (long long)(m->face_offsets[k + 1] - m->face_offsets[k] + m->cells[k].wall_count);
+    int stamp = 0;
+    long long start = 0;
+    while (start < n) {
+      long long end = std::min<long long>(n, start + BT_CELLS);
+      for (;;) {
+        ++stamp;
+        halo.clear();
+        faces.clear();
+        const int nt = (int)(end - start);
+        for (long long k = start; k < end; ++k) {
+          dstamp[k] = stamp;
+          dloc[k] = (int)(k - start);
+        }
+        auto add_cell = [&](long long c) {
+          if (dstamp[c] == stamp) return;
+          dstamp[c] = stamp;
+          dloc[c] = nt + (int)halo.size();
+          halo.push_back((int)c);
+        };
+        for (long long k = start; k < end; ++k) {
+          for (uint64_t q = m->face_offsets[k]; q < m->face_offsets[k + 1]; ++q) {
+            const uint64_t fi = m->cell_faces[q];
+            const amr_face_t& f = m->faces[fi];
+            if (fstamp[fi] != stamp) {
+              fstamp[fi] = stamp;
+              floc[fi] = (int)faces.size();
+              faces.push_back((int)fi);
+            }
+            const int other = f.left == (int)k ? f.right : f.left;
+            if (other >= 0) add_cell(other);
+          }
+          if (viscous)
+            for (uint64_t q = m->cells[k].wall_begin; q < m->cells[k].wall_begin + m->cells[k].wall_count; ++q)
+              add_cell(m->wall_samples[q].donor);
+        }
+        const long long nw = (long long)(m->cells[end - 1].wall_begin + m->cells[end - 1].wall_count) -
+                             (long long)m->cells[start].wall_begin;
+        if (nt + (long long)halo.size() <= BT_DATA && (long long)faces.size() <= BT_FACES && nw <= BT_WALLS) break;
+        if (end - start == 1) return fail(why, "a cell's neighbourhood exceeds the block tile");
+        end = start + std::max<long long>(1, (end - start) * 3 / 4);
+      }
+      BTile t;
+      t.cs = slot;
+      t.c0 = (int)start;
+      t.c1 = (int)end;
+      t.h0 = (int)halo_out->size();
+      t.h1 = t.h0 + (int)halo.size();
+      t.f0 = (int)face_out->size();
+      t.f1 = t.f0 + (int)faces.size();
+      t.w0 = (int)m->cells[start].wall_begin;
+      t.w1 = (int)(m->cells[end - 1].wall_begin + m->cells[end - 1].wall_count);
+      halo_out->insert(halo_out->end(), halo.begin(), halo.end());
+      for (int fi : faces) {
+        const amr_face_t& f = m->faces[fi];
+        const int own = f.left >= 0 ? f.left : f.right, other = f.left >= 0 ? f.right : -1;
+        face_out->push_back(rec[fi]);
+        floc_out->push_back(make_int2(dloc[own], other >= 0 ? dloc[other] : -1));
+      }
+      for (long long k = start; k < end; ++k) {
+        long long q = slot_base[k];
+        for (uint64_t p = m->face_offsets[k]; p < m->face_offsets[k + 1]; ++p, ++q) {
+          const uint64_t fi = m->cell_faces[p];
+          (*s_loc)[q] = 2 * floc[fi] + (m->faces[fi].left == (int)k ? 1 : 0);
+        }
+        for (uint64_t w = m->cells[k].wall_begin; w < m->cells[k].wall_begin + m->cells[k].wall_count; ++w, ++q) {
+          (*s_loc)[q] = (int)(w - (uint64_t)t.w0);
+          if (viscous) (*w_ldon)[w] = dloc[m->wall_samples[w].donor];
+        }
+      }
+      tiles->push_back(t);
+      start = end;
+    }
+    return true;
+  }
+
   long long n_tiles_total() const {
     long long s = 0;
     for (auto& c : cases_)
@@ -875,7 +1016,10 @@ template <class R> class Batch final : public BatchBase {
     a_q_.release(hc.qcells.b, hc.qcells.b >= 0 ? hc.qcells.n : 0);
     a_qlist_.release(hc.qlist.b, hc.qlist.b >= 0 ? hc.qlist.n : 0);
     a_faces_.release(hc.faces.b, hc.faces.b >= 0 ? hc.faces.n : 0);
-    hc.cells = hc.slots = hc.walls = hc.terms = hc.groups = hc.gmembers = hc.qcells = hc.qlist = hc.faces = Range{0, 0};
+    a_halo_.release(hc.halo.b, hc.halo.b >= 0 ? hc.halo.n : 0);
+    a_tface_.release(hc.tfaces.b, hc.tfaces.b >= 0 ? hc.tfaces.n : 0);
+    hc.cells = hc.slots = hc.walls = hc.terms = hc.groups = hc.gmembers = hc.qcells = hc.qlist = hc.faces = hc.halo =
+        hc.tfaces = Range{0, 0};
   }
 
   void refresh_meta(int slot) {
@@ -915,7 +1059,13 @@ template <class R> class Batch final : public BatchBase {
     h_live_end_[0] = (int)hw_cells_;
     h_live_end_[1] = (int)hw_faces_;
     h_live_end_[2] = (int)hw_walls_;
-    h_live_end_[3] = 0;
+    std::vector<BTile> all_bt;
+    for (auto& c : cases_)
+      if (c.live) all_bt.insert(all_bt.end(), c.btiles.begin(), c.btiles.end());
+    h_live_end_[3] = (int)all_bt.size();
+    if (!all_bt.empty() && !cuda_ok(cudaMemcpyAsync(btiles_.p, all_bt.data(), sizeof(BTile) * all_bt.size(),
+                                                    cudaMemcpyHostToDevice, stream_), error, "block tiles"))
+      return false;
     if (!cuda_ok(cudaMemcpyAsync(live_end_.p, h_live_end_, sizeof(h_live_end_), cudaMemcpyHostToDevice, stream_), error,
                  "live ranges"))
       return false;
@@ -929,7 +1079,9 @@ template <class R> class Batch final : public BatchBase {
     tiles_dirty_ = false;
     // a split-mode graph reads the live ranges from the device and keeps its grids; it is
     // recaptured only when the set of kernels changes (SRD launches appear or vanish)
-    if (mode_ != AMR_B200_LAUNCH_SPLIT || any_srd() != graph_srd_ || any_srd_rate() != graph_srd_rate_) graph_dirty_ = true;
+    if ((mode_ != AMR_B200_LAUNCH_SPLIT && mode_ != AMR_B200_LAUNCH_TILED) || any_srd() != graph_srd_ ||
+        any_srd_rate() != graph_srd_rate_)
+      graph_dirty_ = true;
     return cuda_ok(cudaStreamSynchronize(stream_), error, "tiles sync");
   }
 
@@ -1000,6 +1152,12 @@ template <class R> class Batch final : public BatchBase {
     d.w_xm = w_xm_.p;
     d.w_ym = w_ym_.p;
     d.live_end = live_end_.p;
+    d.btiles = btiles_.p;
+    d.bt_halo = bt_halo_.p;
+    d.bt_face = bt_face_.p;
+    d.bt_floc = bt_floc_.p;
+    d.s_loc = s_loc_.p;
+    d.w_ldon = w_ldon_.p;
     d.cap_faces = (int)cap_faces_;
     d.cap_walls = (int)cap_walls_;
     d.n_faces = (int)hw_faces_;
@@ -1017,8 +1175,8 @@ template <class R> class Batch final : public BatchBase {
     // per trial: three flux stages (one kernel, or item + gather), gradients per stage, the
     // first update, SRD after each stage and the commit; plus the opening commit
     const uint64_t flux = mode_ == AMR_B200_LAUNCH_SPLIT ? 2 : 1;
-    const uint64_t per_trial = 3 * flux + (model_ >= MODEL_LAMINAR ? 3 : 0) + 1 + (any_srd() ? 3 : 0) + 1 +
-                               (any_srd_rate() ? 1 : 0);
+    const uint64_t grad = model_ >= MODEL_LAMINAR && mode_ != AMR_B200_LAUNCH_TILED ? 3 : 0;
+    const uint64_t per_trial = 3 * flux + grad + 1 + (any_srd() ? 3 : 0) + 1 + (any_srd_rate() ? 1 : 0);
     return 1 + per_trial * trials;
   }
 
@@ -1058,6 +1216,9 @@ template <class R> class Batch final : public BatchBase {
     } else if (mode_ == AMR_B200_LAUNCH_SPLIT) {
       ok = ok && cuda_ok(EngineOps<R>::launch_split(dev(), model_, flux_, any_srd(), trials, mode, stream_, sms_), error,
                          "split kernel launch");
+    } else if (mode_ == AMR_B200_LAUNCH_TILED) {
+      ok = ok && cuda_ok(EngineOps<R>::launch_tiled(dev(), model_, flux_, any_srd(), trials, mode, stream_, sms_), error,
+                         "tiled kernel launch");
     } else {
       const int grid = mode == MODE_RESIDUAL ? std::min(grid_, std::max(1, (n_tiles_ + block_ / 32 - 1) / (block_ / 32))) : grid_;
       ok = ok && cuda_ok(cudaMemsetAsync(bar_.p, 0, sizeof(GridBarrier), stream_), error, "barrier reset") &&
@@ -1131,6 +1292,7 @@ template <class R> class Batch final : public BatchBase {
     s_own_.free(); s_nb_.free(); s_meta_.free(); s_len_.free(); s_geo_.free(); s_item_.free();
     f_case_.free(); f_own_.free(); f_nb_.free(); f_meta_.free(); f_len_.free(); f_geo_.free(); fval_.free();
     w_owner_.free(); wval_.free(); crec_.free(); live_end_.free(); ddt_.free(); ex_buf_.free();
+    btiles_.free(); bt_halo_.free(); bt_face_.free(); bt_floc_.free(); s_loc_.free(); w_ldon_.free();
     w_nx_.free(); w_ny_.free(); w_len_.free(); w_dist_.free(); w_donor_.free(); w_xm_.free(); w_ym_.free();
     t_own_.free(); t_src_.free(); t_x_.free(); t_y_.free();
     g_mem_.free(); g_cell_.free(); g_cnt_.free(); g_vol_.free(); q_cell_.free(); q_grp_.free(); q_list_.free(); q_cnt_.free();
@@ -1146,9 +1308,15 @@ template <class R> class Batch final : public BatchBase {
   long long hw_cells_ = 0, hw_faces_ = 0, hw_walls_ = 0;
   int h_live_end_[4] = {0, 0, 0, 0};
   bool graph_srd_ = false, graph_srd_rate_ = false;
+
   DevBuf<int> live_end_;
   long long cap_faces_ = 0;
   RangeAlloc a_faces_;
+  long long cap_halo_ = 0, cap_tface_ = 0, cap_btiles_ = 0;
+  RangeAlloc a_halo_, a_tface_;
+  DevBuf<BTile> btiles_;
+  DevBuf<int> bt_halo_, bt_face_, s_loc_, w_ldon_;
+  DevBuf<int2> bt_floc_;
   long long cap_cells_ = 0, cap_slots_ = 0, cap_walls_ = 0, cap_terms_ = 0, cap_groups_ = 0, cap_gmem_ = 0, cap_q_ = 0,
             cap_qlist_ = 0, cap_tiles_ = 0;
   RangeAlloc a_cells_, a_slots_, a_walls_, a_terms_, a_groups_, a_gmem_, a_q_, a_qlist_;

@@ -63,6 +63,21 @@ template <class R> struct CaseCfg {
 struct Tile {
   int cs, c0, c1, leader, s0, s1, t0, t1;
 };
+
+// A block tile (tiled mode): cells [c0, c1) of case cs, their halo cells bt_halo[h0, h1) (face
+// neighbours and wall donors outside the range), the face records bt_face[f0, f1) touching the
+// cells, and the cells' wall fragments [w0, w1).
+struct BTile {
+  int cs, c0, c1, h0, h1, f0, f1, w0, w1;
+};
+#ifndef AMRB_BT_CELLS
+#define AMRB_BT_CELLS 128
+#endif
+constexpr int BT_CELLS = AMRB_BT_CELLS;  // cells per block tile
+constexpr int BT_DATA = 2 * BT_CELLS;    // tile + halo cells (packed records in shared memory)
+constexpr int BT_FACES = 3 * BT_CELLS;   // face records per tile
+constexpr int BT_WALLS = BT_CELLS;       // wall fragments per tile
+constexpr int BT_THREADS = 2 * BT_CELLS;
 constexpr int SLOT_WALL = 1 << 9;  // s_meta flag: the slot is a wall fragment of its owner cell
 // A tile is processed by one warp: at most TILE_W slots and TILE_W gradient terms of whole cells,
 // synchronised by __syncwarp only, so the warps of a block never wait for one another.
@@ -146,6 +161,13 @@ template <class R> struct Dev {
   R* fval;          // 12 per face
   R* wval;          // 12 per wall
   R* crec;          // CREC per cell: packed state and gradient-phase fields (viscous models)
+  // tiled mode
+  const BTile* btiles;
+  const int* bt_halo;   // global cell index per halo entry
+  const int* bt_face;   // global face record index per tile face entry
+  const int2* bt_floc;  // local (tile data) index of the face's own and other cell (-1 outside)
+  const int* s_loc;     // per slot: 2 * tile face + (cell is the face's left), or the tile wall index
+  const int* w_ldon;    // per wall: local data index of the donor cell
   double* ddt;      // 2 per cell: convective and viscous dt limits of the last residual pass
   int any_srd_rate; // some live case limits its viscous dt through the SRD map
   const double* w_xm;  // wall midpoints
@@ -311,7 +333,7 @@ template <class R, int MODEL> __device__ __forceinline__ void load_cell_record(c
 // SA diffusion 13.
 template <class R, int MODEL>
 __device__ __forceinline__ bool grad_finish(const Dev<R>& d, const CaseCfg<R>& cf, int k, const R* Uin, const R* gr,
-                                            const R* sg, bool soa = true, R* rec = nullptr) {
+                                            const R* sg, bool soa = true, R* rec = nullptr, bool src_out = true) {
   const long long n = d.ncap;
   const Prim<R> w = prim(Uin, n, k, cf.gamma);
   const R mu = dyn_visc(cf.trn, w.p / (w.rho * cf.trn.gas_constant));
@@ -333,8 +355,10 @@ __device__ __forceinline__ bool grad_finish(const Dev<R>& d, const CaseCfg<R>& c
       d.sdiff[k] = pt.diffusion;
     }
     sdiff = pt.diffusion;
-    d.ssrc[k] = src;
-    d.srate[k] = pt.source_rate;
+    if (src_out) {
+      d.ssrc[k] = src;
+      d.srate[k] = pt.source_rate;
+    }
     if (!(pt.diffusion > R(0)) || !isfinite(src) || !isfinite(pt.source_rate)) bad = true;
   }
   if (soa) d.eddy[k] = eddy;
@@ -1410,6 +1434,142 @@ __global__ void __launch_bounds__(MAX_BLOCK) srd_rate_kernel(Dev<R> d, int store
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// Tiled mode: one kernel per stage.  Each block takes one block tile at a time and keeps every
+// intermediate in shared memory: (A) the packed records of the tile's cells and halo cells
+// (state, gradients, viscosity, SA fields; each cell's LSQ sums in term order), (B) the fluxes of
+// every face record and wall fragment touching the tile's cells (a face on the tile's border is
+// evaluated by both tiles, each time identically), (C) per cell, the in-order sums over its
+// slots, the residual, dt and the stage update.  Same arithmetic as the other modes.
+// ------------------------------------------------------------------------------------------
+template <class R> struct TiledOcc;
+template <> struct TiledOcc<float> { static constexpr int blocks = 512 / BT_CELLS; };
+template <> struct TiledOcc<double> { static constexpr int blocks = 1; };
+
+template <class R> __host__ __device__ constexpr size_t tiled_smem_bytes() {
+  return sizeof(R) * ((size_t)BT_DATA * CREC + (size_t)(BT_FACES + BT_WALLS) * SM_COLS);
+}
+
+// A slot's record from the tile's shared-memory records, flux columns signed for the slot's cell.
+template <class R, int MODEL> struct TileSlots {
+  const R* fr;  // face records then wall records, SM_COLS each
+  const int* s_loc;
+  int nf;
+  __device__ __forceinline__ void operator()(int q, bool wall, R* col) const {
+    const int loc = __ldg(s_loc + q);
+    const R* src = fr + SM_COLS * (wall ? nf + loc : loc >> 1);
+    const R sg = (wall || (loc & 1)) ? R(1) : R(-1);
+    for (int c = 0; c < SM_COLS; ++c) col[c] = src[c];
+    for (int v = 0; v < 4; ++v) col[v] = sg * col[v];
+    if (MODEL >= MODEL_LAMINAR)
+      for (int v = 4; v < 8; ++v) col[v] = sg * col[v];
+    if (MODEL == MODEL_SA) col[10] = sg * col[10];
+  }
+};
+
+template <class R, int MODEL, int FLUX>
+__global__ void __launch_bounds__(BT_THREADS, TiledOcc<R>::blocks) tiled_stage_kernel(Dev<R> d, int stage) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* cr = reinterpret_cast<R*>(smem_raw);  // BT_DATA x CREC
+  R* fr = cr + BT_DATA * CREC;             // (BT_FACES + BT_WALLS) x SM_COLS
+  __shared__ unsigned long long block_dt;
+  const int rule = stage_rule(stage);
+  const bool base = stage == STAGE_BASE;
+  const bool spec = base || stage == STAGE_DIAG;
+  const long long n = d.ncap;
+  const int ntiles = d.live_end[3];
+  for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+    const BTile t = d.btiles[ti];
+    int cur;
+    // one thread reads the control word for the block (other tiles may flag the case meanwhile)
+    if (read_case_skip(d.ctl, t.cs, rule, false, &cur)) continue;
+    const CaseCfg<R>& cf = d.cfg[t.cs];
+    const R* Uin = stage_input(d, stage, cur);
+    const int nt = t.c1 - t.c0, nd = nt + (t.h1 - t.h0), nf = t.f1 - t.f0, nw = t.w1 - t.w0;
+    if (threadIdx.x == 0) block_dt = DT_INF_BITS;
+    bool bad = false;
+    // (A) packed records of the tile and halo cells
+    for (int i = threadIdx.x; i < nd; i += blockDim.x) {
+      const bool own = i < nt;
+      const int k = own ? t.c0 + i : __ldg(d.bt_halo + t.h0 + i - nt);
+      R* rec = cr + CREC * i;
+      if (MODEL >= MODEL_LAMINAR) {
+        R gr[4] = {0, 0, 0, 0}, sg[4] = {0, 0, 0, 0};
+        for (int q = d.c_term[k]; q < d.c_term[k + 1]; ++q) {
+          R tv[8];
+          term_values<R, MODEL>(d, cf, q, k, Uin, tv);
+          for (int v = 0; v < 4; ++v) gr[v] += tv[v];
+          if (MODEL == MODEL_SA)
+            for (int v = 0; v < 4; ++v) sg[v] += tv[4 + v];
+        }
+        if (!grad_finish<R, MODEL>(d, cf, k, Uin, gr, sg, own && stage == STAGE_DIAG, rec, own) && own) bad = true;
+      } else {
+        for (int v = 0; v < 4; ++v) rec[v] = Uin[v * n + k];
+        rec[4] = R(0);
+      }
+    }
+    __syncthreads();
+    // (B) face and wall fluxes into shared records
+    for (int j = threadIdx.x; j < nf + nw; j += blockDim.x) {
+      R* out = fr + SM_COLS * j;
+      if (j < nf) {
+        const int f = __ldg(d.bt_face + t.f0 + j);
+        const int2 loc = d.bt_floc[t.f0 + j];
+        const R* a = cr + CREC * loc.x;
+        const R* b = cr + CREC * (loc.y >= 0 ? loc.y : loc.x);
+        FaceIn<R> in;
+        for (int v = 0; v < 5; ++v) { in.uk[v] = a[v]; in.um[v] = b[v]; }
+        in.mk = in.mm = in.ek = in.em = in.sdk = in.sdm = 0;
+        in.sgk[0] = in.sgk[1] = in.sgm[0] = in.sgm[1] = 0;
+        if (MODEL >= MODEL_LAMINAR) {
+          for (int v = 0; v < 4; ++v) { in.gk[v] = a[5 + v]; in.gm[v] = b[5 + v]; }
+          in.mk = a[9]; in.mm = b[9]; in.ek = a[10]; in.em = b[10];
+          if (MODEL == MODEL_SA) {
+            in.sgk[0] = a[11]; in.sgk[1] = a[12]; in.sgm[0] = b[11]; in.sgm[1] = b[12];
+            in.sdk = a[13]; in.sdm = b[13];
+          }
+          for (int v = 0; v < 6; ++v) in.geo[v] = __ldg(d.f_geo + 6 * (long long)f + v);
+        }
+        face_fluxes<R, MODEL, FLUX>(cf, in, __ldg(d.f_len + f), loc.y, __ldg(d.f_meta + f), spec, out, 1, false, bad);
+      } else {
+        const int w = t.w0 + j - nf;
+        const R* a = cr + CREC * (d.w_owner[w] - t.c0);
+        WallIn<R> in;
+        for (int v = 0; v < 4; ++v) in.uk[v] = a[v];
+        in.mk = in.md = 0;
+        in.ud[0] = in.ud[1] = in.ud[2] = in.ud[3] = in.ud[4] = 0;
+        if (MODEL >= MODEL_LAMINAR) {
+          const R* b = cr + CREC * __ldg(d.w_ldon + w);
+          for (int v = 0; v < 5; ++v) in.ud[v] = b[v];
+          in.mk = a[9];
+          in.md = b[9];
+        }
+        wall_fluxes<R, MODEL>(cf, in, __ldg(d.w_nx + w), __ldg(d.w_ny + w), __ldg(d.w_dist + w), __ldg(d.w_len + w),
+                              spec, out, 1, bad);
+      }
+    }
+    __syncthreads();
+    // (C) per-cell sums, residual, dt and the stage update
+    double cell_dt = __longlong_as_double(0x7FF0000000000000ll);
+    for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+      const int k = t.c0 + i;
+      const int a = d.c_slot[k], b = d.c_slot[k + 1];
+      const int e = b - (d.c_wall[k + 1] - d.c_wall[k]);
+      cell_dt = rmin(cell_dt, finish_cell<R, MODEL>(d, cf, t.cs, k, stage, a, e, b, TileSlots<R, MODEL>{fr, d.s_loc, nf},
+                                                    Uin, state_buf(d, cur), state_buf(d, cur ^ 1), bad));
+    }
+    if (bad && stage != STAGE_DIAG) atomicOr(&d.ctl[t.cs].bad, 1);
+    if (base) {
+      for (int o = 16; o > 0; o >>= 1) cell_dt = rmin(cell_dt, __shfl_xor_sync(FULL_MASK, cell_dt, o));
+      if ((threadIdx.x & 31) == 0 && cell_dt < __longlong_as_double(0x7FF0000000000000ll))
+        atomicMin(&block_dt, (unsigned long long)__double_as_longlong(cell_dt));
+    }
+    __syncthreads();
+    if (base && threadIdx.x == 0 && block_dt != DT_INF_BITS) atomicMin(&d.ctl[t.cs].dtmin, block_dt);
+    __syncthreads();  // the shared records are reused by the next tile
+  }
+}
+
 // Host-visible launch helpers (defined in amr_engine_f64.cu / amr_engine_f32.cu).
 template <class R> struct EngineOps {
   static cudaError_t launch(const Dev<R>& d, int model, int flux, bool srd, int trials, int mode, int grid, int block,
@@ -1420,6 +1580,11 @@ template <class R> struct EngineOps {
   // The same with the split kernels (gradients per cell, fluxes per face record, gather per cell).
   static cudaError_t launch_split(const Dev<R>& d, int model, int flux, bool srd, int trials, int mode,
                                   cudaStream_t stream, int sms);
+  // The same with one shared-memory tiled kernel per stage.
+  static cudaError_t launch_tiled(const Dev<R>& d, int model, int flux, bool srd, int trials, int mode,
+                                  cudaStream_t stream, int sms);
+  // Lets the tiled kernel of a model and flux use its shared-memory tile (above the 48 KB default).
+  static cudaError_t tiled_setup(int model, int flux);
   static cudaError_t occupancy(int model, int flux, bool srd, int block, int* blocks_per_sm);
   static size_t smem_bytes(int block) { return size_t(12) * block * sizeof(R); }
 };

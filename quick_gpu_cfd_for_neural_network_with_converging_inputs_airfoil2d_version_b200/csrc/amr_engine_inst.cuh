@@ -123,6 +123,60 @@ cudaError_t EngineOps<R>::launch_split(const Dev<R>& d, int model, int flux, boo
                            : launch_split_t<R, MODEL_SA, FLUX_AUSM>(d, srd, trials, mode, stream, sms);
 }
 
+template <class R, int MODEL, int FLUX>
+static cudaError_t launch_tiled_t(const Dev<R>& d, bool srd, int trials, int mode, cudaStream_t st, int sms) {
+  const size_t sm = tiled_smem_bytes<R>();
+  const int grid = sms * TiledOcc<R>::blocks;
+  const int cases = d.n_cases;
+  const int kblocks = (cases + 127) / 128;
+  const int fblocks = (int)std::min<long long>((d.ncap + 255) / 256, (long long)sms * 8);
+  if (mode == MODE_RESIDUAL) {
+    tiled_stage_kernel<R, MODEL, FLUX><<<grid, BT_THREADS, sm, st>>>(d, STAGE_DIAG);
+    return cudaGetLastError();
+  }
+  phase_commit_kernel<<<kblocks, 128, 0, st>>>(d.ctl, cases, 1);
+  for (int t = 0; t < trials; ++t) {
+    tiled_stage_kernel<R, MODEL, FLUX><<<grid, BT_THREADS, sm, st>>>(d, STAGE_BASE);
+    if (srd && MODEL >= MODEL_LAMINAR && d.any_srd_rate) srd_rate_kernel<R, MODEL><<<cases, MAX_BLOCK, 0, st>>>(d, -1);
+    phase_first_cells_kernel<R, MODEL><<<fblocks, 256, 0, st>>>(d);
+    for (int stage = 1; stage <= 2; ++stage) {
+      if (srd) phase_srd_kernel<R, MODEL><<<cases, MAX_BLOCK, 0, st>>>(d, stage);
+      tiled_stage_kernel<R, MODEL, FLUX><<<grid, BT_THREADS, sm, st>>>(d, stage);
+    }
+    if (srd) phase_srd_kernel<R, MODEL><<<cases, MAX_BLOCK, 0, st>>>(d, 3);
+    phase_commit_kernel<<<kblocks, 128, 0, st>>>(d.ctl, cases, 0);
+  }
+  return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t EngineOps<R>::launch_tiled(const Dev<R>& d, int model, int flux, bool srd, int trials, int mode,
+                                       cudaStream_t stream, int sms) {
+  if (model == MODEL_EULER)
+    return flux == FLUX_HLLC ? launch_tiled_t<R, MODEL_EULER, FLUX_HLLC>(d, srd, trials, mode, stream, sms)
+                             : launch_tiled_t<R, MODEL_EULER, FLUX_AUSM>(d, srd, trials, mode, stream, sms);
+  if (model == MODEL_LAMINAR)
+    return flux == FLUX_HLLC ? launch_tiled_t<R, MODEL_LAMINAR, FLUX_HLLC>(d, srd, trials, mode, stream, sms)
+                             : launch_tiled_t<R, MODEL_LAMINAR, FLUX_AUSM>(d, srd, trials, mode, stream, sms);
+  return flux == FLUX_HLLC ? launch_tiled_t<R, MODEL_SA, FLUX_HLLC>(d, srd, trials, mode, stream, sms)
+                           : launch_tiled_t<R, MODEL_SA, FLUX_AUSM>(d, srd, trials, mode, stream, sms);
+}
+
+template <class R> cudaError_t EngineOps<R>::tiled_setup(int model, int flux) {
+  const int bytes = (int)tiled_smem_bytes<R>();
+  const void* k;
+  if (model == MODEL_EULER)
+    k = flux == FLUX_HLLC ? (const void*)tiled_stage_kernel<R, MODEL_EULER, FLUX_HLLC>
+                          : (const void*)tiled_stage_kernel<R, MODEL_EULER, FLUX_AUSM>;
+  else if (model == MODEL_LAMINAR)
+    k = flux == FLUX_HLLC ? (const void*)tiled_stage_kernel<R, MODEL_LAMINAR, FLUX_HLLC>
+                          : (const void*)tiled_stage_kernel<R, MODEL_LAMINAR, FLUX_AUSM>;
+  else
+    k = flux == FLUX_HLLC ? (const void*)tiled_stage_kernel<R, MODEL_SA, FLUX_HLLC>
+                          : (const void*)tiled_stage_kernel<R, MODEL_SA, FLUX_AUSM>;
+  return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
 template <class R> cudaError_t EngineOps<R>::occupancy(int model, int flux, bool srd, int block, int* blocks_per_sm) {
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel_for<R>(model, flux, srd), block,
                                                        smem_bytes(block));
@@ -247,7 +301,7 @@ template <class R> int Batch<R>::autotune(int trials, std::string* error) {
   int best_mode = mode_;
   const bool graph_save = use_graph_;
   use_graph_ = false;
-  for (int mode : {AMR_B200_LAUNCH_PERSISTENT, AMR_B200_LAUNCH_PHASES, AMR_B200_LAUNCH_SPLIT}) {
+  for (int mode : {AMR_B200_LAUNCH_PERSISTENT, AMR_B200_LAUNCH_PHASES, AMR_B200_LAUNCH_SPLIT, AMR_B200_LAUNCH_TILED}) {
     for (int block : {128, 256}) {
       if (mode != AMR_B200_LAUNCH_PERSISTENT && block != PHASE_BLOCK) continue;
       mode_ = mode;

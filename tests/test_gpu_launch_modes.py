@@ -20,6 +20,7 @@ MODES = {
     'persistent': dict(launch_mode=_abi.LAUNCH_PERSISTENT, block_threads=256),
     'phases': dict(launch_mode=_abi.LAUNCH_PHASES, block_threads=128),
     'split': dict(launch_mode=_abi.LAUNCH_SPLIT, block_threads=128),
+    'tiled': dict(launch_mode=_abi.LAUNCH_TILED, block_threads=128),
 }
 
 
@@ -61,8 +62,8 @@ def test_session_modes_bit_exact(golden):
             outs[mode] = s.download()
             err = rel_err(outs[mode], ref['u'], mesh.nv)
             assert err <= TOL, (name, mode, err)
-        assert np.array_equal(outs['persistent'], outs['split']), name
-        assert np.array_equal(outs['phases'], outs['split']), name
+        for mode in MODES:
+            assert np.array_equal(outs[mode], outs['split']), (name, mode)
 
 
 def test_session_residual_all_modes(golden):
@@ -74,7 +75,8 @@ def test_session_residual_all_modes(golden):
         s = StaticAmrGpu.create(mesh, spec.params(), u0, options=default_options(**opts))
         s.advance(1e30, 3)
         res.append(s.residual())
-    assert np.array_equal(res[0], res[1]) and np.array_equal(res[1], res[2])
+    for r in res[1:]:
+        assert np.array_equal(res[0], r)
 
 
 def sa_mix():
@@ -107,30 +109,33 @@ def run_batch(cases_list, precision, nsteps, mode, order=None):
     return out
 
 
-def test_batch_fp64_split_matches_persistent():
+@pytest.mark.parametrize('mode', ['split', 'tiled'])
+def test_batch_fp64_matches_persistent(mode):
     mix = sa_mix()
     a = run_batch(mix, 64, 20, 'persistent')
-    b = run_batch(mix, 64, 20, 'split', order=[2, 0, 1])
+    b = run_batch(mix, 64, 20, mode, order=[2, 0, 1])
     for i in a:
         assert np.array_equal(a[i], b[i]), i
 
 
-def test_batch_fp32_split_alone_and_in_mix_and_close_to_fused():
+@pytest.mark.parametrize('mode', ['split', 'tiled'])
+def test_batch_fp32_alone_and_in_mix_and_close_to_fused(mode):
     mix = sa_mix()
-    split = run_batch(mix, 32, 40, 'split', order=[1, 2, 0])
+    got = run_batch(mix, 32, 40, mode, order=[1, 2, 0])
     fused = run_batch(mix, 32, 40, 'phases')
     for i in range(len(mix)):
-        alone = run_batch([mix[i]], 32, 40, 'split')
-        assert np.array_equal(split[i], alone[0]), i
-        assert rel_err(split[i], fused[i], 5) <= 1e-5, (i, rel_err(split[i], fused[i], 5))
+        alone = run_batch([mix[i]], 32, 40, mode)
+        assert np.array_equal(got[i], alone[0]), i
+        assert rel_err(got[i], fused[i], 5) <= 1e-5, (i, rel_err(got[i], fused[i], 5))
 
 
-def test_split_release_and_readmit_reuses_records():
-    """A released case's face and wall records are dead; a new case admitted into the freed
+@pytest.mark.parametrize('mode', ['split', 'tiled'])
+def test_release_and_readmit_reuses_ranges(mode):
+    """A released case's records and block tiles are dead; a new case admitted into the freed
     ranges computes exactly what it computes in a fresh batch."""
     mix = sa_mix()
     b = Batch(precision=64, model=_abi.MODEL_LAMINAR, sa=True, max_cases=4,
-              max_cells=sum(m.n_cells for _, m in mix) + 1000, **MODES['split'])
+              max_cells=sum(m.n_cells for _, m in mix) + 1000, **MODES[mode])
     specs = []
     for spec, mesh in mix[:2]:
         u0 = cases.initial_state(mesh, spec.initial_primitive())
@@ -143,5 +148,6 @@ def test_split_release_and_readmit_reuses_records():
     for _ in range(4):
         b.advance(16)
     assert b.status(s)['status'] == _abi.STATUS_MAXSTEPS
-    fresh = run_batch([mix[2]], 64, 10, 'split')
+    fresh = run_batch([mix[2]], 64, 10, mode)
     assert np.array_equal(b.download(s), fresh[0])
+
