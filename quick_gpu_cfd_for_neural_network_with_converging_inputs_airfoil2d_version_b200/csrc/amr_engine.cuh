@@ -706,6 +706,11 @@ __device__ __forceinline__ void wall_fluxes(const CaseCfg<R>& cf, const WallIn<R
   }
 }
 
+// The 12 values of one slot, returned by value so that they stay in registers.
+template <class R> struct Cols {
+  R v[SM_COLS];
+};
+
 // Per-cell end of the F phase: in-order sums of the cell's slot values (faces [a, e) in CSR order,
 // then walls [e, b)), residual, cell dt (base stage) and the stage update.  get(q, col) yields
 // the 12 values of slot q with the flux columns signed for cell k.  Returns the cell dt.
@@ -723,8 +728,8 @@ __device__ __forceinline__ double finish_cell(const Dev<R>& d, const CaseCfg<R>&
   R sum[4] = {0, 0, 0, 0}, vs[4] = {0, 0, 0, 0}, spectral = 0, vspec = 0, snet = 0, sspec = 0;
   for (int q = a; q < b; ++q) {
     const bool wall = q >= e;
-    R col[SM_COLS];
-    get(q, wall, col);
+    const Cols<R> cc = get(q, wall);
+    const R* col = cc.v;
     if (!wall) {
       for (int v = 0; v < 4; ++v) sum[v] += col[v];
     } else {
@@ -803,8 +808,10 @@ __device__ __forceinline__ double finish_cell(const Dev<R>& d, const CaseCfg<R>&
 
 template <class R> struct SmemSlots {
   const R* sm;
-  __device__ __forceinline__ void operator()(int q, bool, R* col) const {
-    for (int c = 0; c < SM_COLS; ++c) col[c] = sm[c * TILE_W + q];
+  __device__ __forceinline__ Cols<R> operator()(int q, bool) const {
+    Cols<R> o;
+    for (int c = 0; c < SM_COLS; ++c) o.v[c] = sm[c * TILE_W + q];
+    return o;
   }
 };
 
@@ -1275,8 +1282,13 @@ static __global__ void phase_commit_kernel(CaseCtl* ctl, int n_cases, int begin_
 #define AMRB_SPLIT_CELL_MINB_F32 12
 #endif
 template <class R> struct SplitOcc;
-template <> struct SplitOcc<float> { static constexpr int item = AMRB_SPLIT_MINB_F32, cell = AMRB_SPLIT_CELL_MINB_F32; };
-template <> struct SplitOcc<double> { static constexpr int item = 3, cell = 4; };
+#ifndef AMRB_SPLIT_GATHER_MINB_F32
+#define AMRB_SPLIT_GATHER_MINB_F32 AMRB_SPLIT_CELL_MINB_F32
+#endif
+template <> struct SplitOcc<float> {
+  static constexpr int item = AMRB_SPLIT_MINB_F32, cell = AMRB_SPLIT_CELL_MINB_F32, gather = AMRB_SPLIT_GATHER_MINB_F32;
+};
+template <> struct SplitOcc<double> { static constexpr int item = 3, cell = 4, gather = 4; };
 
 __device__ __forceinline__ int stage_rule(int stage) {
   return stage == STAGE_DIAG ? SKIP_LIVE : (stage == STAGE_BASE ? SKIP_ACTIVE : SKIP_STAGE);
@@ -1371,20 +1383,24 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::item) item_kernel(De
 template <class R, int MODEL> struct ItemSlots {
   const Dev<R>* d;
   bool base;
-  __device__ __forceinline__ void operator()(int q, bool wall, R* col) const {
+  __device__ __forceinline__ Cols<R> operator()(int q, bool wall) const {
     const int id = __ldg(d->s_item + q);  // wall index, or 2 * face record + (cell is the face's left)
     const R* src = wall ? d->wval + SM_COLS * (long long)id : d->fval + SM_COLS * (long long)(id >> 1);
+    Cols<R> o;
+    R* col = o.v;
+    for (int c = 0; c < SM_COLS; ++c) col[c] = R(0);
     load_record<R, MODEL>(src, col, base);
     const R sg = (wall || (id & 1)) ? R(1) : R(-1);
     for (int v = 0; v < 4; ++v) col[v] = sg * col[v];
     if (MODEL >= MODEL_LAMINAR)
       for (int v = 4; v < 8; ++v) col[v] = sg * col[v];
     if (MODEL == MODEL_SA) col[10] = sg * col[10];
+    return o;
   }
 };
 
 template <class R, int MODEL>
-__global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::cell) gather_kernel(Dev<R> d, int stage) {
+__global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::gather) gather_kernel(Dev<R> d, int stage) {
   const int rule = stage_rule(stage);
   const int ncells = d.live_end[0];
   const bool base = stage == STAGE_BASE;
@@ -1455,15 +1471,18 @@ template <class R, int MODEL> struct TileSlots {
   const R* fr;  // face records then wall records, SM_COLS each
   const int* s_loc;
   int nf;
-  __device__ __forceinline__ void operator()(int q, bool wall, R* col) const {
+  __device__ __forceinline__ Cols<R> operator()(int q, bool wall) const {
     const int loc = __ldg(s_loc + q);
     const R* src = fr + SM_COLS * (wall ? nf + loc : loc >> 1);
     const R sg = (wall || (loc & 1)) ? R(1) : R(-1);
+    Cols<R> o;
+    R* col = o.v;
     for (int c = 0; c < SM_COLS; ++c) col[c] = src[c];
     for (int v = 0; v < 4; ++v) col[v] = sg * col[v];
     if (MODEL >= MODEL_LAMINAR)
       for (int v = 4; v < 8; ++v) col[v] = sg * col[v];
     if (MODEL == MODEL_SA) col[10] = sg * col[10];
+    return o;
   }
 };
 

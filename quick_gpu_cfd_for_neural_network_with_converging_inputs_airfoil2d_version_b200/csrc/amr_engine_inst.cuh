@@ -82,6 +82,7 @@ static cudaError_t launch_split_t(const Dev<R>& d, bool srd, int trials, int mod
   const int B = PHASE_BLOCK;
   const long long ncap = d.ncap, icap = (long long)d.cap_faces + d.cap_walls;
   const int cblocks = (int)std::min<long long>((ncap + B - 1) / B, (long long)sms * SplitOcc<R>::cell);
+  const int gblocks = (int)std::min<long long>((ncap + B - 1) / B, (long long)sms * SplitOcc<R>::gather);
   const int iblocks = (int)std::min<long long>((icap + B - 1) / B, (long long)sms * SplitOcc<R>::item);
   const int fblocks = (int)std::min<long long>((ncap + 255) / 256, (long long)sms * 8);
   const int cases = d.n_cases;
@@ -89,7 +90,7 @@ static cudaError_t launch_split_t(const Dev<R>& d, bool srd, int trials, int mod
   auto stage_seq = [&](int stage) {
     if (MODEL >= MODEL_LAMINAR) grad_cells_kernel<R, MODEL><<<cblocks, B, 0, st>>>(d, stage);
     item_kernel<R, MODEL, FLUX><<<iblocks, B, 0, st>>>(d, stage);
-    gather_kernel<R, MODEL><<<cblocks, B, 0, st>>>(d, stage);
+    gather_kernel<R, MODEL><<<gblocks, B, 0, st>>>(d, stage);
   };
   if (mode == MODE_RESIDUAL) {
     stage_seq(STAGE_DIAG);
