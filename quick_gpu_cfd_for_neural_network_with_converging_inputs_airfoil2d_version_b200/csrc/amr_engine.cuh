@@ -908,27 +908,34 @@ template <class R, int MODEL>
 __device__ void phase_srd(const Dev<R>& d, int cs, R* u, bool check) {
   const long long n = d.ncap, gc = d.gcap;
   const CaseCfg<R>& cf = d.cfg[cs];
+  // one pass over the members with the four sums side by side: each member's loads are issued
+  // together, and each sum still adds its terms in member order
   for (int gi = cf.srd_g0 + threadIdx.x; gi < cf.srd_g1; gi += blockDim.x) {
     const int m0 = d.g_mem[gi], m1 = d.g_mem[gi + 1];
-    for (int v = 0; v < 4; ++v) {
-      double sum = 0;
-      for (int q = m0; q < m1; ++q) {
-        const int k = d.g_cell[q];
-        sum += d.c_vol[k] * (double)u[v * n + k] / d.g_cnt[q];
-      }
-      d.qhat[v * gc + gi] = sum / d.g_vol[gi];
+    double sum[4] = {0, 0, 0, 0};
+    for (int q = m0; q < m1; ++q) {
+      const int k = d.g_cell[q];
+      const double vol = d.c_vol[k], cnt = d.g_cnt[q];
+      const double uk[4] = {(double)u[k], (double)u[n + k], (double)u[2 * n + k], (double)u[3 * n + k]};
+      for (int v = 0; v < 4; ++v) sum[v] += vol * uk[v] / cnt;
     }
+    const double gv = d.g_vol[gi];
+    for (int v = 0; v < 4; ++v) d.qhat[v * gc + gi] = sum[v] / gv;
   }
   __syncthreads();
   bool bad = false;
   const R g = cf.gamma;
   for (int qi = cf.srd_q0 + threadIdx.x; qi < cf.srd_q1; qi += blockDim.x) {
     const int k = d.q_cell[qi], a = d.q_grp[qi], b = d.q_grp[qi + 1];
+    double sum[4] = {0, 0, 0, 0};
+    for (int q = a; q < b; ++q) {
+      const int gq = d.q_list[q];
+      for (int v = 0; v < 4; ++v) sum[v] += d.qhat[v * gc + gq];
+    }
+    const double cnt = d.q_cnt[qi];
     R out[4];
     for (int v = 0; v < 4; ++v) {
-      double sum = 0;
-      for (int q = a; q < b; ++q) sum += d.qhat[v * gc + d.q_list[q]];
-      out[v] = (R)(sum / d.q_cnt[qi]);
+      out[v] = (R)(sum[v] / cnt);
       u[v * n + k] = out[v];
     }
     if (check) {

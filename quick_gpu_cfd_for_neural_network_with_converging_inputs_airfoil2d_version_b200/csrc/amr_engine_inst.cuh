@@ -297,11 +297,13 @@ template <class R> int Batch<R>::autotune(int trials, std::string* error) {
   std::vector<CaseCtl> ctl_save(h_ctl_, h_ctl_ + config_.max_cases);
   cudaMemcpyAsync(s0.p, U0_.p, nbytes, cudaMemcpyDeviceToDevice, stream_);
   cudaMemcpyAsync(s1.p, U1_.p, nbytes, cudaMemcpyDeviceToDevice, stream_);
+  // the tuning runs are not the caller's work: the advance statistics are restored afterwards
+  const amr_gpu_stats_t stats_save = stats_;
   double best = 1e30;
   int best_block = block_, best_grid = grid_request_;
   int best_mode = mode_;
-  const bool graph_save = use_graph_;
-  use_graph_ = false;
+  // candidates run the way they run in production: replayed from a CUDA graph when graphs are on
+  // (direct launches would penalise the multi-kernel modes by their host launch cost)
   for (int mode : {AMR_B200_LAUNCH_PERSISTENT, AMR_B200_LAUNCH_PHASES, AMR_B200_LAUNCH_SPLIT, AMR_B200_LAUNCH_TILED}) {
     for (int block : {128, 256}) {
       if (mode != AMR_B200_LAUNCH_PERSISTENT && block != PHASE_BLOCK) continue;
@@ -324,6 +326,7 @@ template <class R> int Batch<R>::autotune(int trials, std::string* error) {
       for (int grid : grids) {
         grid_request_ = grid;
         configure_grid(error);
+        graph_dirty_ = true;  // a new launch configuration needs its own graph
         std::string e;
         // one untimed pass, then the timed one
         bool ok = advance(trials, &e) == 0;
@@ -347,11 +350,11 @@ template <class R> int Batch<R>::autotune(int trials, std::string* error) {
   for (auto& c : cases_)
     if (c.live) retile(c);
   tiles_dirty_ = true;
-  use_graph_ = graph_save;
   graph_dirty_ = true;
   for (int i = 0; i < config_.max_cases; ++i) refresh_meta(i);
   s0.free();
   s1.free();
+  stats_ = stats_save;
   return sync_tiles(error) ? 0 : 1;
 }
 
