@@ -177,27 +177,33 @@ def run_e2e(case_list, precision, steps, device=0, trials=32, block=0, grid=0, m
     total_cells = sum(m.n_cells for _, m in case_list)
     b = Batch(precision=precision, model=_abi.MODEL_LAMINAR, sa=True, max_cases=len(case_list),
               max_cells=total_cells + 64, device=device, block_threads=block, grid_blocks=grid, launch_mode=mode)
+    t_create = time.perf_counter()
     slots, h2d = [], 0
     for spec, mesh in case_list:
         u0 = cases.initial_state(mesh, spec.initial_primitive())
         slots.append(b.admit(mesh, spec.params(), u0, case_control(1e30, 10 ** 9, steady=False)))
         h2d += mesh_bytes(mesh, precision) + u0.nbytes * precision // 64
+    t_admit = time.perf_counter()
     adv, advances = 0, 0
     while adv < steps:
         k = min(trials, steps - adv)
         b.advance(k)
         adv += k
         advances += 1
+    t_advance = time.perf_counter()
     d2h = 0
     cell_steps = 0
     for (_, mesh), s in zip(case_list, slots):
         u = b.download(s)
         d2h += u.nbytes * precision // 64
         cell_steps += mesh.n_cells * b.status(s)['steps']
-    seconds = time.perf_counter() - t0
+    t_end = time.perf_counter()
+    seconds = t_end - t0
     d2h += advances * 96 * len(slots)  # per-launch control read-back
     b.destroy()
-    return dict(value=cell_steps / seconds, seconds=seconds, h2d=h2d, d2h=d2h)
+    return dict(value=cell_steps / seconds, seconds=seconds, h2d=h2d, d2h=d2h,
+                phases=dict(create=t_create - t0, admit=t_admit - t_create, advance=t_advance - t_admit,
+                            download=t_end - t_advance))
 
 
 def mesh_bytes(mesh, precision):
@@ -446,7 +452,8 @@ def main():
                               bytes_per_step=bytes_per_step,
                               launch_ms=1e3 * per_launch, steps_per_launch=args.steps / r['advances']),
                 e2e=dict(value=e2e_value, unit='cell-steps/s', h2d_bytes_per_step=e2e['h2d'] / args.steps,
-                         d2h_bytes_per_step=e2e['d2h'] / args.steps, seconds=e2e['seconds']),
+                         d2h_bytes_per_step=e2e['d2h'] / args.steps, seconds=e2e['seconds'],
+                         phases_seconds=e2e['phases']),
                 gpu_launches=r['launches'], clocks=clk.summary(),
                 rejected=sum(st['rejected'] for st in r['status']))
     if rank == 0:
