@@ -9,8 +9,10 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -86,6 +88,104 @@ template <class T> struct DevBuf {
   }
 };
 
+// Host staging of one admission (or one download).  Tables are built straight into
+// page-locked blocks by a bump allocator that is reset per call, so an upload needs no
+// host-side copy: one DMA per used block into a device staging buffer laid out like the
+// blocks, then one kernel scatters each table to its range.  Blocks stay allocated for
+// the batch's lifetime; a block whose page-locked allocation fails is plain heap memory
+// (correct, only a slower copy).
+class PinnedStage {
+ public:
+  struct Block {
+    char* p;
+    size_t size, used, dev;  // dev: offset of the block in the device staging buffer
+    bool pinned;
+  };
+  ~PinnedStage() {
+    for (Block& b : blocks_) b.pinned ? (void)cudaFreeHost(b.p) : std::free(b.p);
+  }
+  void reset() {
+    for (Block& b : blocks_) b.used = 0;
+    cur_ = 0;
+  }
+  void* take(size_t bytes) {
+    bytes = (bytes + 255) & ~size_t(255);
+    while (cur_ < blocks_.size() && blocks_[cur_].used + bytes > blocks_[cur_].size) ++cur_;
+    if (cur_ == blocks_.size()) {
+      const size_t size = std::max(bytes, blocks_.empty() ? size_t(8) << 20 : 2 * blocks_.back().size);
+      void* p = nullptr;
+      bool pinned = cudaHostAlloc(&p, size, cudaHostAllocDefault) == cudaSuccess;
+      if (!pinned) {
+        cudaGetLastError();
+        p = std::malloc(size);
+        if (!p) throw std::bad_alloc();
+      }
+      blocks_.push_back({static_cast<char*>(p), size, 0, total_, pinned});
+      total_ += size;
+      if (pinned) pinned_ += size;
+    }
+    Block& b = blocks_[cur_];
+    void* p = b.p + b.used;
+    b.used += bytes;
+    return p;
+  }
+  // offset in the device staging buffer of a host address inside a block, or -1
+  long long dev_offset(const void* host) const {
+    const char* h = static_cast<const char*>(host);
+    for (const Block& b : blocks_)
+      if (h >= b.p && h < b.p + b.size) return (long long)(b.dev + (size_t)(h - b.p));
+    return -1;
+  }
+  const std::vector<Block>& blocks() const { return blocks_; }
+  size_t total() const { return total_; }
+  size_t pinned_bytes() const { return pinned_; }
+
+ private:
+  std::vector<Block> blocks_;
+  size_t cur_ = 0, total_ = 0, pinned_ = 0;
+};
+
+template <class T> struct PinAlloc {
+  using value_type = T;
+  PinnedStage* stage;
+  explicit PinAlloc(PinnedStage* s) : stage(s) {}
+  template <class U> PinAlloc(const PinAlloc<U>& o) : stage(o.stage) {}
+  T* allocate(size_t n) { return static_cast<T*>(stage->take(n * sizeof(T))); }
+  void deallocate(T*, size_t) {}  // released all at once by PinnedStage::reset
+  template <class U> bool operator==(const PinAlloc<U>& o) const { return stage == o.stage; }
+  template <class U> bool operator!=(const PinAlloc<U>& o) const { return stage != o.stage; }
+};
+template <class T> using PVec = std::vector<T, PinAlloc<T>>;
+
+// One scatter launch moves up to UPLOAD_TABLES tables from the device staging buffer.
+constexpr int UPLOAD_TABLES = 64;
+struct UploadTable {
+  unsigned long long dst[UPLOAD_TABLES], src[UPLOAD_TABLES], bytes[UPLOAD_TABLES];
+  int n;
+};
+
+// blockIdx.y picks the table; the copy width is the widest of 8, 4 or 1 bytes that divides
+// both addresses and the size.
+static __global__ void scatter_uploads_kernel(const unsigned char* __restrict__ stage, UploadTable t) {
+  const int i = blockIdx.y;
+  if (i >= t.n) return;
+  unsigned char* dst = reinterpret_cast<unsigned char*>(t.dst[i]);
+  const unsigned char* src = stage + t.src[i];
+  const unsigned long long nb = t.bytes[i];
+  const unsigned long long a = t.dst[i] | reinterpret_cast<unsigned long long>(src) | nb;
+  const unsigned long long tid = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  if ((a & 7) == 0) {
+    for (unsigned long long w = tid; w < nb / 8; w += stride)
+      reinterpret_cast<unsigned long long*>(dst)[w] = reinterpret_cast<const unsigned long long*>(src)[w];
+  } else if ((a & 3) == 0) {
+    for (unsigned long long w = tid; w < nb / 4; w += stride)
+      reinterpret_cast<unsigned int*>(dst)[w] = reinterpret_cast<const unsigned int*>(src)[w];
+  } else {
+    for (unsigned long long w = tid; w < nb; w += stride) dst[w] = src[w];
+  }
+}
+
 struct Range {
   long long b = 0, n = 0;
 };
@@ -114,13 +214,14 @@ template <class R> class Batch final : public BatchBase {
     nv_ = model_ == MODEL_SA ? 5 : 4;
     if (c.max_cases < 1) return fail(error, "max_cases must be positive");
     if (!cuda_ok(cudaSetDevice(c.device), error, "cudaSetDevice")) return false;
-    cudaDeviceProp prop;
-    if (!cuda_ok(cudaGetDeviceProperties(&prop, c.device), error, "device properties")) return false;
-    sms_ = prop.multiProcessorCount;
+    int coop = 0;  // single attribute queries (a full property query costs milliseconds)
+    if (!cuda_ok(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, c.device), error, "device attributes") ||
+        !cuda_ok(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c.device), error, "device attributes"))
+      return false;
     clock_khz_ = 1965000;
     int v = 0;
     if (cudaDeviceGetAttribute(&v, cudaDevAttrClockRate, c.device) == cudaSuccess && v > 0) clock_khz_ = v;
-    if (!prop.cooperativeLaunch) return fail(error, "device lacks cooperative launch");
+    if (!coop) return fail(error, "device lacks cooperative launch");
     long long cells = c.max_cells, slots = c.max_faces, walls = c.max_walls, terms = c.max_terms, srd = c.max_srd;
     if (cells == 0) {
       // size from the HBM budget: ~bytes per cell of tables and state for this model
@@ -242,6 +343,19 @@ template <class R> class Batch final : public BatchBase {
   int admit(const amr_mesh_view_t* m, const amr_params_t* p, const double* u0, uint64_t u0_count, double time0,
             long long steps0, long long rejected0, double target, long long maxsteps, int* slot_out,
             std::string* error) override {
+    HostCase<R> hc;
+    try {
+      return admit_into(hc, m, p, u0, u0_count, time0, steps0, rejected0, target, maxsteps, slot_out, error);
+    } catch (const std::bad_alloc&) {
+      cudaStreamSynchronize(stream_);
+      release_ranges(hc);
+      return fail1(error, "host memory exhausted during admission");
+    }
+  }
+
+  int admit_into(HostCase<R>& hc, const amr_mesh_view_t* m, const amr_params_t* p, const double* u0,
+                 uint64_t u0_count, double time0, long long steps0, long long rejected0, double target,
+                 long long maxsteps, int* slot_out, std::string* error) {
     if (!m || !p || !u0) return fail1(error, "null mesh, parameters or state");
     std::string why;
     if (!validate(*m, *p, u0_count, &why)) return fail1(error, why);
@@ -250,7 +364,6 @@ template <class R> class Batch final : public BatchBase {
     for (int i = 0; i < config_.max_cases; ++i)
       if (!cases_[i].live) { slot = i; break; }
     if (slot < 0) return 3;
-    HostCase<R> hc;
     const long long n = (long long)m->n_cells;
     const long long nw = (long long)m->n_walls;
     const long long ns = (long long)m->face_offsets[n] + nw;  // face slots then wall slots, per cell
@@ -321,22 +434,27 @@ template <class R> class Batch final : public BatchBase {
       return 3;
     }
     // build host staging arrays
+    // (in page-locked staging memory, moved to the device by flush_uploads)
+    stage_.reset();
+    uploads_.clear();
     const int cb = (int)hc.cells.b, sb = (int)hc.slots.b, wb = (int)hc.walls.b, tb = (int)hc.terms.b;
-    std::vector<int> c_case(n + 1, slot), c_slot(n + 1), c_wall(n + 1), c_term(n + 1);
+    PVec<int> c_case = pv<int>(n + 1, slot), c_slot = pv<int>(n + 1), c_wall = pv<int>(n + 1), c_term = pv<int>(n + 1);
     c_case[n] = -1;
-    std::vector<double> c_vol(n + 1, 1.0), c_area(n + 1, 1.0), c_gvol(n + 1, 1.0), c_cx(n + 1, 0.0), c_cy(n + 1, 0.0);
-    std::vector<unsigned char> c_flags(n + 1, 0);
-    std::vector<R> c_wd(n + 1, R(1));
-    std::vector<int> s_own(ns), s_nb(ns), s_meta(ns);
-    std::vector<R> s_len(ns), s_geo(6 * ns, R(0));
-    std::vector<R> w_nx(nw), w_ny(nw), w_len(nw), w_dist(nw, R(1));
-    std::vector<double> w_xm(nw), w_ym(nw);
-    std::vector<int> w_donor(nw, cb);
-    std::vector<int> t_own(nt), t_src(nt);
-    std::vector<R> t_x(nt), t_y(nt);
+    PVec<double> c_vol = pv<double>(n + 1, 1.0), c_area = pv<double>(n + 1, 1.0), c_gvol = pv<double>(n + 1, 1.0),
+                 c_cx = pv<double>(n + 1), c_cy = pv<double>(n + 1);
+    PVec<unsigned char> c_flags = pv<unsigned char>(n + 1);
+    PVec<R> c_wd = pv<R>(model_ == MODEL_SA ? n + 1 : 0, R(1));
+    PVec<int> s_own = pv<int>(ns), s_nb = pv<int>(ns), s_meta = pv<int>(ns);
+    PVec<R> s_len = pv<R>(ns), s_geo = pv<R>(6 * ns);
+    PVec<R> w_nx = pv<R>(nw), w_ny = pv<R>(nw), w_len = pv<R>(nw), w_dist = pv<R>(nw, R(1));
+    PVec<double> w_xm = pv<double>(nw), w_ym = pv<double>(nw);
+    PVec<int> w_donor = pv<int>(nw, cb);
+    PVec<int> t_own = pv<int>(nt), t_src = pv<int>(nt);
+    PVec<R> t_x = pv<R>(nt), t_y = pv<R>(nt);
     const int fb = (int)hc.faces.b;
-    std::vector<int> s_item(ns), f_case(nf, slot), f_own(nf), f_nb(nf), f_meta(nf), w_owner(nw);
-    std::vector<R> f_len(nf), f_geo(6 * nf, R(0));
+    PVec<int> s_item = pv<int>(ns), f_case = pv<int>(nf, slot), f_own = pv<int>(nf), f_nb = pv<int>(nf),
+              f_meta = pv<int>(nf), w_owner = pv<int>(nw);
+    PVec<R> f_len = pv<R>(nf), f_geo = pv<R>(6 * nf);
     // face records go in order of first reference by a cell, in slot order, so that the
     // records of neighbouring cells are neighbours in memory (the reference's face order runs
     // along grid lines)
@@ -460,13 +578,14 @@ template <class R> class Batch final : public BatchBase {
     c_wall[n] = wb + (int)nw;
     c_term[n] = tb + (int)nt;
     // block tiles (tiled mode)
-    std::vector<int> bt_halo, bt_face, s_loc(ns, 0), w_ldon(nw, 0);
-    std::vector<int2> bt_floc;
+    std::vector<int> bt_halo_v, bt_face_v;
+    std::vector<int2> bt_floc_v;
+    PVec<int> s_loc = pv<int>(ns), w_ldon = pv<int>(nw);
     std::vector<BTile> btiles;
-    if (!make_block_tiles(m, n, rec, slot, &btiles, &bt_halo, &bt_face, &bt_floc, &s_loc, &w_ldon, &why))
+    if (!make_block_tiles(m, n, rec, slot, &btiles, &bt_halo_v, &bt_face_v, &bt_floc_v, &s_loc, &w_ldon, &why))
       return fail_release(hc, error, why);
-    hc.halo = {a_halo_.alloc((long long)bt_halo.size()), (long long)bt_halo.size()};
-    hc.tfaces = {a_tface_.alloc((long long)bt_face.size()), (long long)bt_face.size()};
+    hc.halo = {a_halo_.alloc((long long)bt_halo_v.size()), (long long)bt_halo_v.size()};
+    hc.tfaces = {a_tface_.alloc((long long)bt_face_v.size()), (long long)bt_face_v.size()};
     if (hc.halo.b < 0 || hc.tfaces.b < 0 || n_btiles_total() + (long long)btiles.size() > cap_btiles_) {
       release_ranges(hc);
       return 3;
@@ -481,13 +600,16 @@ template <class R> class Batch final : public BatchBase {
       t.w0 += wb;
       t.w1 += wb;
     }
-    for (int& h : bt_halo) h += cb;
-    for (int& f : bt_face) f += fb;
+    PVec<int> bt_halo = pv<int>(bt_halo_v.size()), bt_face = pv<int>(bt_face_v.size());
+    PVec<int2> bt_floc(bt_floc_v.begin(), bt_floc_v.end(), PinAlloc<int2>(&stage_));
+    for (size_t i = 0; i < bt_halo_v.size(); ++i) bt_halo[i] = bt_halo_v[i] + cb;
+    for (size_t i = 0; i < bt_face_v.size(); ++i) bt_face[i] = bt_face_v[i] + fb;
     hc.btiles = std::move(btiles);
     // SRD arrays
     const int gb = (int)hc.groups.b, gmb = (int)hc.gmembers.b, qb = (int)hc.qcells.b, qlb = (int)hc.qlist.b;
-    std::vector<int> g_mem(ng + 1), g_cell(gmem), q_cell(ng + 1, cb + (int)n), q_grp(ng + 1), q_list(qlist);
-    std::vector<double> g_cnt(gmem), g_vol(ng + 1, 1.0), q_cnt(ng + 1, 1.0);
+    PVec<int> g_mem = pv<int>(ng + 1), g_cell = pv<int>(gmem), q_cell = pv<int>(ng + 1, cb + (int)n),
+              q_grp = pv<int>(ng + 1), q_list = pv<int>(qlist);
+    PVec<double> g_cnt = pv<double>(gmem), g_vol = pv<double>(ng + 1, 1.0), q_cnt = pv<double>(ng + 1, 1.0);
     {
       long long pos = 0;
       for (long long gi = 0; gi < ng; ++gi) {
@@ -556,7 +678,7 @@ template <class R> class Batch final : public BatchBase {
     cf.cell1 = cb + (int)n;
     // state
     const long long ncap = cap_cells_;
-    std::vector<R> u(nv_ * (n + 1), R(1));
+    PVec<R> u = pv<R>(nv_ * (n + 1), R(1));
     for (int v = 0; v < nv_; ++v)
       for (long long k = 0; k < n; ++k) u[v * (n + 1) + k] = (R)u0[v * n + k];
     // control
@@ -594,11 +716,14 @@ template <class R> class Batch final : public BatchBase {
            up(t_x_.p + tb, t_x, G) && up(t_y_.p + tb, t_y, G);
     if (ok && model_ == MODEL_SA) ok = up(c_wd_.p + cb, c_wd, G);
     for (int v = 0; ok && v < nv_; ++v) {
-      ok = cuda_ok(cudaMemcpyAsync(U0_.p + v * ncap + cb, u.data() + v * (n + 1), sizeof(R) * (n + 1),
-                                   cudaMemcpyHostToDevice, stream_), error, "state upload");
+      ok = stage_up(U0_.p + v * ncap + cb, u.data() + v * (n + 1), sizeof(R) * (n + 1));
       stats_.state_h2d_bytes += sizeof(R) * (n + 1);
     }
-    ok = ok && cuda_ok(cudaMemcpyAsync(cfg_.p + slot, &cf, sizeof(cf), cudaMemcpyHostToDevice, stream_), error, "cfg upload");
+    CaseCfg<R>* cf_staged = static_cast<CaseCfg<R>*>(stage_.take(sizeof(cf)));
+    *cf_staged = cf;
+    ok = ok && stage_up(cfg_.p + slot, cf_staged, sizeof(cf));
+    if (!ok) return fail_release(hc, error, "upload staging");
+    ok = flush_uploads(error);
     h_ctl_[slot] = ctl;
     ok = ok && cuda_ok(cudaMemcpyAsync(ctl_.p + slot, &h_ctl_[slot], sizeof(CaseCtl), cudaMemcpyHostToDevice, stream_),
                        error, "control upload");
@@ -777,10 +902,52 @@ template <class R> class Batch final : public BatchBase {
     return fail1(error, text);
   }
 
-  template <class T> bool up(T* dst, const std::vector<T>& src, uint64_t* counter) {
-    if (src.empty()) return true;
+  template <class T> PVec<T> pv(size_t count, const T& value = T()) {
+    return PVec<T>(count, value, PinAlloc<T>(&stage_));
+  }
+
+  // Records the upload of a staged table; flush_uploads moves them all.
+  bool stage_up(void* dst, const void* host, size_t bytes) {
+    if (bytes == 0) return true;
+    const long long off = stage_.dev_offset(host);
+    if (off < 0) return false;
+    uploads_.push_back({reinterpret_cast<unsigned long long>(dst), (unsigned long long)off, (unsigned long long)bytes});
+    return true;
+  }
+  template <class T> bool up(T* dst, const PVec<T>& src, uint64_t* counter) {
     *counter += sizeof(T) * src.size();
-    return cudaMemcpyAsync(dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, stream_) == cudaSuccess;
+    return stage_up(dst, src.data(), sizeof(T) * src.size());
+  }
+
+  // One DMA per used staging block into the device staging buffer, then the scatter kernel;
+  // asynchronous on stream_ (the caller synchronises before the staging memory is reused).
+  bool flush_uploads(std::string* error) {
+    if (d_stage_.n < stage_.total()) {
+      stats_.allocated_bytes -= d_stage_.p ? d_stage_.n : 0;
+      d_stage_.free();
+      if (!d_stage_.alloc(stage_.total(), &stats_.allocated_bytes, error, "upload staging")) return false;
+    }
+    stats_.pinned_bytes += stage_.pinned_bytes() - stage_pinned_seen_;
+    stage_pinned_seen_ = stage_.pinned_bytes();
+    for (const PinnedStage::Block& b : stage_.blocks())
+      if (b.used && !cuda_ok(cudaMemcpyAsync(d_stage_.p + b.dev, b.p, b.used, cudaMemcpyHostToDevice, stream_), error,
+                             "staging upload"))
+        return false;
+    for (size_t i0 = 0; i0 < uploads_.size(); i0 += UPLOAD_TABLES) {
+      UploadTable t;
+      t.n = (int)std::min<size_t>(UPLOAD_TABLES, uploads_.size() - i0);
+      unsigned long long most = 0;
+      for (int i = 0; i < t.n; ++i) {
+        t.dst[i] = uploads_[i0 + i].dst;
+        t.src[i] = uploads_[i0 + i].src;
+        t.bytes[i] = uploads_[i0 + i].bytes;
+        most = std::max(most, t.bytes[i]);
+      }
+      const unsigned gx = (unsigned)std::min<unsigned long long>(64, (most + 8191) / 8192);
+      scatter_uploads_kernel<<<dim3(gx, (unsigned)t.n), 256, 0, stream_>>>(d_stage_.p, t);
+      if (!cuda_ok(cudaGetLastError(), error, "upload scatter")) return false;
+    }
+    return true;
   }
 
   int copy_out(const R* buf, int slot, double* out, uint64_t count, std::string* error) {
@@ -788,11 +955,12 @@ template <class R> class Batch final : public BatchBase {
     const HostCase<R>& hc = cases_[slot];
     const long long n = hc.n;
     if (count != (uint64_t)(nv_ * n)) return fail1(error, "state size mismatch");
-    std::vector<R> tmp(nv_ * n);
-    for (int v = 0; v < nv_; ++v)
-      if (!cuda_ok(cudaMemcpyAsync(tmp.data() + v * n, buf + v * cap_cells_ + hc.cells.b, sizeof(R) * n,
+    // one strided copy of the nv variable rows into page-locked staging
+    stage_.reset();
+    R* tmp = static_cast<R*>(stage_.take(sizeof(R) * nv_ * n));
+    if (!cuda_ok(cudaMemcpy2DAsync(tmp, sizeof(R) * n, buf + hc.cells.b, sizeof(R) * cap_cells_, sizeof(R) * n, nv_,
                                    cudaMemcpyDeviceToHost, stream_), error, "download"))
-        return 1;
+      return 1;
     if (!cuda_ok(cudaStreamSynchronize(stream_), error, "download sync")) return 1;
     for (long long i = 0; i < nv_ * n; ++i) out[i] = (double)tmp[i];
     return 0;
@@ -915,7 +1083,7 @@ template <class R> class Batch final : public BatchBase {
   // is the face's left, or the tile wall index) and per wall the donor's local index.
   bool make_block_tiles(const amr_mesh_view_t* m, long long n, const std::vector<int>& rec, int slot,
                         std::vector<BTile>* tiles, std::vector<int>* halo_out, std::vector<int>* face_out,
-                        std::vector<int2>* floc_out, std::vector<int>* s_loc, std::vector<int>* w_ldon,
+                        std::vector<int2>* floc_out, PVec<int>* s_loc, PVec<int>* w_ldon,
                         std::string* why) const {
     const long long nf = (long long)m->n_faces;
     const bool viscous = model_ >= MODEL_LAMINAR;
@@ -1286,6 +1454,7 @@ template <class R> class Batch final : public BatchBase {
   }
 
   void DevBufFreeAll() {
+    d_stage_.free();
     ctl_.free(); cfg_.free(); tiles_.free(); bar_.free();
     c_case_.free(); c_vol_.free(); c_area_.free(); c_gvol_.free(); c_flags_.free(); c_slot_.free(); c_wall_.free();
     c_term_.free(); c_cx_.free(); c_cy_.free(); c_wd_.free();
@@ -1357,6 +1526,13 @@ template <class R> class Batch final : public BatchBase {
   DevBuf<R> U0_, U1_, U2_, R0_, grad_, mu_, eddy_, sgrad_, sdiff_, ssrc_, srate_;
   DevBuf<double> diag_part_, diag_out_, diag_cfg_, ddt_, ex_buf_;
   DevBuf<int> case_tiles_;
+  PinnedStage stage_;  // host staging of admissions and downloads
+  struct Upload {
+    unsigned long long dst, src, bytes;
+  };
+  std::vector<Upload> uploads_;
+  DevBuf<unsigned char> d_stage_;
+  size_t stage_pinned_seen_ = 0;
 };
 
 }  // namespace amrb
