@@ -171,18 +171,19 @@ def run_batched(case_list, precision, steps, warmup, device=0, trials=32, block=
 
 def run_e2e(case_list, precision, steps, device=0, trials=32, block=0, grid=0, mode=0):
     """The same work end to end through the C ABI from host buffers: batch creation, mesh and
-    state upload of every case, `steps` trials with a control read-back per launch, and the
+    state upload of every case (one bulk admission), `steps` trials with a control read-back per launch, and the
     download of every final state; host wall clock."""
     t0 = time.perf_counter()
     total_cells = sum(m.n_cells for _, m in case_list)
     b = Batch(precision=precision, model=_abi.MODEL_LAMINAR, sa=True, max_cases=len(case_list),
               max_cells=total_cells + 64, device=device, block_threads=block, grid_blocks=grid, launch_mode=mode)
     t_create = time.perf_counter()
-    slots, h2d = [], 0
+    items, h2d = [], 0
     for spec, mesh in case_list:
         u0 = cases.initial_state(mesh, spec.initial_primitive())
-        slots.append(b.admit(mesh, spec.params(), u0, case_control(1e30, 10 ** 9, steady=False)))
+        items.append((mesh, spec.params(), u0, case_control(1e30, 10 ** 9, steady=False)))
         h2d += mesh_bytes(mesh, precision) + u0.nbytes * precision // 64
+    slots = b.admit_many(items)
     t_admit = time.perf_counter()
     adv, advances = 0, 0
     while adv < steps:

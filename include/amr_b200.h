@@ -311,6 +311,18 @@ int amr_batch_create(const amr_batch_config_t* config, amr_batch** out, char* er
 int amr_batch_admit(amr_batch* batch, const amr_mesh_view_t* mesh, const amr_params_t* params,
                     const double* u0, uint64_t u0_count, const amr_case_control_t* control,
                     int32_t* slot, char* error, uint64_t error_size);
+/* Admits `count` cases at once (entry i: meshes[i], params[i], u0[i][u0_counts[i]],
+ * controls[i]), converting them into the engine layout on `threads` host threads (0 = up to
+ * 8) with one stream synchronisation for the lot.  slots[i] receives the id or -1,
+ * status[i] 0 (admitted), 1 (invalid; the first such message goes to error) or 3 (no room).
+ * Ids and arena placement follow the request order whatever the thread count, so the result
+ * equals `count` amr_batch_admit calls.  Returns 1 if any case was invalid, else 3 if any
+ * found no room, else 0.  No counterpart in the reference, which sets up one case per
+ * session. */
+int amr_batch_admit_many(amr_batch* batch, uint64_t count, const amr_mesh_view_t* const* meshes,
+                         const amr_params_t* const* params, const double* const* u0, const uint64_t* u0_counts,
+                         const amr_case_control_t* const* controls, int32_t threads, int32_t* slots,
+                         int32_t* status, char* error, uint64_t error_size);
 /* Runs `trials` trials of every live case (one persistent launch, replayed from a CUDA
  * graph that is recaptured when the case set changes), then refreshes host-side status. */
 int amr_batch_advance(amr_batch* batch, int32_t trials, char* error, uint64_t error_size);

@@ -25,6 +25,7 @@ SIGNATURES = {
                                             _S, C.c_uint64]),
     'amr_batch_create': (C.c_int, [_P, _P, _S, C.c_uint64]),
     'amr_batch_admit': (C.c_int, [_P, _P, _P, _P, C.c_uint64, _P, _P, _S, C.c_uint64]),
+    'amr_batch_admit_many': (C.c_int, [_P, C.c_uint64, _P, _P, _P, _P, _P, C.c_int32, _P, _P, _S, C.c_uint64]),
     'amr_batch_advance': (C.c_int, [_P, C.c_int32, _S, C.c_uint64]),
     'amr_batch_check': (C.c_int, [_P, _S, C.c_uint64]),
     'amr_batch_status': (C.c_int, [_P, C.c_int32, _P]),

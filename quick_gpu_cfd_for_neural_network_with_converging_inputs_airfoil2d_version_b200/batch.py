@@ -63,6 +63,41 @@ class Batch:
         self.ncells[slot.value] = mesh.n_cells
         return slot.value
 
+    def admit_many(self, items, threads=0):
+        """Admits (mesh, params, u0, control) tuples in one call, converting them on `threads`
+        host threads (0: up to 8).  Returns one slot per item (None where the arena had no
+        room); slots and placement equal those of admitting the items one by one, in order.
+        Raises BatchError naming the first invalid item (the valid ones stay admitted; their
+        slots are on the exception's `slots`)."""
+        n = len(items)
+        if n == 0:
+            return []
+        u0s = [np.ascontiguousarray(u0, dtype=np.float64) for _, _, u0, _ in items]
+        views = [mesh.view() for mesh, _, _, _ in items]
+        params = [p for _, p, _, _ in items]
+        controls = [c for _, _, _, c in items]
+        P = C.c_void_p * n
+        meshes_p = P(*[C.addressof(v) for v in views])
+        params_p = P(*[C.addressof(p) for p in params])
+        u0_p = P(*[u.ctypes.data for u in u0s])
+        ctl_p = P(*[C.addressof(c) for c in controls])
+        counts = (C.c_uint64 * n)(*[len(u) for u in u0s])
+        slots = (C.c_int32 * n)()
+        status = (C.c_int32 * n)()
+        err = errbuf()
+        lib().amr_batch_admit_many(self._h, n, meshes_p, params_p, u0_p, counts, ctl_p, int(threads), slots, status,
+                                   err, len(err))
+        out = []
+        for (mesh, _, _, _), s, st in zip(items, slots, status):
+            if st == 0:
+                self.ncells[s] = mesh.n_cells
+            out.append(s if st == 0 else None)
+        if any(st == 1 for st in status):
+            e = BatchError(err.value.decode())
+            e.slots = out
+            raise e
+        return out
+
     def advance(self, trials=32):
         err = errbuf()
         if lib().amr_batch_advance(self._h, int(trials), err, len(err)):

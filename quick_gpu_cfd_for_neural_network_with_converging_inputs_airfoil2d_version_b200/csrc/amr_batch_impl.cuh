@@ -7,13 +7,16 @@
 // captured in a CUDA graph that is recaptured whenever the case set changes.
 #pragma once
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "amr_engine.cuh"
@@ -91,18 +94,24 @@ template <class T> struct DevBuf {
 // Host staging of one admission (or one download).  Tables are built straight into
 // page-locked blocks by a bump allocator that is reset per call, so an upload needs no
 // host-side copy: one DMA per used block into a device staging buffer laid out like the
-// blocks, then one kernel scatters each table to its range.  Blocks stay allocated for
-// the batch's lifetime; a block whose page-locked allocation fails is plain heap memory
+// blocks, then one kernel scatters each table to its range.  The first block is normally a
+// slice of the batch's staging arena (adopt); further blocks are allocated on demand and stay
+// for the batch's lifetime; a block whose page-locked allocation fails is plain heap memory
 // (correct, only a slower copy).
 class PinnedStage {
  public:
   struct Block {
     char* p;
     size_t size, used, dev;  // dev: offset of the block in the device staging buffer
-    bool pinned;
+    bool pinned, owned;
   };
-  ~PinnedStage() {
-    for (Block& b : blocks_) b.pinned ? (void)cudaFreeHost(b.p) : std::free(b.p);
+  ~PinnedStage() { release(); }
+  // Replaces every block by caller-owned page-locked memory [p, p + size) (none if size is 0).
+  void adopt(char* p, size_t size) {
+    release();
+    if (!p || !size) return;
+    blocks_.push_back({p, size, 0, 0, true, false});
+    total_ = size;
   }
   void reset() {
     for (Block& b : blocks_) b.used = 0;
@@ -120,7 +129,7 @@ class PinnedStage {
         p = std::malloc(size);
         if (!p) throw std::bad_alloc();
       }
-      blocks_.push_back({static_cast<char*>(p), size, 0, total_, pinned});
+      blocks_.push_back({static_cast<char*>(p), size, 0, total_, pinned, true});
       total_ += size;
       if (pinned) pinned_ += size;
     }
@@ -141,6 +150,13 @@ class PinnedStage {
   size_t pinned_bytes() const { return pinned_; }
 
  private:
+  void release() {
+    for (Block& b : blocks_)
+      if (b.owned) b.pinned ? (void)cudaFreeHost(b.p) : std::free(b.p);
+    blocks_.clear();
+    cur_ = 0;
+    total_ = 0;
+  }
   std::vector<Block> blocks_;
   size_t cur_ = 0, total_ = 0, pinned_ = 0;
 };
@@ -152,6 +168,10 @@ template <class T> struct PinAlloc {
   template <class U> PinAlloc(const PinAlloc<U>& o) : stage(o.stage) {}
   T* allocate(size_t n) { return static_cast<T*>(stage->take(n * sizeof(T))); }
   void deallocate(T*, size_t) {}  // released all at once by PinnedStage::reset
+  template <class U> void construct(U* p) { ::new (static_cast<void*>(p)) U; }  // default-initialised
+  template <class U, class A0, class... A> void construct(U* p, A0&& a0, A&&... a) {
+    ::new (static_cast<void*>(p)) U(std::forward<A0>(a0), std::forward<A>(a)...);
+  }
   template <class U> bool operator==(const PinAlloc<U>& o) const { return stage == o.stage; }
   template <class U> bool operator!=(const PinAlloc<U>& o) const { return stage != o.stage; }
 };
@@ -260,6 +280,9 @@ template <class R> class Batch final : public BatchBase {
     a_qlist_ = RangeAlloc(cap_qlist_);
     cases_.assign(c.max_cases, HostCase<R>());
     meta_.assign(c.max_cases, CaseMeta{});
+    reserved_.assign(c.max_cases, 0);
+    stagers_.clear();
+    stagers_.emplace_back(new Stager());
     if (!cuda_ok(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), error, "stream")) return false;
     if (!cuda_ok(cudaEventCreate(&ev0_), error, "event") || !cuda_ok(cudaEventCreate(&ev1_), error, "event")) return false;
     uint64_t* A = &stats_.allocated_bytes;
@@ -343,76 +366,310 @@ template <class R> class Batch final : public BatchBase {
   int admit(const amr_mesh_view_t* m, const amr_params_t* p, const double* u0, uint64_t u0_count, double time0,
             long long steps0, long long rejected0, double target, long long maxsteps, int* slot_out,
             std::string* error) override {
+    AdmitSpec s{m, p, u0, u0_count, time0, target, steps0, rejected0, maxsteps};
+    std::vector<int> slots, status;
+    std::vector<std::string> errors;
+    admit_many(std::vector<AdmitSpec>{s}, 1, &slots, &status, &errors);
+    if (status[0] == 1 && error) *error = errors[0];
+    if (status[0] == 0) *slot_out = slots[0];
+    return status[0];
+  }
+
+  // Admission in four stages: prepare (case-local tables and checks; parallel), reserve (slot
+  // and arena ranges; serial, in request order, so placement does not depend on the thread
+  // count), fill (engine tables in page-locked staging and their upload; parallel, one staging
+  // area per worker) and commit (controls, one stream synchronisation, host bookkeeping).
+  int admit_many(const std::vector<AdmitSpec>& specs, int threads, std::vector<int>* slots, std::vector<int>* status,
+                 std::vector<std::string>* errors) override {
+    const size_t count = specs.size();
+    slots->assign(count, -1);
+    status->assign(count, 0);
+    errors->assign(count, std::string());
+    // the fill is bound by host memory bandwidth, which 8 threads saturate on common hosts
+    if (threads <= 0) threads = (int)std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency()));
+    threads = (int)std::max<size_t>(1, std::min<size_t>((size_t)threads, count));
+    while ((int)stagers_.size() < threads) stagers_.emplace_back(new Stager());
+    // The staging arena, sized by a bound over every request, is allocated on a helper thread
+    // while the first cases are prepared (page-locking runs at about a GB/s).
+    size_t bound = 0;
+    for (const AdmitSpec& sp : specs) bound = std::max(bound, staged_bound(sp));
+    // If it fails, the stages allocate their own blocks, as for a case above the bound.
+    std::thread arena_thread;
+    if (bound)
+      arena_thread = std::thread([&] {
+        cudaSetDevice(config_.device);
+        std::string ignored;
+        if (!ensure_arena(threads, bound, &ignored)) cudaGetLastError();
+      });
+    // chunks bound the host memory of prepared cases
+    const size_t chunk = std::max<size_t>(32, 4 * (size_t)threads);
+    bool invalid = false, full = false;
+    for (size_t c0 = 0; c0 < count; c0 += chunk) {
+      const size_t c1 = std::min(count, c0 + chunk);
+      std::vector<AdmitJob> jobs(c1 - c0);
+      for (size_t i = c0; i < c1; ++i) jobs[i - c0].spec = specs[i];
+      parallel_for(jobs.size(), threads, [&](size_t i, int) { guarded(jobs[i], [&] { prepare(jobs[i]); }); });
+      for (AdmitJob& j : jobs)
+        if (j.status == 0) guarded(j, [&] { reserve(j); });
+      if (arena_thread.joinable()) arena_thread.join();
+      parallel_for(jobs.size(), threads, [&](size_t i, int w) {
+        if (jobs[i].status == 0) guarded(jobs[i], [&] { fill(jobs[i], *stagers_[w]); });
+      });
+      commit(jobs);
+      for (size_t i = c0; i < c1; ++i) {
+        AdmitJob& j = jobs[i - c0];
+        (*status)[i] = j.status;
+        (*slots)[i] = j.status == 0 ? j.slot : -1;
+        (*errors)[i] = j.error;
+        invalid = invalid || j.status == 1;
+        full = full || j.status == 3;
+      }
+    }
+    if (arena_thread.joinable()) arena_thread.join();
+    return invalid ? 1 : (full ? 3 : 0);
+  }
+
+  // One admission in flight: its request, the case-local tables prepare() builds, the slot and
+  // ranges reserve() gives it, and its outcome (0 admitted, 1 invalid input, 3 no room).
+  struct AdmitJob {
+    AdmitSpec spec{};
+    long long n = 0, nw = 0, ns = 0, nt = 0, nf = 0, ng = 0, gmem = 0, qlist = 0;
+    bool has_srd = false;
+    int kinds[4] = {0, 0, 0, 0};
+    std::vector<unsigned char> simple;
+    std::vector<int> group_index, rec, bt_halo, bt_face, s_loc, w_ldon;
+    std::vector<long long> nontrivial;  // cells (and groups) with a non-trivial SRD neighbourhood
+    std::vector<int2> bt_floc;
     HostCase<R> hc;
+    int slot = -1;
+    bool reserved = false;
+    CaseCtl ctl{};
+    uint64_t geometry_bytes = 0, state_bytes = 0;
+    int status = 0;
+    std::string error;
+  };
+
+  struct Upload {
+    unsigned long long dst, src, bytes;
+  };
+
+  // A worker's staging: page-locked host blocks, their device copy and the pending uploads.
+  struct Stager {
+    PinnedStage stage;
+    std::vector<Upload> uploads;
+    DevBuf<unsigned char> dev;      // own device staging, used when the stage outgrows dev_ext
+    unsigned char* dev_ext = nullptr;  // the device slice of the batch's staging arena
+    size_t dev_ext_n = 0;
+    cudaEvent_t done = nullptr;  // recorded after the stage's last flush
+    bool pending = false;
+    uint64_t allocated = 0;
+    size_t pinned_seen = 0;
+    ~Stager() {
+      if (done) cudaEventDestroy(done);
+      dev.free();
+    }
+  };
+
+  template <class F> static void guarded(AdmitJob& j, F&& f) {
     try {
-      return admit_into(hc, m, p, u0, u0_count, time0, steps0, rejected0, target, maxsteps, slot_out, error);
+      f();
     } catch (const std::bad_alloc&) {
-      cudaStreamSynchronize(stream_);
-      release_ranges(hc);
-      return fail1(error, "host memory exhausted during admission");
+      j.status = 1;
+      j.error = "host memory exhausted during admission";
     }
   }
 
-  int admit_into(HostCase<R>& hc, const amr_mesh_view_t* m, const amr_params_t* p, const double* u0,
-                 uint64_t u0_count, double time0, long long steps0, long long rejected0, double target,
-                 long long maxsteps, int* slot_out, std::string* error) {
-    if (!m || !p || !u0) return fail1(error, "null mesh, parameters or state");
+  // Runs f(i, worker) for i in [0, n) on `threads` host threads (worker-indexed resources).
+  template <class F> void parallel_for(size_t n, int threads, F&& f) {
+    if (threads <= 1 || n <= 1) {
+      for (size_t i = 0; i < n; ++i) f(i, 0);
+      return;
+    }
+    std::atomic<size_t> next{0};
+    std::vector<std::thread> pool;
+    const int t = (int)std::min<size_t>((size_t)threads, n);
+    for (int w = 0; w < t; ++w)
+      pool.emplace_back([&, w] {
+        cudaSetDevice(config_.device);  // the current device is per host thread
+        for (size_t i = next++; i < n; i = next++) f(i, w);
+      });
+    for (std::thread& th : pool) th.join();
+  }
+
+  static void job_fail(AdmitJob& j, int status, const std::string& text) {
+    j.status = status;
+    j.error = text;
+  }
+
+  // Bytes fill() stages for a prepared case (each table rounded to the 256-byte allocation
+  // grain), which sizes the staging arena; a larger case only takes a slower overflow path.
+  size_t staged_bytes(size_t n, size_t nw, size_t ns, size_t nt, size_t nf, size_t ng, size_t gm, size_t ql,
+                      size_t halo, size_t tface) const {
+    const size_t r = sizeof(R), n1 = n + 1, g1 = ng + 1;
+    const size_t tables[] = {4 * n1, 4 * n1, 4 * n1, 4 * n1, 8 * n1, 8 * n1, 8 * n1, 8 * n1, 8 * n1, n1,
+                             model_ == MODEL_SA ? r * n1 : 0, 4 * ns, 4 * ns, 4 * ns, 4 * ns, r * ns, 6 * r * ns,
+                             r * nw, r * nw, r * nw, r * nw, 8 * nw, 8 * nw, 4 * nw, 4 * nw, 4 * nt, 4 * nt, r * nt,
+                             r * nt, 4 * nf, 4 * nf, 4 * nf, 4 * nf, r * nf, 6 * r * nf, 4 * halo, 4 * tface,
+                             8 * tface, 4 * ns, 4 * nw, 4 * g1, 4 * gm, 4 * g1, 4 * g1, 4 * ql, 8 * gm, 8 * g1, 8 * g1,
+                             r * nv_ * n1, sizeof(CaseCfg<R>)};
+    size_t total = 0;
+    for (size_t b : tables) total += (b + 255) & ~size_t(255);
+    return total;
+  }
+
+  // The same from a request's counts alone, with the block-tile tables at their arena bounds
+  // (halo <= 2 cells, face records <= 2 faces + 64 per case); 0 for a request that does not
+  // name its tables (it fails validation later).
+  size_t staged_bound(const AdmitSpec& sp) const {
+    const amr_mesh_view_t* m = sp.mesh;
+    if (!m || !m->face_offsets || !m->n_cells) return 0;
+    const size_t n = m->n_cells, nw = m->n_walls, nf = m->n_faces, ns = m->face_offsets[n] + nw;
+    const size_t nt = model_ >= MODEL_LAMINAR && m->visc_offsets ? m->visc_offsets[n] : 0;
+    const bool srd = m->small_cells && m->group_offsets && m->member_offsets;
+    return staged_bytes(n, nw, ns, nt, nf, srd ? n : 0, srd ? m->group_offsets[n] : 0, srd ? m->member_offsets[n] : 0,
+                        2 * n, 2 * nf + 64);
+  }
+
+  // One page-locked host allocation and one device allocation, cut into `stages` equal slices
+  // that the first `stages` stagers adopt (allocation calls contend in the driver, so one large
+  // call replaces one per stage).  Grows only; every earlier upload has completed when called.
+  bool ensure_arena(int stages, size_t slice, std::string* error) {
+    slice = (slice + 4095) & ~size_t(4095);
+    if (stages <= arena_stages_ && slice <= arena_slice_) return true;
+    stages = std::max(stages, arena_stages_);
+    slice = std::max(slice, arena_slice_);
+    free_arena();
+    const size_t bytes = (size_t)stages * slice;
+    if (!cuda_ok(cudaHostAlloc(reinterpret_cast<void**>(&arena_h_), bytes, cudaHostAllocDefault), error,
+                 "staging arena") ||
+        !cuda_ok(cudaMalloc(reinterpret_cast<void**>(&arena_d_), bytes), error, "staging arena")) {
+      free_arena();
+      return false;
+    }
+    stats_.pinned_bytes += bytes;
+    stats_.allocated_bytes += bytes;
+    arena_stages_ = stages;
+    arena_slice_ = slice;
+    for (int i = 0; i < stages; ++i) {
+      stagers_[i]->stage.adopt(arena_h_ + (size_t)i * slice, slice);
+      stagers_[i]->pinned_seen = stagers_[i]->stage.pinned_bytes();
+      stagers_[i]->dev_ext = arena_d_ + (size_t)i * slice;
+      stagers_[i]->dev_ext_n = slice;
+    }
+    return true;
+  }
+
+  void free_arena() {
+    for (int i = 0; i < arena_stages_ && i < (int)stagers_.size(); ++i) {
+      stagers_[i]->stage.adopt(nullptr, 0);
+      stagers_[i]->dev_ext = nullptr;
+      stagers_[i]->dev_ext_n = 0;
+    }
+    if (arena_h_) cudaFreeHost(arena_h_);
+    if (arena_d_) cudaFree(arena_d_);
+    arena_h_ = nullptr;
+    arena_d_ = nullptr;
+    arena_stages_ = 0;
+    arena_slice_ = 0;
+  }
+
+  // Index checks the table fills rely on: every face, wall, donor, gradient source and SRD
+  // index in range, offsets non-decreasing from zero, walls grouped by owner cell.
+  bool check_topology(const AdmitJob& j, std::string* why) const {
+    const amr_mesh_view_t* m = j.spec.mesh;
+    const long long n = j.n, nf = j.nf, nw = j.nw;
+    const bool viscous = model_ >= MODEL_LAMINAR;
+    if (m->face_offsets[0] != 0 || (viscous && m->visc_offsets[0] != 0)) return fail(why, "offsets do not start at zero");
+    if (nw && !m->walls) return fail(why, "wall table missing");
+    long long wpos = 0;
+    for (long long k = 0; k < n; ++k) {
+      if (m->face_offsets[k + 1] < m->face_offsets[k] || (viscous && m->visc_offsets[k + 1] < m->visc_offsets[k]))
+        return fail(why, "offsets decrease");
+      for (uint64_t q = m->face_offsets[k]; q < m->face_offsets[k + 1]; ++q) {
+        const uint64_t fi = m->cell_faces[q];
+        if (fi >= (uint64_t)nf) return fail(why, "cell_faces index out of range");
+        const amr_face_t& f = m->faces[fi];
+        const bool own_left = f.left == (int)k;
+        if (!own_left && f.right != (int)k) return fail(why, "cell_faces lists a face of another cell");
+        const int other = own_left ? f.right : f.left;
+        if (other >= (int)n) return fail(why, "face neighbour out of range");
+        if ((other < 0) != (f.boundary >= 0) || f.boundary > 3) return fail(why, "face boundary marker inconsistent");
+      }
+      const amr_cell_t& c = m->cells[k];
+      if (c.wall_begin != (uint64_t)wpos) return fail(why, "walls are not grouped by owner cell");
+      if (c.wall_begin + c.wall_count > (uint64_t)nw) return fail(why, "wall count mismatch");
+      for (uint64_t q = c.wall_begin; q < c.wall_begin + c.wall_count; ++q) {
+        if (m->walls[q].owner_cell != (uint64_t)k) return fail(why, "wall owner mismatch");
+        if (viscous && (m->wall_samples[q].donor < 0 || m->wall_samples[q].donor >= n))
+          return fail(why, "wall donor out of range");
+      }
+      wpos += (long long)c.wall_count;
+      if (viscous)
+        for (uint64_t q = m->visc_offsets[k]; q < m->visc_offsets[k + 1]; ++q) {
+          const amr_gradient_term_t& t = m->visc_terms[q];
+          if (t.source >= n) return fail(why, "gradient source out of range");
+          if (t.source == -2 && (t.side < 0 || t.side > 3)) return fail(why, "gradient wall side out of range");
+        }
+    }
+    if (wpos != nw) return fail(why, "wall count mismatch");
+    for (long long fi = 0; fi < nf; ++fi) {
+      const amr_face_t& f = m->faces[fi];
+      const int own = f.left >= 0 ? f.left : f.right;
+      const int other = f.left >= 0 ? f.right : -1;
+      if (own < 0 || own >= (int)n || other >= (int)n || (other < 0) != (f.boundary >= 0) || f.boundary > 3)
+        return fail(why, "face cells or boundary marker inconsistent");
+    }
+    return true;
+  }
+
+  // Stage 1 (any thread): validation and the case-local tables; touches no batch state.
+  void prepare(AdmitJob& j) const {
+    const AdmitSpec& s = j.spec;
+    const amr_mesh_view_t* m = s.mesh;
+    if (!m || !s.params || !s.u0) return job_fail(j, 1, "null mesh, parameters or state");
     std::string why;
-    if (!validate(*m, *p, u0_count, &why)) return fail1(error, why);
-    if (!std::isfinite(time0) || time0 < 0) return fail1(error, "invalid initial time");
-    int slot = -1;
-    for (int i = 0; i < config_.max_cases; ++i)
-      if (!cases_[i].live) { slot = i; break; }
-    if (slot < 0) return 3;
-    const long long n = (long long)m->n_cells;
-    const long long nw = (long long)m->n_walls;
-    const long long ns = (long long)m->face_offsets[n] + nw;  // face slots then wall slots, per cell
-    const long long nt = model_ >= MODEL_LAMINAR ? (long long)m->visc_offsets[n] : 0;
-    const long long nf = (long long)m->n_faces;
+    if (!validate(*m, *s.params, s.u0_count, &why)) return job_fail(j, 1, why);
+    if (!std::isfinite(s.time0) || s.time0 < 0) return job_fail(j, 1, "invalid initial time");
+    const long long n = j.n = (long long)m->n_cells;
+    j.nw = (long long)m->n_walls;
+    j.ns = (long long)m->face_offsets[n] + j.nw;  // face slots then wall slots, per cell
+    j.nt = model_ >= MODEL_LAMINAR ? (long long)m->visc_offsets[n] : 0;
+    j.nf = (long long)m->n_faces;
+    if (!check_topology(j, &why)) return job_fail(j, 1, why);
     // SRD lists (only non-trivial neighbourhoods)
-    std::vector<unsigned char> simple(n, 1);
-    std::vector<int> group_index(n, -1);
-    std::vector<long long> groups_nt, cells_nt;
-    long long gmem = 0, qlist = 0;
-    const bool has_srd = m->small_cells > 0;
-    if (has_srd) {
+    j.has_srd = m->small_cells > 0;
+    j.simple.assign(n, 1);
+    j.group_index.assign(n, -1);
+    if (j.has_srd) {
       for (long long k = 0; k < n; ++k) {
+        if (m->member_offsets[k + 1] < m->member_offsets[k] || m->group_offsets[k + 1] < m->group_offsets[k])
+          return job_fail(j, 1, "SRD offsets decrease");
         const uint64_t cnt = m->member_offsets[k + 1] - m->member_offsets[k];
         const uint64_t size = m->group_offsets[k + 1] - m->group_offsets[k];
-        if (cnt == 0 || size == 0) return fail1(error, "empty SRD neighbourhood");
-        simple[k] = cnt == 1 && size == 1 && m->group_members[m->group_offsets[k]] == (uint64_t)k;
+        if (cnt == 0 || size == 0) return job_fail(j, 1, "empty SRD neighbourhood");
+        for (uint64_t q = m->group_offsets[k]; q < m->group_offsets[k + 1]; ++q)
+          if (m->group_members[q] >= (uint64_t)n) return job_fail(j, 1, "SRD group member out of range");
+        for (uint64_t q = m->member_offsets[k]; q < m->member_offsets[k + 1]; ++q)
+          if (m->member_groups[q] >= (uint64_t)n) return job_fail(j, 1, "SRD member group out of range");
+        j.simple[k] = cnt == 1 && size == 1 && m->group_members[m->group_offsets[k]] == (uint64_t)k;
       }
       for (long long k = 0; k < n; ++k)
-        if (!simple[k]) {
-          group_index[k] = (int)groups_nt.size();
-          groups_nt.push_back(k);
-          gmem += (long long)(m->group_offsets[k + 1] - m->group_offsets[k]);
-          cells_nt.push_back(k);
-          qlist += (long long)(m->member_offsets[k + 1] - m->member_offsets[k]);
+        if (!j.simple[k]) {
+          j.group_index[k] = (int)j.nontrivial.size();
+          j.nontrivial.push_back(k);
+          j.gmem += (long long)(m->group_offsets[k + 1] - m->group_offsets[k]);
+          j.qlist += (long long)(m->member_offsets[k + 1] - m->member_offsets[k]);
         }
-      for (long long k : cells_nt)
+      for (long long k : j.nontrivial)
         for (uint64_t q = m->member_offsets[k]; q < m->member_offsets[k + 1]; ++q)
-          if (group_index[m->member_groups[q]] < 0) return fail1(error, "SRD neighbourhood references a trivial group");
+          if (j.group_index[m->member_groups[q]] < 0) return job_fail(j, 1, "SRD neighbourhood references a trivial group");
     }
-    // allocate ranges
+    j.ng = (long long)j.nontrivial.size();
+    for (int side = 0; side < 4; ++side)
+      j.kinds[side] = m->boundaries[side].kind < 0 ? s.params->bc[side] : m->boundaries[side].kind;
+    // warp tiles (case-local; reserve() moves them to the case's ranges)
+    HostCase<R>& hc = j.hc;
     hc.n = (int)n;
-    hc.cells = {a_cells_.alloc(n + 1), n + 1};
-    hc.slots = {a_slots_.alloc(ns), ns};
-    hc.walls = {a_walls_.alloc(nw), nw};
-    hc.terms = {a_terms_.alloc(nt), nt};
-    const long long ng = (long long)groups_nt.size();
-    hc.groups = {a_groups_.alloc(ng + 1), ng + 1};
-    hc.gmembers = {a_gmem_.alloc(gmem), gmem};
-    hc.qcells = {a_q_.alloc(ng + 1), ng + 1};
-    hc.qlist = {a_qlist_.alloc(qlist), qlist};
-    hc.faces = {a_faces_.alloc(nf), nf};
-    if (hc.cells.b < 0 || hc.slots.b < 0 || hc.walls.b < 0 || hc.terms.b < 0 || hc.groups.b < 0 || hc.gmembers.b < 0 ||
-        hc.qcells.b < 0 || hc.qlist.b < 0 || hc.faces.b < 0) {
-      release_ranges(hc);
-      return 3;
-    }
-    // tiles
-    hc.slot = slot;
     hc.nslot.resize(n);
     hc.nterm.assign(n, 0);
     for (long long k = 0; k < n; ++k) {
@@ -425,73 +682,138 @@ template <class R> class Batch final : public BatchBase {
       hc.slot_prefix[k + 1] = hc.slot_prefix[k] + hc.nslot[k];
       hc.term_prefix[k + 1] = hc.term_prefix[k] + hc.nterm[k];
     }
-    if (!make_tiles(hc, &why)) {
-      release_ranges(hc);
-      return fail1(error, why);
-    }
-    if (n_tiles_total() + (long long)hc.tiles.size() > cap_tiles_) {
-      release_ranges(hc);
-      return 3;
-    }
-    // build host staging arrays
-    // (in page-locked staging memory, moved to the device by flush_uploads)
-    stage_.reset();
-    uploads_.clear();
-    const int cb = (int)hc.cells.b, sb = (int)hc.slots.b, wb = (int)hc.walls.b, tb = (int)hc.terms.b;
-    PVec<int> c_case = pv<int>(n + 1, slot), c_slot = pv<int>(n + 1), c_wall = pv<int>(n + 1), c_term = pv<int>(n + 1);
-    c_case[n] = -1;
-    PVec<double> c_vol = pv<double>(n + 1, 1.0), c_area = pv<double>(n + 1, 1.0), c_gvol = pv<double>(n + 1, 1.0),
-                 c_cx = pv<double>(n + 1), c_cy = pv<double>(n + 1);
-    PVec<unsigned char> c_flags = pv<unsigned char>(n + 1);
-    PVec<R> c_wd = pv<R>(model_ == MODEL_SA ? n + 1 : 0, R(1));
-    PVec<int> s_own = pv<int>(ns), s_nb = pv<int>(ns), s_meta = pv<int>(ns);
-    PVec<R> s_len = pv<R>(ns), s_geo = pv<R>(6 * ns);
-    PVec<R> w_nx = pv<R>(nw), w_ny = pv<R>(nw), w_len = pv<R>(nw), w_dist = pv<R>(nw, R(1));
-    PVec<double> w_xm = pv<double>(nw), w_ym = pv<double>(nw);
-    PVec<int> w_donor = pv<int>(nw, cb);
-    PVec<int> t_own = pv<int>(nt), t_src = pv<int>(nt);
-    PVec<R> t_x = pv<R>(nt), t_y = pv<R>(nt);
-    const int fb = (int)hc.faces.b;
-    PVec<int> s_item = pv<int>(ns), f_case = pv<int>(nf, slot), f_own = pv<int>(nf), f_nb = pv<int>(nf),
-              f_meta = pv<int>(nf), w_owner = pv<int>(nw);
-    PVec<R> f_len = pv<R>(nf), f_geo = pv<R>(6 * nf);
+    if (!make_tiles(hc, &why)) return job_fail(j, 1, why);
     // face records go in order of first reference by a cell, in slot order, so that the
     // records of neighbouring cells are neighbours in memory (the reference's face order runs
     // along grid lines)
-    std::vector<int> rec(nf, -1);
-    {
-      int next = 0;
-      for (long long k = 0; k < n; ++k)
-        for (uint64_t q = m->face_offsets[k]; q < m->face_offsets[k + 1]; ++q) {
-          const uint64_t fi = m->cell_faces[q];
-          if (fi < (uint64_t)nf && rec[fi] < 0) rec[fi] = next++;
-        }
-      for (long long fi = 0; fi < nf; ++fi)
-        if (rec[fi] < 0) rec[fi] = next++;  // a face no cell lists (still evaluated, never gathered)
+    j.rec.assign(j.nf, -1);
+    int next = 0;
+    for (long long k = 0; k < n; ++k)
+      for (uint64_t q = m->face_offsets[k]; q < m->face_offsets[k + 1]; ++q) {
+        const uint64_t fi = m->cell_faces[q];
+        if (j.rec[fi] < 0) j.rec[fi] = next++;
+      }
+    for (long long fi = 0; fi < j.nf; ++fi)
+      if (j.rec[fi] < 0) j.rec[fi] = next++;  // a face no cell lists (still evaluated, never gathered)
+    // block tiles (tiled mode), case-local
+    j.s_loc.assign(j.ns, 0);
+    j.w_ldon.assign(j.nw, 0);
+    if (!make_block_tiles(m, n, j.rec, -1, &hc.btiles, &j.bt_halo, &j.bt_face, &j.bt_floc, &j.s_loc, &j.w_ldon, &why))
+      return job_fail(j, 1, why);
+  }
+
+  // Stage 2 (serial, request order): a free slot and the case's ranges of every arena table.
+  void reserve(AdmitJob& j) {
+    int slot = -1;
+    for (int i = 0; i < config_.max_cases; ++i)
+      if (!cases_[i].live && !reserved_[i]) {
+        slot = i;
+        break;
+      }
+    if (slot < 0) return job_fail(j, 3, "");
+    HostCase<R>& hc = j.hc;
+    const long long n = j.n;
+    hc.cells = {a_cells_.alloc(n + 1), n + 1};
+    hc.slots = {a_slots_.alloc(j.ns), j.ns};
+    hc.walls = {a_walls_.alloc(j.nw), j.nw};
+    hc.terms = {a_terms_.alloc(j.nt), j.nt};
+    hc.groups = {a_groups_.alloc(j.ng + 1), j.ng + 1};
+    hc.gmembers = {a_gmem_.alloc(j.gmem), j.gmem};
+    hc.qcells = {a_q_.alloc(j.ng + 1), j.ng + 1};
+    hc.qlist = {a_qlist_.alloc(j.qlist), j.qlist};
+    hc.faces = {a_faces_.alloc(j.nf), j.nf};
+    hc.halo = {a_halo_.alloc((long long)j.bt_halo.size()), (long long)j.bt_halo.size()};
+    hc.tfaces = {a_tface_.alloc((long long)j.bt_face.size()), (long long)j.bt_face.size()};
+    if (hc.cells.b < 0 || hc.slots.b < 0 || hc.walls.b < 0 || hc.terms.b < 0 || hc.groups.b < 0 || hc.gmembers.b < 0 ||
+        hc.qcells.b < 0 || hc.qlist.b < 0 || hc.faces.b < 0 || hc.halo.b < 0 || hc.tfaces.b < 0 ||
+        n_tiles_total() + pending_tiles_ + (long long)hc.tiles.size() > cap_tiles_ ||
+        n_btiles_total() + pending_btiles_ + (long long)hc.btiles.size() > cap_btiles_) {
+      release_ranges(hc);
+      return job_fail(j, 3, "");
     }
-    int kinds[4];
-    for (int side = 0; side < 4; ++side) kinds[side] = m->boundaries[side].kind < 0 ? p->bc[side] : m->boundaries[side].kind;
+    j.slot = hc.slot = slot;
+    j.reserved = reserved_[slot] = 1;
+    pending_tiles_ += (long long)hc.tiles.size();
+    pending_btiles_ += (long long)hc.btiles.size();
+    const int cb = (int)hc.cells.b;
+    for (Tile& t : hc.tiles) {
+      t.cs = slot;
+      t.c0 += cb;
+      t.c1 += cb;
+      t.s0 += (int)hc.slots.b;
+      t.s1 += (int)hc.slots.b;
+      t.t0 += (int)hc.terms.b;
+      t.t1 += (int)hc.terms.b;
+    }
+    for (BTile& t : hc.btiles) {
+      t.cs = slot;
+      t.c0 += cb;
+      t.c1 += cb;
+      t.h0 += (int)hc.halo.b;
+      t.h1 += (int)hc.halo.b;
+      t.f0 += (int)hc.tfaces.b;
+      t.f1 += (int)hc.tfaces.b;
+      t.w0 += (int)hc.walls.b;
+      t.w1 += (int)hc.walls.b;
+    }
+  }
+
+  // Stage 3 (any thread): the engine tables of one reserved case, written straight into the
+  // worker's page-locked staging, and their upload (asynchronous on stream_).
+  void fill(AdmitJob& j, Stager& st) {
+    if (st.pending && !cuda_ok(cudaEventSynchronize(st.done), &j.error, "staging reuse")) return (void)(j.status = 1);
+    st.pending = false;
+    st.stage.reset();
+    st.uploads.clear();
+    PinnedStage& S = st.stage;
+    const AdmitSpec& sp = j.spec;
+    const amr_mesh_view_t* m = sp.mesh;
+    const amr_params_t* p = sp.params;
+    HostCase<R>& hc = j.hc;
+    const long long n = j.n, nw = j.nw, ns = j.ns, nt = j.nt, nf = j.nf, ng = j.ng;
+    const int slot = j.slot;
+    const bool has_srd = j.has_srd, viscous = model_ >= MODEL_LAMINAR;
+    const int* kinds = j.kinds;
+    const std::vector<int>& rec = j.rec;
+    const int cb = (int)hc.cells.b, sb = (int)hc.slots.b, wb = (int)hc.walls.b, tb = (int)hc.terms.b, fb = (int)hc.faces.b;
+    // tables every entry of which the loops below write are left uninitialised (pvu)
+    PVec<int> c_case = pv<int>(S, n + 1, slot), c_slot = pvu<int>(S, n + 1), c_wall = pvu<int>(S, n + 1),
+              c_term = pvu<int>(S, n + 1);
+    c_case[n] = -1;
+    PVec<double> c_vol = pvu<double>(S, n + 1), c_area = pvu<double>(S, n + 1), c_gvol = pvu<double>(S, n + 1),
+                 c_cx = pvu<double>(S, n + 1), c_cy = pvu<double>(S, n + 1);
+    c_vol[n] = c_area[n] = c_gvol[n] = 1.0;
+    c_cx[n] = c_cy[n] = 0.0;
+    PVec<unsigned char> c_flags = pvu<unsigned char>(S, n + 1);
+    c_flags[n] = 0;
+    PVec<R> c_wd = pvu<R>(S, model_ == MODEL_SA ? n + 1 : 0);
+    if (model_ == MODEL_SA) c_wd[n] = R(1);
+    PVec<int> s_own = pvu<int>(S, ns), s_nb = pvu<int>(S, ns), s_meta = pvu<int>(S, ns), s_item = pvu<int>(S, ns);
+    PVec<R> s_len = pvu<R>(S, ns), s_geo = pv<R>(S, 6 * ns, R(0));
+    PVec<R> w_nx = pvu<R>(S, nw), w_ny = pvu<R>(S, nw), w_len = pvu<R>(S, nw), w_dist = pv<R>(S, nw, R(1));
+    PVec<double> w_xm = pvu<double>(S, nw), w_ym = pvu<double>(S, nw);
+    PVec<int> w_donor = pv<int>(S, nw, cb), w_owner = pvu<int>(S, nw);
+    PVec<int> t_own = pvu<int>(S, nt), t_src = pvu<int>(S, nt);
+    PVec<R> t_x = pvu<R>(S, nt), t_y = pvu<R>(S, nt);
+    PVec<int> f_case = pv<int>(S, nf, slot), f_own = pvu<int>(S, nf), f_nb = pvu<int>(S, nf), f_meta = pvu<int>(S, nf);
+    PVec<R> f_len = pvu<R>(S, nf), f_geo = viscous ? pvu<R>(S, 6 * nf) : pv<R>(S, 6 * nf, R(0));
     long long wpos = 0, spos = 0;
     for (long long k = 0; k < n; ++k) {
       const amr_cell_t& c = m->cells[k];
       c_vol[k] = c.volume;
       c_area[k] = m->agglomerate_small ? c.volume : (c.x1 - c.x0) * (c.y1 - c.y0);
       c_gvol[k] = has_srd ? m->group_volume[k] : 1.0;
-      c_flags[k] = has_srd && simple[k] ? 1 : 0;
+      c_flags[k] = has_srd && j.simple[k] ? 1 : 0;
       c_cx[k] = c.cx;
       c_cy[k] = c.cy;
       c_slot[k] = sb + (int)spos;
-      c_term[k] = tb + (model_ >= MODEL_LAMINAR ? (int)m->visc_offsets[k] : 0);
+      c_term[k] = tb + (viscous ? (int)m->visc_offsets[k] : 0);
       if (model_ == MODEL_SA) c_wd[k] = (R)m->wall_distance[k];
       for (uint64_t q = m->face_offsets[k]; q < m->face_offsets[k + 1]; ++q, ++spos) {
         const uint64_t fi = m->cell_faces[q];
-        if (fi >= m->n_faces) return fail_release(hc, error, "cell_faces index out of range");
         const amr_face_t& f = m->faces[fi];
         const bool own_left = f.left == (int)k;
-        if (!own_left && f.right != (int)k) return fail_release(hc, error, "cell_faces lists a face of another cell");
         const int other = own_left ? f.right : f.left;
-        if (other >= (int)n) return fail_release(hc, error, "face neighbour out of range");
-        if ((other < 0) != (f.boundary >= 0) || f.boundary > 3) return fail_release(hc, error, "face boundary marker inconsistent");
         const int side = f.boundary;
         const int kind = side >= 0 ? kinds[side] : 0;
         s_own[spos] = cb + (int)k;
@@ -499,21 +821,20 @@ template <class R> class Batch final : public BatchBase {
         s_meta[spos] = (own_left ? 1 : 0) | ((f.axis & 1) << 1) | ((side + 1) << 2) | ((kind & 15) << 5);
         s_len[spos] = (R)f.length;
         s_item[spos] = 2 * (fb + rec[fi]) + (own_left ? 1 : 0);  // record index and orientation
-        if (model_ >= MODEL_LAMINAR) {
+        if (viscous) {
           const amr_face_geometry_t& g = m->face_geometry[fi];
-          s_geo[6 * spos + 0] = (R)g.dx;
-          s_geo[6 * spos + 1] = (R)g.dy;
-          s_geo[6 * spos + 2] = (R)g.ex;
-          s_geo[6 * spos + 3] = (R)g.ey;
-          s_geo[6 * spos + 4] = (R)g.distance;
-          s_geo[6 * spos + 5] = (R)m->face_samples[fi].distance;
+          R* geo = &s_geo[6 * spos];
+          geo[0] = (R)g.dx;
+          geo[1] = (R)g.dy;
+          geo[2] = (R)g.ex;
+          geo[3] = (R)g.ey;
+          geo[4] = (R)g.distance;
+          geo[5] = (R)m->face_samples[fi].distance;
         }
       }
       c_wall[k] = wb + (int)wpos;
-      if (c.wall_begin != (uint64_t)wpos) return fail_release(hc, error, "walls are not grouped by owner cell");
       for (uint64_t q = c.wall_begin; q < c.wall_begin + c.wall_count; ++q, ++wpos, ++spos) {
         const amr_wall_t& w = m->walls[q];
-        if (w.owner_cell != (uint64_t)k) return fail_release(hc, error, "wall owner mismatch");
         w_nx[wpos] = (R)w.nx;
         w_ny[wpos] = (R)w.ny;
         w_len[wpos] = (R)w.length;
@@ -528,35 +849,29 @@ template <class R> class Batch final : public BatchBase {
         s_geo[6 * spos + 0] = (R)w.nx;
         s_geo[6 * spos + 1] = (R)w.ny;
         s_geo[6 * spos + 2] = R(1);
-        if (model_ >= MODEL_LAMINAR) {
+        if (viscous) {
           const amr_wall_sample_t& smp = m->wall_samples[q];
-          if (smp.donor < 0 || smp.donor >= n) return fail_release(hc, error, "wall donor out of range");
           w_donor[wpos] = cb + smp.donor;
           w_dist[wpos] = (R)smp.distance;
           s_nb[spos] = cb + smp.donor;
           s_geo[6 * spos + 2] = (R)smp.distance;
         }
       }
-      if (model_ >= MODEL_LAMINAR)
+      if (viscous)
         for (uint64_t q = m->visc_offsets[k]; q < m->visc_offsets[k + 1]; ++q) {
           const amr_gradient_term_t& t = m->visc_terms[q];
           t_own[q] = cb + (int)k;
-          if (t.source >= n) return fail_release(hc, error, "gradient source out of range");
           t_src[q] = t.source >= 0 ? cb + t.source : (t.source == -1 ? -1 : -2 - t.side);
-          if (t.source == -2 && (t.side < 0 || t.side > 3)) return fail_release(hc, error, "gradient wall side out of range");
           t_x[q] = (R)t.x;
           t_y[q] = (R)t.y;
         }
     }
-    if (wpos != nw || spos != ns) return fail_release(hc, error, "wall count mismatch");
     // face records in face orientation (left to right; a boundary face's inside cell is its owner)
     for (long long fi = 0; fi < nf; ++fi) {
       const amr_face_t& f = m->faces[fi];
       const bool own_left = f.left >= 0;
       const int own = own_left ? f.left : f.right;
       const int other = own_left ? f.right : -1;
-      if (own < 0 || own >= (int)n || other >= (int)n || (other < 0) != (f.boundary >= 0) || f.boundary > 3)
-        return fail_release(hc, error, "face cells or boundary marker inconsistent");
       const int side = f.boundary;
       const int kind = side >= 0 ? kinds[side] : 0;
       const long long r = rec[fi];
@@ -564,56 +879,36 @@ template <class R> class Batch final : public BatchBase {
       f_nb[r] = other >= 0 ? cb + other : -1;
       f_meta[r] = (own_left ? 1 : 0) | ((f.axis & 1) << 1) | ((side + 1) << 2) | ((kind & 15) << 5);
       f_len[r] = (R)f.length;
-      if (model_ >= MODEL_LAMINAR) {
+      if (viscous) {
         const amr_face_geometry_t& g = m->face_geometry[fi];
-        f_geo[6 * r + 0] = (R)g.dx;
-        f_geo[6 * r + 1] = (R)g.dy;
-        f_geo[6 * r + 2] = (R)g.ex;
-        f_geo[6 * r + 3] = (R)g.ey;
-        f_geo[6 * r + 4] = (R)g.distance;
-        f_geo[6 * r + 5] = (R)m->face_samples[fi].distance;
+        R* geo = &f_geo[6 * r];
+        geo[0] = (R)g.dx;
+        geo[1] = (R)g.dy;
+        geo[2] = (R)g.ex;
+        geo[3] = (R)g.ey;
+        geo[4] = (R)g.distance;
+        geo[5] = (R)m->face_samples[fi].distance;
       }
     }
     c_slot[n] = sb + (int)ns;
     c_wall[n] = wb + (int)nw;
     c_term[n] = tb + (int)nt;
-    // block tiles (tiled mode)
-    std::vector<int> bt_halo_v, bt_face_v;
-    std::vector<int2> bt_floc_v;
-    PVec<int> s_loc = pv<int>(ns), w_ldon = pv<int>(nw);
-    std::vector<BTile> btiles;
-    if (!make_block_tiles(m, n, rec, slot, &btiles, &bt_halo_v, &bt_face_v, &bt_floc_v, &s_loc, &w_ldon, &why))
-      return fail_release(hc, error, why);
-    hc.halo = {a_halo_.alloc((long long)bt_halo_v.size()), (long long)bt_halo_v.size()};
-    hc.tfaces = {a_tface_.alloc((long long)bt_face_v.size()), (long long)bt_face_v.size()};
-    if (hc.halo.b < 0 || hc.tfaces.b < 0 || n_btiles_total() + (long long)btiles.size() > cap_btiles_) {
-      release_ranges(hc);
-      return 3;
-    }
-    for (BTile& t : btiles) {
-      t.c0 += cb;
-      t.c1 += cb;
-      t.h0 += (int)hc.halo.b;
-      t.h1 += (int)hc.halo.b;
-      t.f0 += (int)hc.tfaces.b;
-      t.f1 += (int)hc.tfaces.b;
-      t.w0 += wb;
-      t.w1 += wb;
-    }
-    PVec<int> bt_halo = pv<int>(bt_halo_v.size()), bt_face = pv<int>(bt_face_v.size());
-    PVec<int2> bt_floc(bt_floc_v.begin(), bt_floc_v.end(), PinAlloc<int2>(&stage_));
-    for (size_t i = 0; i < bt_halo_v.size(); ++i) bt_halo[i] = bt_halo_v[i] + cb;
-    for (size_t i = 0; i < bt_face_v.size(); ++i) bt_face[i] = bt_face_v[i] + fb;
-    hc.btiles = std::move(btiles);
+    // block-tile tables in the case's ranges
+    PVec<int> bt_halo = pvu<int>(S, j.bt_halo.size()), bt_face = pvu<int>(S, j.bt_face.size());
+    for (size_t i = 0; i < j.bt_halo.size(); ++i) bt_halo[i] = j.bt_halo[i] + cb;
+    for (size_t i = 0; i < j.bt_face.size(); ++i) bt_face[i] = j.bt_face[i] + fb;
+    PVec<int2> bt_floc(j.bt_floc.begin(), j.bt_floc.end(), PinAlloc<int2>(&S));
+    PVec<int> s_loc(j.s_loc.begin(), j.s_loc.end(), PinAlloc<int>(&S));
+    PVec<int> w_ldon(j.w_ldon.begin(), j.w_ldon.end(), PinAlloc<int>(&S));
     // SRD arrays
     const int gb = (int)hc.groups.b, gmb = (int)hc.gmembers.b, qb = (int)hc.qcells.b, qlb = (int)hc.qlist.b;
-    PVec<int> g_mem = pv<int>(ng + 1), g_cell = pv<int>(gmem), q_cell = pv<int>(ng + 1, cb + (int)n),
-              q_grp = pv<int>(ng + 1), q_list = pv<int>(qlist);
-    PVec<double> g_cnt = pv<double>(gmem), g_vol = pv<double>(ng + 1, 1.0), q_cnt = pv<double>(ng + 1, 1.0);
+    PVec<int> g_mem = pv<int>(S, ng + 1, 0), g_cell = pv<int>(S, j.gmem, 0), q_cell = pv<int>(S, ng + 1, cb + (int)n),
+              q_grp = pv<int>(S, ng + 1, 0), q_list = pv<int>(S, j.qlist, 0);
+    PVec<double> g_cnt = pv<double>(S, j.gmem, 0.0), g_vol = pv<double>(S, ng + 1, 1.0), q_cnt = pv<double>(S, ng + 1, 1.0);
     {
-      long long pos = 0;
+      long long pos = 0, lpos = 0;
       for (long long gi = 0; gi < ng; ++gi) {
-        const long long g = groups_nt[gi];
+        const long long g = j.nontrivial[gi];
         g_mem[gi] = gmb + (int)pos;
         g_vol[gi] = m->group_volume[g];
         for (uint64_t q = m->group_offsets[g]; q < m->group_offsets[g + 1]; ++q, ++pos) {
@@ -623,14 +918,13 @@ template <class R> class Batch final : public BatchBase {
         }
       }
       g_mem[ng] = gmb + (int)pos;
-      long long lpos = 0;
       for (long long qi = 0; qi < ng; ++qi) {
-        const long long k = cells_nt[qi];
+        const long long k = j.nontrivial[qi];
         q_cell[qi] = cb + (int)k;
         q_grp[qi] = qlb + (int)lpos;
         q_cnt[qi] = (double)(m->member_offsets[k + 1] - m->member_offsets[k]);
         for (uint64_t q = m->member_offsets[k]; q < m->member_offsets[k + 1]; ++q, ++lpos)
-          q_list[lpos] = gb + group_index[m->member_groups[q]];
+          q_list[lpos] = gb + j.group_index[m->member_groups[q]];
       }
       q_grp[ng] = qlb + (int)lpos;
     }
@@ -672,74 +966,104 @@ template <class R> class Batch final : public BatchBase {
     cf.srd_g1 = gb + (int)ng;
     cf.srd_q0 = qb;
     cf.srd_q1 = qb + (int)ng;
-    cf.srd_rate = model_ >= MODEL_LAMINAR && m->transport.stabilization == AMR_B200_VISCOUS_SRD && m->small_cells > 0 &&
-                  cf.has_srd;
+    cf.srd_rate = viscous && m->transport.stabilization == AMR_B200_VISCOUS_SRD && m->small_cells > 0 && cf.has_srd;
     cf.cell0 = cb;
     cf.cell1 = cb + (int)n;
-    // state
-    const long long ncap = cap_cells_;
-    PVec<R> u = pv<R>(nv_ * (n + 1), R(1));
-    for (int v = 0; v < nv_; ++v)
-      for (long long k = 0; k < n; ++k) u[v * (n + 1) + k] = (R)u0[v * n + k];
+    // state (variable-major, each variable's n cells then the padding cell)
+    PVec<R> u = pvu<R>(S, nv_ * (n + 1));
+    for (int v = 0; v < nv_; ++v) {
+      for (long long k = 0; k < n; ++k) u[v * (n + 1) + k] = (R)sp.u0[v * n + k];
+      u[v * (n + 1) + n] = R(1);
+    }
     // control
-    CaseCtl ctl;
+    CaseCtl& ctl = j.ctl;
     std::memset(&ctl, 0, sizeof(ctl));
-    ctl.time = time0;
-    ctl.target = target;
-    ctl.steps = steps0;
-    ctl.rejected = rejected0;
-    ctl.maxsteps = maxsteps;
-    ctl.finished = time0 >= target;
+    ctl.time = sp.time0;
+    ctl.target = sp.target;
+    ctl.steps = sp.steps0;
+    ctl.rejected = sp.rejected0;
+    ctl.maxsteps = sp.maxsteps;
+    ctl.finished = sp.time0 >= sp.target;
     ctl.live = 1;
     ctl.cur = 0;
     ctl.dtmin = DT_INF_BITS;
     // uploads
-    uint64_t* G = &stats_.geometry_h2d_bytes;
-    bool ok = up(c_case_.p + cb, c_case, G) && up(c_vol_.p + cb, c_vol, G) && up(c_area_.p + cb, c_area, G) &&
-              up(c_gvol_.p + cb, c_gvol, G) && up(c_flags_.p + cb, c_flags, G) && up(c_slot_.p + cb, c_slot, G) &&
-              up(c_wall_.p + cb, c_wall, G) && up(c_term_.p + cb, c_term, G) && up(c_cx_.p + cb, c_cx, G) &&
-              up(c_cy_.p + cb, c_cy, G) && up(s_own_.p + sb, s_own, G) && up(s_nb_.p + sb, s_nb, G) &&
-              up(s_meta_.p + sb, s_meta, G) && up(s_len_.p + sb, s_len, G) && up(w_nx_.p + wb, w_nx, G) &&
-              up(w_ny_.p + wb, w_ny, G) && up(w_len_.p + wb, w_len, G) && up(w_dist_.p + wb, w_dist, G) &&
-              up(w_donor_.p + wb, w_donor, G) && up(w_xm_.p + wb, w_xm, G) && up(w_ym_.p + wb, w_ym, G) &&
-              up(g_mem_.p + gb, g_mem, G) && up(g_cell_.p + gmb, g_cell, G) && up(g_cnt_.p + gmb, g_cnt, G) &&
-              up(g_vol_.p + gb, g_vol, G) && up(q_cell_.p + qb, q_cell, G) && up(q_grp_.p + qb, q_grp, G) &&
-              up(q_list_.p + qlb, q_list, G) && up(q_cnt_.p + qb, q_cnt, G);
-    ok = ok && up(s_geo_.p + 6 * (long long)sb, s_geo, G) && up(s_item_.p + sb, s_item, G) &&
-         up(f_case_.p + fb, f_case, G) && up(f_own_.p + fb, f_own, G) && up(f_nb_.p + fb, f_nb, G) &&
-         up(f_meta_.p + fb, f_meta, G) && up(f_len_.p + fb, f_len, G) && up(f_geo_.p + 6 * (long long)fb, f_geo, G) &&
-         up(w_owner_.p + wb, w_owner, G) && up(bt_halo_.p + hc.halo.b, bt_halo, G) &&
-         up(bt_face_.p + hc.tfaces.b, bt_face, G) && up(bt_floc_.p + hc.tfaces.b, bt_floc, G) &&
-         up(s_loc_.p + sb, s_loc, G) && up(w_ldon_.p + wb, w_ldon, G);
-    if (ok && model_ >= MODEL_LAMINAR)
-      ok = up(t_own_.p + tb, t_own, G) && up(t_src_.p + tb, t_src, G) &&
-           up(t_x_.p + tb, t_x, G) && up(t_y_.p + tb, t_y, G);
-    if (ok && model_ == MODEL_SA) ok = up(c_wd_.p + cb, c_wd, G);
+    uint64_t* G = &j.geometry_bytes;
+    bool ok = up(st, c_case_.p + cb, c_case, G) && up(st, c_vol_.p + cb, c_vol, G) && up(st, c_area_.p + cb, c_area, G) &&
+              up(st, c_gvol_.p + cb, c_gvol, G) && up(st, c_flags_.p + cb, c_flags, G) &&
+              up(st, c_slot_.p + cb, c_slot, G) && up(st, c_wall_.p + cb, c_wall, G) && up(st, c_term_.p + cb, c_term, G) &&
+              up(st, c_cx_.p + cb, c_cx, G) && up(st, c_cy_.p + cb, c_cy, G) && up(st, s_own_.p + sb, s_own, G) &&
+              up(st, s_nb_.p + sb, s_nb, G) && up(st, s_meta_.p + sb, s_meta, G) && up(st, s_len_.p + sb, s_len, G) &&
+              up(st, w_nx_.p + wb, w_nx, G) && up(st, w_ny_.p + wb, w_ny, G) && up(st, w_len_.p + wb, w_len, G) &&
+              up(st, w_dist_.p + wb, w_dist, G) && up(st, w_donor_.p + wb, w_donor, G) && up(st, w_xm_.p + wb, w_xm, G) &&
+              up(st, w_ym_.p + wb, w_ym, G) && up(st, g_mem_.p + gb, g_mem, G) && up(st, g_cell_.p + gmb, g_cell, G) &&
+              up(st, g_cnt_.p + gmb, g_cnt, G) && up(st, g_vol_.p + gb, g_vol, G) && up(st, q_cell_.p + qb, q_cell, G) &&
+              up(st, q_grp_.p + qb, q_grp, G) && up(st, q_list_.p + qlb, q_list, G) && up(st, q_cnt_.p + qb, q_cnt, G);
+    ok = ok && up(st, s_geo_.p + 6 * (long long)sb, s_geo, G) && up(st, s_item_.p + sb, s_item, G) &&
+         up(st, f_case_.p + fb, f_case, G) && up(st, f_own_.p + fb, f_own, G) && up(st, f_nb_.p + fb, f_nb, G) &&
+         up(st, f_meta_.p + fb, f_meta, G) && up(st, f_len_.p + fb, f_len, G) &&
+         up(st, f_geo_.p + 6 * (long long)fb, f_geo, G) && up(st, w_owner_.p + wb, w_owner, G) &&
+         up(st, bt_halo_.p + hc.halo.b, bt_halo, G) && up(st, bt_face_.p + hc.tfaces.b, bt_face, G) &&
+         up(st, bt_floc_.p + hc.tfaces.b, bt_floc, G) && up(st, s_loc_.p + sb, s_loc, G) &&
+         up(st, w_ldon_.p + wb, w_ldon, G);
+    if (ok && viscous)
+      ok = up(st, t_own_.p + tb, t_own, G) && up(st, t_src_.p + tb, t_src, G) && up(st, t_x_.p + tb, t_x, G) &&
+           up(st, t_y_.p + tb, t_y, G);
+    if (ok && model_ == MODEL_SA) ok = up(st, c_wd_.p + cb, c_wd, G);
     for (int v = 0; ok && v < nv_; ++v) {
-      ok = stage_up(U0_.p + v * ncap + cb, u.data() + v * (n + 1), sizeof(R) * (n + 1));
-      stats_.state_h2d_bytes += sizeof(R) * (n + 1);
+      ok = stage_up(st, U0_.p + v * cap_cells_ + cb, u.data() + v * (n + 1), sizeof(R) * (n + 1));
+      j.state_bytes += sizeof(R) * (n + 1);
     }
-    CaseCfg<R>* cf_staged = static_cast<CaseCfg<R>*>(stage_.take(sizeof(cf)));
+    CaseCfg<R>* cf_staged = static_cast<CaseCfg<R>*>(S.take(sizeof(cf)));
     *cf_staged = cf;
-    ok = ok && stage_up(cfg_.p + slot, cf_staged, sizeof(cf));
-    if (!ok) return fail_release(hc, error, "upload staging");
-    ok = flush_uploads(error);
-    h_ctl_[slot] = ctl;
-    ok = ok && cuda_ok(cudaMemcpyAsync(ctl_.p + slot, &h_ctl_[slot], sizeof(CaseCtl), cudaMemcpyHostToDevice, stream_),
-                       error, "control upload");
-    stats_.control_h2d_bytes += sizeof(CaseCtl);
-    ok = ok && cuda_ok(cudaStreamSynchronize(stream_), error, "admit sync");
-    if (!ok) {
-      release_ranges(hc);
-      return 1;
+    ok = ok && stage_up(st, cfg_.p + slot, cf_staged, sizeof(cf));
+    if (!ok) return job_fail(j, 1, "upload staging");
+    if (!flush_uploads(st, &j.error)) return (void)(j.status = 1);
+    if (!st.done && !cuda_ok(cudaEventCreateWithFlags(&st.done, cudaEventDisableTiming), &j.error, "staging event"))
+      return (void)(j.status = 1);
+    if (!cuda_ok(cudaEventRecord(st.done, stream_), &j.error, "staging event")) return (void)(j.status = 1);
+    st.pending = true;
+  }
+
+  // Stage 4 (serial): control records of the filled cases, one synchronisation, then the
+  // host bookkeeping in request order; failed cases give their slot and ranges back.
+  void commit(std::vector<AdmitJob>& jobs) {
+    for (AdmitJob& j : jobs)
+      if (j.status == 0) {
+        h_ctl_[j.slot] = j.ctl;
+        if (!cuda_ok(cudaMemcpyAsync(ctl_.p + j.slot, &h_ctl_[j.slot], sizeof(CaseCtl), cudaMemcpyHostToDevice, stream_),
+                     &j.error, "control upload"))
+          j.status = 1;
+      }
+    std::string err;
+    const bool synced = cuda_ok(cudaStreamSynchronize(stream_), &err, "admit sync");
+    for (std::unique_ptr<Stager>& s : stagers_) {
+      s->pending = false;
+      stats_.allocated_bytes += s->allocated;
+      s->allocated = 0;
+      stats_.pinned_bytes += s->stage.pinned_bytes() - s->pinned_seen;
+      s->pinned_seen = s->stage.pinned_bytes();
     }
-    hc.live = true;
-    cases_[slot] = std::move(hc);
-    live_++;
-    refresh_meta(slot);
-    tiles_dirty_ = true;
-    *slot_out = slot;
-    return 0;
+    for (AdmitJob& j : jobs) {
+      if (j.status == 0 && !synced) job_fail(j, 1, err);
+      if (j.reserved) {
+        reserved_[j.slot] = 0;
+        pending_tiles_ -= (long long)j.hc.tiles.size();
+        pending_btiles_ -= (long long)j.hc.btiles.size();
+      }
+      if (j.status != 0) {
+        if (j.reserved) release_ranges(j.hc);
+        continue;
+      }
+      stats_.geometry_h2d_bytes += j.geometry_bytes;
+      stats_.state_h2d_bytes += j.state_bytes;
+      stats_.control_h2d_bytes += sizeof(CaseCtl);
+      j.hc.live = true;
+      cases_[j.slot] = std::move(j.hc);
+      live_++;
+      refresh_meta(j.slot);
+      tiles_dirty_ = true;
+    }
   }
 
   int release(int slot) override {
@@ -902,49 +1226,54 @@ template <class R> class Batch final : public BatchBase {
     return fail1(error, text);
   }
 
-  template <class T> PVec<T> pv(size_t count, const T& value = T()) {
-    return PVec<T>(count, value, PinAlloc<T>(&stage_));
+  template <class T> static PVec<T> pv(PinnedStage& S, size_t count, const T& value) {
+    return PVec<T>(count, value, PinAlloc<T>(&S));
+  }
+  template <class T> static PVec<T> pvu(PinnedStage& S, size_t count) {  // contents left uninitialised
+    return PVec<T>(count, PinAlloc<T>(&S));
   }
 
   // Records the upload of a staged table; flush_uploads moves them all.
-  bool stage_up(void* dst, const void* host, size_t bytes) {
+  static bool stage_up(Stager& st, void* dst, const void* host, size_t bytes) {
     if (bytes == 0) return true;
-    const long long off = stage_.dev_offset(host);
+    const long long off = st.stage.dev_offset(host);
     if (off < 0) return false;
-    uploads_.push_back({reinterpret_cast<unsigned long long>(dst), (unsigned long long)off, (unsigned long long)bytes});
+    st.uploads.push_back({reinterpret_cast<unsigned long long>(dst), (unsigned long long)off, (unsigned long long)bytes});
     return true;
   }
-  template <class T> bool up(T* dst, const PVec<T>& src, uint64_t* counter) {
+  template <class T> static bool up(Stager& st, T* dst, const PVec<T>& src, uint64_t* counter) {
     *counter += sizeof(T) * src.size();
-    return stage_up(dst, src.data(), sizeof(T) * src.size());
+    return stage_up(st, dst, src.data(), sizeof(T) * src.size());
   }
 
-  // One DMA per used staging block into the device staging buffer, then the scatter kernel;
-  // asynchronous on stream_ (the caller synchronises before the staging memory is reused).
-  bool flush_uploads(std::string* error) {
-    if (d_stage_.n < stage_.total()) {
-      stats_.allocated_bytes -= d_stage_.p ? d_stage_.n : 0;
-      d_stage_.free();
-      if (!d_stage_.alloc(stage_.total(), &stats_.allocated_bytes, error, "upload staging")) return false;
+  // One DMA per used staging block into the worker's device staging buffer, then the scatter
+  // kernel; asynchronous on stream_ (the staging memory is reused only after the worker's event).
+  bool flush_uploads(Stager& st, std::string* error) {
+    unsigned char* base = st.dev_ext;
+    if (!base || st.stage.total() > st.dev_ext_n) {
+      if (st.dev.n < st.stage.total()) {
+        st.allocated -= st.dev.p ? st.dev.n : 0;
+        st.dev.free();
+        if (!st.dev.alloc(st.stage.total(), &st.allocated, error, "upload staging")) return false;
+      }
+      base = st.dev.p;
     }
-    stats_.pinned_bytes += stage_.pinned_bytes() - stage_pinned_seen_;
-    stage_pinned_seen_ = stage_.pinned_bytes();
-    for (const PinnedStage::Block& b : stage_.blocks())
-      if (b.used && !cuda_ok(cudaMemcpyAsync(d_stage_.p + b.dev, b.p, b.used, cudaMemcpyHostToDevice, stream_), error,
+    for (const PinnedStage::Block& b : st.stage.blocks())
+      if (b.used && !cuda_ok(cudaMemcpyAsync(base + b.dev, b.p, b.used, cudaMemcpyHostToDevice, stream_), error,
                              "staging upload"))
         return false;
-    for (size_t i0 = 0; i0 < uploads_.size(); i0 += UPLOAD_TABLES) {
+    for (size_t i0 = 0; i0 < st.uploads.size(); i0 += UPLOAD_TABLES) {
       UploadTable t;
-      t.n = (int)std::min<size_t>(UPLOAD_TABLES, uploads_.size() - i0);
+      t.n = (int)std::min<size_t>(UPLOAD_TABLES, st.uploads.size() - i0);
       unsigned long long most = 0;
       for (int i = 0; i < t.n; ++i) {
-        t.dst[i] = uploads_[i0 + i].dst;
-        t.src[i] = uploads_[i0 + i].src;
-        t.bytes[i] = uploads_[i0 + i].bytes;
+        t.dst[i] = st.uploads[i0 + i].dst;
+        t.src[i] = st.uploads[i0 + i].src;
+        t.bytes[i] = st.uploads[i0 + i].bytes;
         most = std::max(most, t.bytes[i]);
       }
       const unsigned gx = (unsigned)std::min<unsigned long long>(64, (most + 8191) / 8192);
-      scatter_uploads_kernel<<<dim3(gx, (unsigned)t.n), 256, 0, stream_>>>(d_stage_.p, t);
+      scatter_uploads_kernel<<<dim3(gx, (unsigned)t.n), 256, 0, stream_>>>(base, t);
       if (!cuda_ok(cudaGetLastError(), error, "upload scatter")) return false;
     }
     return true;
@@ -956,8 +1285,9 @@ template <class R> class Batch final : public BatchBase {
     const long long n = hc.n;
     if (count != (uint64_t)(nv_ * n)) return fail1(error, "state size mismatch");
     // one strided copy of the nv variable rows into page-locked staging
-    stage_.reset();
-    R* tmp = static_cast<R*>(stage_.take(sizeof(R) * nv_ * n));
+    PinnedStage& S = stagers_[0]->stage;  // idle: every admission ends synchronised
+    S.reset();
+    R* tmp = static_cast<R*>(S.take(sizeof(R) * nv_ * n));
     if (!cuda_ok(cudaMemcpy2DAsync(tmp, sizeof(R) * n, buf + hc.cells.b, sizeof(R) * cap_cells_, sizeof(R) * n, nv_,
                                    cudaMemcpyDeviceToHost, stream_), error, "download"))
       return 1;
@@ -1032,7 +1362,7 @@ template <class R> class Batch final : public BatchBase {
     return true;
   }
 
-  bool make_tiles(HostCase<R>& hc, std::string* why) {
+  bool make_tiles(HostCase<R>& hc, std::string* why) const {
     const long long n = hc.n;
     const int cb = (int)hc.cells.b;
     const int B = TILE_W;
@@ -1083,7 +1413,7 @@ template <class R> class Batch final : public BatchBase {
   // is the face's left, or the tile wall index) and per wall the donor's local index.
   bool make_block_tiles(const amr_mesh_view_t* m, long long n, const std::vector<int>& rec, int slot,
                         std::vector<BTile>* tiles, std::vector<int>* halo_out, std::vector<int>* face_out,
-                        std::vector<int2>* floc_out, PVec<int>* s_loc, PVec<int>* w_ldon,
+                        std::vector<int2>* floc_out, std::vector<int>* s_loc, std::vector<int>* w_ldon,
                         std::string* why) const {
     const long long nf = (long long)m->n_faces;
     const bool viscous = model_ >= MODEL_LAMINAR;
@@ -1454,7 +1784,8 @@ template <class R> class Batch final : public BatchBase {
   }
 
   void DevBufFreeAll() {
-    d_stage_.free();
+    free_arena();
+    stagers_.clear();
     ctl_.free(); cfg_.free(); tiles_.free(); bar_.free();
     c_case_.free(); c_vol_.free(); c_area_.free(); c_gvol_.free(); c_flags_.free(); c_slot_.free(); c_wall_.free();
     c_term_.free(); c_cx_.free(); c_cy_.free(); c_wd_.free();
@@ -1526,13 +1857,13 @@ template <class R> class Batch final : public BatchBase {
   DevBuf<R> U0_, U1_, U2_, R0_, grad_, mu_, eddy_, sgrad_, sdiff_, ssrc_, srate_;
   DevBuf<double> diag_part_, diag_out_, diag_cfg_, ddt_, ex_buf_;
   DevBuf<int> case_tiles_;
-  PinnedStage stage_;  // host staging of admissions and downloads
-  struct Upload {
-    unsigned long long dst, src, bytes;
-  };
-  std::vector<Upload> uploads_;
-  DevBuf<unsigned char> d_stage_;
-  size_t stage_pinned_seen_ = 0;
+  std::vector<std::unique_ptr<Stager>> stagers_;  // two per admission worker; the first also serves downloads
+  char* arena_h_ = nullptr;                        // staging arena (ensure_arena)
+  unsigned char* arena_d_ = nullptr;
+  size_t arena_slice_ = 0;
+  int arena_stages_ = 0;
+  std::vector<char> reserved_;                     // slots reserved by an admission in progress
+  long long pending_tiles_ = 0, pending_btiles_ = 0;
 };
 
 }  // namespace amrb

@@ -15,6 +15,7 @@
 #include "amr_host.h"
 
 using amrb::BatchBase;
+using amrb::AdmitSpec;
 
 namespace {
 void put(char* buf, uint64_t size, const std::string& text) {
@@ -309,6 +310,42 @@ int amr_batch_admit(amr_batch* b, const amr_mesh_view_t* mesh, const amr_params_
   b->steady[s] = cs;
   *slot = s;
   return 0;
+}
+
+int amr_batch_admit_many(amr_batch* b, uint64_t count, const amr_mesh_view_t* const* meshes,
+                         const amr_params_t* const* params, const double* const* u0, const uint64_t* u0_counts,
+                         const amr_case_control_t* const* controls, int32_t threads, int32_t* slots,
+                         int32_t* status, char* error, uint64_t error_size) {
+  if (!b || (count && (!meshes || !params || !u0 || !u0_counts || !controls || !slots || !status))) return 1;
+  std::vector<AdmitSpec> specs(count);
+  for (uint64_t i = 0; i < count; ++i) {
+    if (!meshes[i] || !controls[i]) {
+      put(error, error_size, "null mesh or control");
+      return 1;
+    }
+    const amr_case_control_t& c = *controls[i];
+    const double first = c.check_period > 0 ? std::min(c.first_check, c.tend) : c.tend;
+    specs[i] = AdmitSpec{meshes[i], params[i], u0[i], u0_counts[i], 0.0, first, 0, 0, c.maxsteps};
+  }
+  std::vector<int> s, st;
+  std::vector<std::string> errs;
+  const int rc = b->batch->admit_many(specs, threads, &s, &st, &errs);
+  bool reported = false;
+  for (uint64_t i = 0; i < count; ++i) {
+    slots[i] = s[i];
+    status[i] = st[i];
+    if (st[i] == 1 && !reported) {
+      put(error, error_size, "case " + std::to_string(i) + ": " + errs[i]);
+      reported = true;
+    }
+    if (st[i] != 0) continue;
+    CaseSteady cs;
+    cs.ctl = *controls[i];
+    cs.sa_nu_inf = meshes[i]->transport.sa_nu_inf;
+    cs.nv = meshes[i]->transport.sa_model ? 5 : 4;
+    b->steady[s[i]] = cs;
+  }
+  return rc;
 }
 
 int amr_batch_advance(amr_batch* b, int32_t trials, char* error, uint64_t error_size) {

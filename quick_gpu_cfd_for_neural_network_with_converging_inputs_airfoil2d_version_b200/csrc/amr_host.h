@@ -16,6 +16,17 @@ struct CaseMeta {
   int fatal, finished, active, live, cur;
 };
 
+// One admission request: mesh, parameters, initial state u0[u0_count] and the case's start
+// (time, accepted and rejected steps) and first advance target.
+struct AdmitSpec {
+  const amr_mesh_view_t* mesh;
+  const amr_params_t* params;
+  const double* u0;
+  uint64_t u0_count;
+  double time0, target;
+  long long steps0, rejected0, maxsteps;
+};
+
 class BatchBase {
  public:
   virtual ~BatchBase() = default;
@@ -23,6 +34,12 @@ class BatchBase {
   virtual int admit(const amr_mesh_view_t* mesh, const amr_params_t* params, const double* u0, uint64_t u0_count,
                     double time0, long long steps0, long long rejected0, double target, long long maxsteps,
                     int* slot, std::string* error) = 0;
+  // Admits several cases, preparing them on `threads` host threads (0: up to 8); per case the
+  // slot (-1 unless admitted), the status (0, 1 or 3 as admit) and the message of a status 1.
+  // Slots and arena ranges go in request order whatever the thread count.  Returns 1 if any
+  // case was invalid, else 3 if any found no room, else 0.
+  virtual int admit_many(const std::vector<AdmitSpec>& specs, int threads, std::vector<int>* slots,
+                         std::vector<int>* status, std::vector<std::string>* errors) = 0;
   virtual int release(int slot) = 0;
   // Runs `trials` trials of every live case and refreshes the host copies of the controls.
   virtual int advance(int trials, std::string* error) = 0;

@@ -1,0 +1,75 @@
+"""GPU tests of bulk admission (amr_batch_admit_many): cases converted on several host threads
+land in the same slots and arena ranges as one-by-one admissions in request order, so the
+batch computes bit for bit the same; an invalid or unplaceable entry is reported per entry
+while the others are admitted."""
+import numpy as np
+import pytest
+
+from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200 import _abi, cases
+from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200.batch import Batch, BatchError, case_control
+from tests.test_gpu_launch_modes import MODES, sa_mix
+
+pytestmark = pytest.mark.gpu
+
+
+def items_of(mix, nsteps):
+    out = []
+    for spec, mesh in mix:
+        u0 = cases.initial_state(mesh, spec.initial_primitive())
+        out.append((mesh, spec.params(), u0, case_control(1e30, nsteps, steady=False, mach=spec.mach, aoa=spec.aoa)))
+    return out
+
+
+def run(items, precision, mode, threads, max_cases, bulk):
+    b = Batch(precision=precision, model=_abi.MODEL_LAMINAR, sa=True, max_cases=max_cases,
+              max_cells=sum(m.n_cells for m, _, _, _ in items) + 1000, **MODES[mode])
+    if bulk:
+        slots = b.admit_many(items, threads=threads)
+    else:
+        slots = [b.admit(*it) for it in items]
+    for _ in range(8):
+        b.advance(16)
+    states = [b.download(s) for s in slots]
+    steps = [b.status(s)['steps'] for s in slots]
+    b.destroy()
+    return slots, states, steps
+
+
+@pytest.mark.parametrize('precision,mode', [(32, 'split'), (64, 'tiled')])
+def test_bulk_equals_sequential(precision, mode):
+    mix = sa_mix()
+    items = items_of(mix + mix[:2], 12)
+    ref_slots, ref_states, ref_steps = run(items, precision, mode, 1, 8, bulk=False)
+    for threads in (1, 4, 0):
+        slots, states, steps = run(items, precision, mode, threads, 8, bulk=True)
+        assert slots == ref_slots and steps == ref_steps, threads
+        for a, b in zip(states, ref_states):
+            assert np.array_equal(a, b), threads
+
+
+def test_bulk_more_cases_than_a_chunk():
+    """40 entries span two preparation chunks; slots follow the request order."""
+    mix = sa_mix()
+    items = items_of([mix[i % 3] for i in range(40)], 4)
+    ref_slots, ref_states, _ = run(items, 32, 'split', 1, 40, bulk=False)
+    slots, states, _ = run(items, 32, 'split', 6, 40, bulk=True)
+    assert slots == ref_slots == list(range(40))
+    for a, b in zip(states, ref_states):
+        assert np.array_equal(a, b)
+
+
+def test_bulk_reports_invalid_and_full_entries():
+    mix = sa_mix()
+    items = items_of(mix, 8)
+    mesh, params, u0, ctl = items[1]
+    bad = (mesh, params, u0[:-1], ctl)  # wrong state size
+    b = Batch(precision=32, model=_abi.MODEL_LAMINAR, sa=True, max_cases=2,
+              max_cells=sum(m.n_cells for _, m in mix) + 1000, **MODES['split'])
+    with pytest.raises(BatchError) as e:
+        b.admit_many([items[0], bad, items[2], items[1]], threads=3)
+    assert 'case 1' in str(e.value) and 'initial state size mismatch' in str(e.value)
+    assert e.value.slots == [0, None, 1, None]  # entry 3 found no free case slot
+    b.advance(16)
+    alone = run([items[2]], 32, 'split', 1, 2, bulk=False)[1][0]
+    assert np.array_equal(b.download(1), alone)
+    b.destroy()
