@@ -15,6 +15,7 @@ import json
 import math
 import os
 import pathlib
+import select
 import statistics
 import subprocess
 import sys
@@ -68,21 +69,29 @@ def algorithmic_bytes(mesh, s=4, sg=4):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every `interval_ms` while entered (the
+    batched bench enters it for the warm-up and timed loop only, so idle set-up time, when the
+    GPU drops its clocks, does not count)."""
     FIELDS = 'index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,' \
              'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap'
 
-    def __init__(self, device):
+    def __init__(self, device, interval_ms=200):
         self.device = device
+        self.interval_ms = int(interval_ms)
         self.proc = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.device), '--query-gpu=' + self.FIELDS,
-                                          '--format=csv,noheader,nounits', '-lms', '200'], stdout=subprocess.PIPE,
+                                          '--format=csv,noheader,nounits', '-lms', str(self.interval_ms)], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+        # wait (at most 5 s) for nvidia-smi's first sample, taken before the sampled work starts,
+        # and drop it, so that every kept sample falls inside the sampled region
+        if self.proc:
+            if select.select([self.proc.stdout], [], [], 5.0)[0]:
+                self.proc.stdout.readline()
         return self
 
     def __exit__(self, *exc):
@@ -135,9 +144,10 @@ def parse_launch(cfg):
     return block, grid, mode
 
 
-def run_batched(case_list, precision, steps, warmup, device=0, trials=32, block=0, grid=0, tune=True):
+def run_batched(case_list, precision, steps, warmup, device=0, trials=32, block=0, grid=0, tune=True, clock=None):
     """Admit every case, autotune, warm up, then time `steps` trials with CUDA events on the
-    engine stream.  Accepted cell-steps are counted per case from the device counters."""
+    engine stream.  Accepted cell-steps are counted per case from the device counters.  `clock`
+    (a ClockSampler) samples the warm-up and timed loop."""
     total_cells = sum(m.n_cells for _, m in case_list)
     b = Batch(precision=precision, model=_abi.MODEL_LAMINAR, sa=True, max_cases=len(case_list),
               max_cells=total_cells + 64, device=device, block_threads=block, grid_blocks=grid)
@@ -149,6 +159,8 @@ def run_batched(case_list, precision, steps, warmup, device=0, trials=32, block=
         slots.append(s)
     if tune:
         b.autotune(4)
+    if clock is not None:
+        clock.__enter__()
     done = 0
     while done < warmup:
         k = min(trials, warmup - done)
@@ -163,6 +175,8 @@ def run_batched(case_list, precision, steps, warmup, device=0, trials=32, block=
         dev_seconds += b.last_advance_seconds
         adv += k
         advances += 1
+    if clock is not None:
+        clock.__exit__(None, None, None)
     status = [b.status(s) for s in slots]
     cell_steps = sum(m.n_cells * (st['steps'] - b0) for (_, m), st, b0 in zip(case_list, status, before))
     return dict(batch=b, slots=slots, dev_seconds=dev_seconds, launches=b.kernel_launches - launches0,
@@ -421,8 +435,8 @@ def main():
         return
     hbm, peak_kind = peaks()
     dist_barrier(world)
-    with ClockSampler(local) as clk:
-        r = run_batched(case_list, 32, args.steps, args.warmup, device=local)
+    clk = ClockSampler(local, interval_ms=50)
+    r = run_batched(case_list, 32, args.steps, args.warmup, device=local, clock=clk)
     dev_seconds = dist_max(r['dev_seconds'], world)
     cell_steps = r['cell_steps']
     value = cell_steps * world / dev_seconds
