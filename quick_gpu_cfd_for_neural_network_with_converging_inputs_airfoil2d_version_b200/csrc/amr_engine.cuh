@@ -158,8 +158,8 @@ template <class R> struct Dev {
   const R* f_geo;   // 6 per face
   const int* w_owner;
   const int* s_item;
-  R* fval;          // 12 per face
-  R* wval;          // 12 per wall
+  R* fval;          // per face: 12 values, 8 in the compact FP32 viscous format (RecFormat)
+  R* wval;          // per wall: the same
   R* crec;          // CREC per cell: packed state and gradient-phase fields (viscous models)
   // tiled mode
   const BTile* btiles;
@@ -1316,6 +1316,55 @@ template <class R, int MODEL> __device__ __forceinline__ void load_record(const 
   if (base || MODEL == MODEL_SA) load_group(src + 8, col + 8);
 }
 
+// FP32 viscous records in split mode are compact: 8 values, the net flux (convective minus
+// viscous, which the cell sums only ever use as that difference) and the four spectral / SA
+// columns, 32 bytes instead of 48.  A wall contributes only momentum columns 1-2 of its
+// convective part, so its columns 0 and 3 carry the viscous values alone.  FP64 keeps all 12
+// columns so that its sums are formed exactly as the reference forms them.
+template <class R, int MODEL> struct RecFormat {
+  static constexpr bool compact = sizeof(R) == 4 && MODEL >= MODEL_LAMINAR;
+  static constexpr int stride = compact ? 8 : SM_COLS;
+};
+
+template <class R, int MODEL> __device__ __forceinline__ void store_item(R* dst, R* rec, bool base, bool wall) {
+  if (!RecFormat<R, MODEL>::compact) {
+    store_record<R, MODEL>(dst, rec, base);
+    return;
+  }
+  if (!base) rec[8] = rec[9] = rec[11] = R(0);
+  if (MODEL < MODEL_SA) rec[10] = rec[11] = R(0);
+  R net[4];
+  for (int v = 0; v < 4; ++v) net[v] = rec[v] - rec[4 + v];
+  if (wall) {
+    net[0] = rec[4];
+    net[3] = rec[7];
+  }
+  store_group(dst, net);
+  if (base || MODEL == MODEL_SA) store_group(dst + 4, rec + 8);
+}
+
+// The 12 columns of a stored item, flux columns multiplied by sg (the slot's orientation).
+template <class R, int MODEL>
+__device__ __forceinline__ void load_item(const R* src, R* col, bool base, bool wall, R sg) {
+  for (int c = 0; c < SM_COLS; ++c) col[c] = R(0);
+  if (!RecFormat<R, MODEL>::compact) {
+    load_record<R, MODEL>(src, col, base);
+    for (int v = 0; v < 4; ++v) col[v] = sg * col[v];
+    if (MODEL >= MODEL_LAMINAR)
+      for (int v = 4; v < 8; ++v) col[v] = sg * col[v];
+  } else {
+    load_group(src, col);
+    for (int v = 0; v < 4; ++v) col[v] = sg * col[v];
+    if (wall) {  // the viscous columns the cell sums take from a wall
+      col[4] = col[0];
+      col[7] = col[3];
+      col[0] = col[3] = R(0);
+    }
+    if (base || MODEL == MODEL_SA) load_group(src + 4, col + 8);
+  }
+  if (MODEL == MODEL_SA) col[10] = sg * col[10];
+}
+
 template <class R, int MODEL>
 __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::cell) grad_cells_kernel(Dev<R> d, int stage) {
   const int rule = stage_rule(stage);
@@ -1365,7 +1414,7 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::item) item_kernel(De
         slot_face<R, MODEL, FLUX>(d, d.cfg[cs], d.f_geo + 6 * (long long)f, __ldg(d.f_len + f), own, nb,
                                   __ldg(d.f_meta + f), stage_input(d, stage, c.cur), base, rec, 1, false, bad);
       }
-      store_record<R, MODEL>(d.fval + SM_COLS * (long long)f, rec, base);
+      store_item<R, MODEL>(d.fval + RecFormat<R, MODEL>::stride * (long long)f, rec, base, false);
     } else {
       const int w = idx - nf;
       const int owner = d.w_owner[w];
@@ -1380,7 +1429,7 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::item) item_kernel(De
       else
         slot_wall<R, MODEL>(d, d.cfg[cs], __ldg(d.w_nx + w), __ldg(d.w_ny + w), __ldg(d.w_dist + w), __ldg(d.w_len + w),
                             owner, __ldg(d.w_donor + w), stage_input(d, stage, c.cur), base, rec, 1, bad);
-      store_record<R, MODEL>(d.wval + SM_COLS * (long long)w, rec, base);
+      store_item<R, MODEL>(d.wval + RecFormat<R, MODEL>::stride * (long long)w, rec, base, true);
     }
     if (bad && stage != STAGE_DIAG) atomicOr(&d.ctl[cs].bad, 1);
   }
@@ -1392,16 +1441,10 @@ template <class R, int MODEL> struct ItemSlots {
   bool base;
   __device__ __forceinline__ Cols<R> operator()(int q, bool wall) const {
     const int id = __ldg(d->s_item + q);  // wall index, or 2 * face record + (cell is the face's left)
-    const R* src = wall ? d->wval + SM_COLS * (long long)id : d->fval + SM_COLS * (long long)(id >> 1);
+    constexpr int S = RecFormat<R, MODEL>::stride;
+    const R* src = wall ? d->wval + S * (long long)id : d->fval + S * (long long)(id >> 1);
     Cols<R> o;
-    R* col = o.v;
-    for (int c = 0; c < SM_COLS; ++c) col[c] = R(0);
-    load_record<R, MODEL>(src, col, base);
-    const R sg = (wall || (id & 1)) ? R(1) : R(-1);
-    for (int v = 0; v < 4; ++v) col[v] = sg * col[v];
-    if (MODEL >= MODEL_LAMINAR)
-      for (int v = 4; v < 8; ++v) col[v] = sg * col[v];
-    if (MODEL == MODEL_SA) col[10] = sg * col[10];
+    load_item<R, MODEL>(src, o.v, base, wall, (wall || (id & 1)) ? R(1) : R(-1));
     return o;
   }
 };
