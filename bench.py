@@ -38,7 +38,7 @@ SOLVE_STEPS = 5000  # steps per solve of the batched workload
 # DRAM bytes (read + write) of one split-mode trial of the 256-case workload, summed over its
 # kernels from one ncu capture (profiles/split_trial_f32_sa_256cases.md; cold cache, so an upper
 # bound of a warm trial).  Reported as roofline.traffic when the run matches that configuration.
-SPLIT_256_TRAFFIC_PER_STEP = 3.5563e9
+SPLIT_256_TRAFFIC_PER_STEP = 3.1200e9
 
 
 def peaks():
@@ -423,12 +423,16 @@ def main():
         for spec, mesh in case_list:
             b.admit(mesh, spec.params(), cases.initial_state(mesh, spec.initial_primitive()),
                     case_control(1e30, 10 ** 9, steady=False))
-        done, sec = 0, 0.0
-        while done < args.warmup + args.steps:
-            k = min(32, args.warmup + args.steps - done)
+        done = 0
+        while done < args.warmup:
+            k = min(32, args.warmup - done)
             b.advance(k)
-            if done >= args.warmup:
-                sec += b.last_advance_seconds
+            done += k
+        done, sec = 0, 0.0
+        while done < args.steps:
+            k = min(32, args.steps - done)
+            b.advance(k)
+            sec += b.last_advance_seconds
             done += k
         print(json.dumps(dict(profile=args.profile, cases=len(case_list), precision=args.precision, block=args.block,
                               launch=b.launch_config(), ms_per_step=1e3 * sec / max(1, args.steps))))
