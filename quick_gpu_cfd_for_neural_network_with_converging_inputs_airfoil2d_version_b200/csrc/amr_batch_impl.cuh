@@ -357,6 +357,8 @@ template <class R> class Batch final : public BatchBase {
       return fail(error, "unknown launch mode");
     if (!cuda_ok(EngineOps<R>::tiled_setup(model_, flux_), error, "tiled kernel shared memory")) return false;
     mode_ = c.launch_mode == AMR_B200_LAUNCH_AUTO ? AMR_B200_LAUNCH_PERSISTENT : c.launch_mode;
+    // block tiles serve only the tiled mode, which a batch reaches by asking for it or by autotuning
+    block_tiles_ = c.launch_mode == AMR_B200_LAUNCH_AUTO || c.launch_mode == AMR_B200_LAUNCH_TILED;
     if (mode_ != AMR_B200_LAUNCH_PERSISTENT && block_ != PHASE_BLOCK)
       return fail(error, "the phase, split and tiled launch modes take block_threads 128");
     if (!configure_grid(error)) return false;
@@ -504,13 +506,13 @@ template <class R> class Batch final : public BatchBase {
   // Bytes fill() stages for a prepared case (each table rounded to the 256-byte allocation
   // grain), which sizes the staging arena; a larger case only takes a slower overflow path.
   size_t staged_bytes(size_t n, size_t nw, size_t ns, size_t nt, size_t nf, size_t ng, size_t gm, size_t ql,
-                      size_t halo, size_t tface) const {
-    const size_t r = sizeof(R), n1 = n + 1, g1 = ng + 1;
+                      size_t halo, size_t tface, bool tiles) const {
+    const size_t r = sizeof(R), n1 = n + 1, g1 = ng + 1, tl = tiles ? 1 : 0;
     const size_t tables[] = {4 * n1, 4 * n1, 4 * n1, 4 * n1, 8 * n1, 8 * n1, 8 * n1, 8 * n1, 8 * n1, n1,
                              model_ == MODEL_SA ? r * n1 : 0, 4 * ns, 4 * ns, 4 * ns, 4 * ns, r * ns, 6 * r * ns,
                              r * nw, r * nw, r * nw, r * nw, 8 * nw, 8 * nw, 4 * nw, 4 * nw, 4 * nt, 4 * nt, r * nt,
                              r * nt, 4 * nf, 4 * nf, 4 * nf, 4 * nf, r * nf, 6 * r * nf, 4 * halo, 4 * tface,
-                             8 * tface, 4 * ns, 4 * nw, 4 * g1, 4 * gm, 4 * g1, 4 * g1, 4 * ql, 8 * gm, 8 * g1, 8 * g1,
+                             8 * tface, 4 * ns * tl, 4 * nw * tl, 4 * g1, 4 * gm, 4 * g1, 4 * g1, 4 * ql, 8 * gm, 8 * g1, 8 * g1,
                              r * nv_ * n1, sizeof(CaseCfg<R>)};
     size_t total = 0;
     for (size_t b : tables) total += (b + 255) & ~size_t(255);
@@ -527,7 +529,7 @@ template <class R> class Batch final : public BatchBase {
     const size_t nt = model_ >= MODEL_LAMINAR && m->visc_offsets ? m->visc_offsets[n] : 0;
     const bool srd = m->small_cells && m->group_offsets && m->member_offsets;
     return staged_bytes(n, nw, ns, nt, nf, srd ? n : 0, srd ? m->group_offsets[n] : 0, srd ? m->member_offsets[n] : 0,
-                        2 * n, 2 * nf + 64);
+                        block_tiles_ ? 2 * n : 0, block_tiles_ ? 2 * nf + 64 : 0, block_tiles_);
   }
 
   // One page-locked host allocation and one device allocation, cut into `stages` equal slices
@@ -696,10 +698,12 @@ template <class R> class Batch final : public BatchBase {
     for (long long fi = 0; fi < j.nf; ++fi)
       if (j.rec[fi] < 0) j.rec[fi] = next++;  // a face no cell lists (still evaluated, never gathered)
     // block tiles (tiled mode), case-local
-    j.s_loc.assign(j.ns, 0);
-    j.w_ldon.assign(j.nw, 0);
-    if (!make_block_tiles(m, n, j.rec, -1, &hc.btiles, &j.bt_halo, &j.bt_face, &j.bt_floc, &j.s_loc, &j.w_ldon, &why))
-      return job_fail(j, 1, why);
+    if (block_tiles_) {
+      j.s_loc.assign(j.ns, 0);
+      j.w_ldon.assign(j.nw, 0);
+      if (!make_block_tiles(m, n, j.rec, -1, &hc.btiles, &j.bt_halo, &j.bt_face, &j.bt_floc, &j.s_loc, &j.w_ldon, &why))
+        return job_fail(j, 1, why);
+    }
   }
 
   // Stage 2 (serial, request order): a free slot and the case's ranges of every arena table.
@@ -1005,7 +1009,7 @@ template <class R> class Batch final : public BatchBase {
          up(st, f_geo_.p + 6 * (long long)fb, f_geo, G) && up(st, w_owner_.p + wb, w_owner, G) &&
          up(st, bt_halo_.p + hc.halo.b, bt_halo, G) && up(st, bt_face_.p + hc.tfaces.b, bt_face, G) &&
          up(st, bt_floc_.p + hc.tfaces.b, bt_floc, G) && up(st, s_loc_.p + sb, s_loc, G) &&
-         up(st, w_ldon_.p + wb, w_ldon, G);
+         up(st, w_ldon_.p + wb, w_ldon, G);  // the last five are empty without block tiles
     if (ok && viscous)
       ok = up(st, t_own_.p + tb, t_own, G) && up(st, t_src_.p + tb, t_src, G) && up(st, t_x_.p + tb, t_x, G) &&
            up(st, t_y_.p + tb, t_y, G);
@@ -1864,6 +1868,7 @@ template <class R> class Batch final : public BatchBase {
   int arena_stages_ = 0;
   std::vector<char> reserved_;                     // slots reserved by an admission in progress
   long long pending_tiles_ = 0, pending_btiles_ = 0;
+  bool block_tiles_ = true;  // cases carry block tiles (the batch may run the tiled mode)
 };
 
 }  // namespace amrb

@@ -305,6 +305,7 @@ template <class R> int Batch<R>::autotune(int trials, std::string* error) {
   // candidates run the way they run in production: replayed from a CUDA graph when graphs are on
   // (direct launches would penalise the multi-kernel modes by their host launch cost)
   for (int mode : {AMR_B200_LAUNCH_PERSISTENT, AMR_B200_LAUNCH_PHASES, AMR_B200_LAUNCH_SPLIT, AMR_B200_LAUNCH_TILED}) {
+    if (mode == AMR_B200_LAUNCH_TILED && !block_tiles_) continue;  // the cases carry no block tiles
     for (int block : {128, 256}) {
       if (mode != AMR_B200_LAUNCH_PERSISTENT && block != PHASE_BLOCK) continue;
       mode_ = mode;
