@@ -16,6 +16,7 @@
 #include <memory>
 #include <new>
 #include <string>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -397,12 +398,18 @@ template <class R> class Batch final : public BatchBase {
     for (const AdmitSpec& sp : specs) bound = std::max(bound, staged_bound(sp));
     // If it fails, the stages allocate their own blocks, as for a case above the bound.
     std::thread arena_thread;
-    if (bound)
-      arena_thread = std::thread([&] {
-        cudaSetDevice(config_.device);
+    if (bound) {
+      try {
+        arena_thread = std::thread([&] {
+          cudaSetDevice(config_.device);
+          std::string ignored;
+          if (!ensure_arena(threads, bound, &ignored)) cudaGetLastError();
+        });
+      } catch (const std::system_error&) {
         std::string ignored;
         if (!ensure_arena(threads, bound, &ignored)) cudaGetLastError();
-      });
+      }
+    }
     // chunks bound the host memory of prepared cases
     const size_t chunk = std::max<size_t>(32, 4 * (size_t)threads);
     bool invalid = false, full = false;
@@ -490,11 +497,18 @@ template <class R> class Batch final : public BatchBase {
     std::atomic<size_t> next{0};
     std::vector<std::thread> pool;
     const int t = (int)std::min<size_t>((size_t)threads, n);
-    for (int w = 0; w < t; ++w)
-      pool.emplace_back([&, w] {
-        cudaSetDevice(config_.device);  // the current device is per host thread
-        for (size_t i = next++; i < n; i = next++) f(i, w);
-      });
+    for (int w = 0; w < t; ++w) {
+      try {
+        pool.emplace_back([&, w] {
+          cudaSetDevice(config_.device);  // the current device is per host thread
+          for (size_t i = next++; i < n; i = next++) f(i, w);
+        });
+      } catch (const std::system_error&) {
+        break;  // the threads that started take all the work
+      }
+    }
+    if (pool.empty())
+      for (size_t i = 0; i < n; ++i) f(i, 0);
     for (std::thread& th : pool) th.join();
   }
 

@@ -191,6 +191,17 @@ __device__ __forceinline__ void st_release(unsigned int* p, unsigned int v) {
 }
 __device__ __forceinline__ int ld_volatile(const int* p) { return *(volatile const int*)p; }
 
+// Start of every kernel of a launch chain (phase, split and tiled modes).  The chain is launched
+// with programmatic stream serialization, so a kernel may be scheduled while its predecessor is
+// still finishing: griddepcontrol.wait blocks until the predecessor has completed and its writes
+// are visible, and no kernel touches memory before it.  launch_dependents then lets the next
+// kernel be scheduled once every block of this one has started, so its blocks take SM slots
+// during this kernel's tail instead of after it.  Launched without the attribute, both are no-ops.
+__device__ __forceinline__ void chain_begin() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Grid-wide barrier for a cooperative launch.  The wait is bounded: after
 // barrier_cycles SM clocks the block records a timeout, every later barrier returns false at
 // once, and the kernel unwinds.  Returns true when all blocks arrived.
@@ -1210,12 +1221,14 @@ template <> struct PhaseOcc<double> { static constexpr int flux = 3, grad = 4; }
 
 template <class R, int MODEL>
 __global__ void __launch_bounds__(PHASE_BLOCK, PhaseOcc<R>::grad) phase_grad_kernel(Dev<R> d, int stage) {
+  chain_begin();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   tile_sweep<R, MODEL, 0, true>(d, stage, reinterpret_cast<R*>(smem_raw));
 }
 
 template <class R, int MODEL, int FLUX>
 __global__ void __launch_bounds__(PHASE_BLOCK, PhaseOcc<R>::flux) phase_flux_kernel(Dev<R> d, int stage) {
+  chain_begin();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   tile_sweep<R, MODEL, FLUX, false>(d, stage, reinterpret_cast<R*>(smem_raw));
 }
@@ -1224,6 +1237,7 @@ __global__ void __launch_bounds__(PHASE_BLOCK, PhaseOcc<R>::flux) phase_flux_ker
 // from the control record; the first cell of each case records it.
 template <class R, int MODEL>
 __global__ void __launch_bounds__(MAX_BLOCK) phase_first_cells_kernel(Dev<R> d) {
+  chain_begin();
   const long long n = d.ncap;
   const int ncells = d.live_end[0];
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ncells; k += gridDim.x * blockDim.x) {
@@ -1260,6 +1274,7 @@ __global__ void __launch_bounds__(MAX_BLOCK) phase_first_cells_kernel(Dev<R> d) 
 // stage 1: SRD of U1, stage 2: of U2, stage 3: of the final candidate with the admissibility check.
 template <class R, int MODEL>
 __global__ void __launch_bounds__(MAX_BLOCK) phase_srd_kernel(Dev<R> d, int stage) {
+  chain_begin();
   for (int cs = blockIdx.x; cs < d.n_cases; cs += gridDim.x) {
     int cur;
     if (read_case_skip(d.ctl, cs, SKIP_STAGE, !d.cfg[cs].has_srd, &cur)) continue;
@@ -1270,6 +1285,7 @@ __global__ void __launch_bounds__(MAX_BLOCK) phase_srd_kernel(Dev<R> d, int stag
 
 // Accept/reject the trial (unless begin_only) and begin the next one, one thread per case.
 static __global__ void phase_commit_kernel(CaseCtl* ctl, int n_cases, int begin_only) {
+  chain_begin();
   const int cs = blockIdx.x * blockDim.x + threadIdx.x;
   if (cs >= n_cases) return;
   CaseCtl& c = ctl[cs];
@@ -1367,6 +1383,7 @@ __device__ __forceinline__ void load_item(const R* src, R* col, bool base, bool 
 
 template <class R, int MODEL>
 __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::cell) grad_cells_kernel(Dev<R> d, int stage) {
+  chain_begin();
   const int rule = stage_rule(stage);
   const int ncells = d.live_end[0];
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ncells; k += gridDim.x * blockDim.x) {
@@ -1392,6 +1409,7 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::cell) grad_cells_ker
 
 template <class R, int MODEL, int FLUX>
 __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::item) item_kernel(Dev<R> d, int stage) {
+  chain_begin();
   const int rule = stage_rule(stage);
   const bool base = stage == STAGE_BASE || stage == STAGE_DIAG;  // spectral columns wanted
   const int nf = d.live_end[1], total = nf + d.live_end[2];
@@ -1451,6 +1469,7 @@ template <class R, int MODEL> struct ItemSlots {
 
 template <class R, int MODEL>
 __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::gather) gather_kernel(Dev<R> d, int stage) {
+  chain_begin();
   const int rule = stage_rule(stage);
   const int ncells = d.live_end[0];
   const bool base = stage == STAGE_BASE;
@@ -1488,6 +1507,7 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::gather) gather_kerne
 
 template <class R, int MODEL>
 __global__ void __launch_bounds__(MAX_BLOCK) srd_rate_kernel(Dev<R> d, int store_only_case) {
+  chain_begin();
   for (int cs = blockIdx.x; cs < d.n_cases; cs += gridDim.x) {
     int cur;
     if (store_only_case >= 0) {
@@ -1538,6 +1558,7 @@ template <class R, int MODEL> struct TileSlots {
 
 template <class R, int MODEL, int FLUX>
 __global__ void __launch_bounds__(BT_THREADS, TiledOcc<R>::blocks) tiled_stage_kernel(Dev<R> d, int stage) {
+  chain_begin();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* cr = reinterpret_cast<R*>(smem_raw);  // BT_DATA x CREC
   R* fr = cr + BT_DATA * CREC;             // (BT_FACES + BT_WALLS) x SM_COLS

@@ -34,6 +34,23 @@ cudaError_t EngineOps<R>::launch(const Dev<R>& d, int model, int flux, bool srd,
   return cudaLaunchKernelExC(&cfg, kernel_for<R>(model, flux, srd), args);
 }
 
+// One kernel launch of a chain (see chain_begin): programmatic stream serialization lets the
+// kernel be scheduled during its predecessor's tail.  Errors surface through cudaGetLastError.
+template <class... P, class... A>
+static void chain(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 template <class R, int MODEL, int FLUX>
 static cudaError_t launch_phases_t(const Dev<R>& d, bool srd, int trials, int mode, int block, cudaStream_t st) {
   const int tiles = d.n_tiles > 0 ? (d.n_tiles + block / 32 - 1) / (block / 32) : 1;  // blocks of block/32 tile-warps
@@ -41,23 +58,23 @@ static cudaError_t launch_phases_t(const Dev<R>& d, bool srd, int trials, int mo
   const int cases = d.n_cases;
   const int cblocks = (cases + 127) / 128;
   if (mode == MODE_RESIDUAL) {
-    if (MODEL >= MODEL_LAMINAR) phase_grad_kernel<R, MODEL><<<tiles, block, sm, st>>>(d, STAGE_DIAG);
-    phase_flux_kernel<R, MODEL, FLUX><<<tiles, block, sm, st>>>(d, STAGE_DIAG);
+    if (MODEL >= MODEL_LAMINAR) chain(phase_grad_kernel<R, MODEL>, dim3(tiles), dim3(block), sm, st, d, STAGE_DIAG);
+    chain(phase_flux_kernel<R, MODEL, FLUX>, dim3(tiles), dim3(block), sm, st, d, STAGE_DIAG);
     return cudaGetLastError();
   }
-  phase_commit_kernel<<<cblocks, 128, 0, st>>>(d.ctl, cases, 1);
+  chain(phase_commit_kernel, dim3(cblocks), dim3(128), 0, st, d.ctl, cases, 1);
   for (int t = 0; t < trials; ++t) {
-    if (MODEL >= MODEL_LAMINAR) phase_grad_kernel<R, MODEL><<<tiles, block, sm, st>>>(d, STAGE_BASE);
-    phase_flux_kernel<R, MODEL, FLUX><<<tiles, block, sm, st>>>(d, STAGE_BASE);
-    if (srd && MODEL >= MODEL_LAMINAR && d.any_srd_rate) srd_rate_kernel<R, MODEL><<<cases, MAX_BLOCK, 0, st>>>(d, -1);
-    phase_first_cells_kernel<R, MODEL><<<(d.n_cells + 255) / 256 + 1, 256, 0, st>>>(d);
+    if (MODEL >= MODEL_LAMINAR) chain(phase_grad_kernel<R, MODEL>, dim3(tiles), dim3(block), sm, st, d, STAGE_BASE);
+    chain(phase_flux_kernel<R, MODEL, FLUX>, dim3(tiles), dim3(block), sm, st, d, STAGE_BASE);
+    if (srd && MODEL >= MODEL_LAMINAR && d.any_srd_rate) chain(srd_rate_kernel<R, MODEL>, dim3(cases), dim3(MAX_BLOCK), 0, st, d, -1);
+    chain(phase_first_cells_kernel<R, MODEL>, dim3((d.n_cells + 255) / 256 + 1), dim3(256), 0, st, d);
     for (int stage = 1; stage <= 2; ++stage) {
-      if (srd) phase_srd_kernel<R, MODEL><<<cases, block, 0, st>>>(d, stage);
-      if (MODEL >= MODEL_LAMINAR) phase_grad_kernel<R, MODEL><<<tiles, block, sm, st>>>(d, stage);
-      phase_flux_kernel<R, MODEL, FLUX><<<tiles, block, sm, st>>>(d, stage);
+      if (srd) chain(phase_srd_kernel<R, MODEL>, dim3(cases), dim3(block), 0, st, d, stage);
+      if (MODEL >= MODEL_LAMINAR) chain(phase_grad_kernel<R, MODEL>, dim3(tiles), dim3(block), sm, st, d, stage);
+      chain(phase_flux_kernel<R, MODEL, FLUX>, dim3(tiles), dim3(block), sm, st, d, stage);
     }
-    if (srd) phase_srd_kernel<R, MODEL><<<cases, block, 0, st>>>(d, 3);
-    phase_commit_kernel<<<cblocks, 128, 0, st>>>(d.ctl, cases, 0);
+    if (srd) chain(phase_srd_kernel<R, MODEL>, dim3(cases), dim3(block), 0, st, d, 3);
+    chain(phase_commit_kernel, dim3(cblocks), dim3(128), 0, st, d.ctl, cases, 0);
   }
   return cudaGetLastError();
 }
@@ -88,25 +105,25 @@ static cudaError_t launch_split_t(const Dev<R>& d, bool srd, int trials, int mod
   const int cases = d.n_cases;
   const int kblocks = (cases + 127) / 128;
   auto stage_seq = [&](int stage) {
-    if (MODEL >= MODEL_LAMINAR) grad_cells_kernel<R, MODEL><<<cblocks, B, 0, st>>>(d, stage);
-    item_kernel<R, MODEL, FLUX><<<iblocks, B, 0, st>>>(d, stage);
-    gather_kernel<R, MODEL><<<gblocks, B, 0, st>>>(d, stage);
+    if (MODEL >= MODEL_LAMINAR) chain(grad_cells_kernel<R, MODEL>, dim3(cblocks), dim3(B), 0, st, d, stage);
+    chain(item_kernel<R, MODEL, FLUX>, dim3(iblocks), dim3(B), 0, st, d, stage);
+    chain(gather_kernel<R, MODEL>, dim3(gblocks), dim3(B), 0, st, d, stage);
   };
   if (mode == MODE_RESIDUAL) {
     stage_seq(STAGE_DIAG);
     return cudaGetLastError();
   }
-  phase_commit_kernel<<<kblocks, 128, 0, st>>>(d.ctl, cases, 1);
+  chain(phase_commit_kernel, dim3(kblocks), dim3(128), 0, st, d.ctl, cases, 1);
   for (int t = 0; t < trials; ++t) {
     stage_seq(STAGE_BASE);
-    if (srd && MODEL >= MODEL_LAMINAR && d.any_srd_rate) srd_rate_kernel<R, MODEL><<<cases, MAX_BLOCK, 0, st>>>(d, -1);
-    phase_first_cells_kernel<R, MODEL><<<fblocks, 256, 0, st>>>(d);
+    if (srd && MODEL >= MODEL_LAMINAR && d.any_srd_rate) chain(srd_rate_kernel<R, MODEL>, dim3(cases), dim3(MAX_BLOCK), 0, st, d, -1);
+    chain(phase_first_cells_kernel<R, MODEL>, dim3(fblocks), dim3(256), 0, st, d);
     for (int stage = 1; stage <= 2; ++stage) {
-      if (srd) phase_srd_kernel<R, MODEL><<<cases, MAX_BLOCK, 0, st>>>(d, stage);
+      if (srd) chain(phase_srd_kernel<R, MODEL>, dim3(cases), dim3(MAX_BLOCK), 0, st, d, stage);
       stage_seq(stage);
     }
-    if (srd) phase_srd_kernel<R, MODEL><<<cases, MAX_BLOCK, 0, st>>>(d, 3);
-    phase_commit_kernel<<<kblocks, 128, 0, st>>>(d.ctl, cases, 0);
+    if (srd) chain(phase_srd_kernel<R, MODEL>, dim3(cases), dim3(MAX_BLOCK), 0, st, d, 3);
+    chain(phase_commit_kernel, dim3(kblocks), dim3(128), 0, st, d.ctl, cases, 0);
   }
   return cudaGetLastError();
 }
@@ -132,20 +149,20 @@ static cudaError_t launch_tiled_t(const Dev<R>& d, bool srd, int trials, int mod
   const int kblocks = (cases + 127) / 128;
   const int fblocks = (int)std::min<long long>((d.ncap + 255) / 256, (long long)sms * 8);
   if (mode == MODE_RESIDUAL) {
-    tiled_stage_kernel<R, MODEL, FLUX><<<grid, BT_THREADS, sm, st>>>(d, STAGE_DIAG);
+    chain(tiled_stage_kernel<R, MODEL, FLUX>, dim3(grid), dim3(BT_THREADS), sm, st, d, STAGE_DIAG);
     return cudaGetLastError();
   }
-  phase_commit_kernel<<<kblocks, 128, 0, st>>>(d.ctl, cases, 1);
+  chain(phase_commit_kernel, dim3(kblocks), dim3(128), 0, st, d.ctl, cases, 1);
   for (int t = 0; t < trials; ++t) {
-    tiled_stage_kernel<R, MODEL, FLUX><<<grid, BT_THREADS, sm, st>>>(d, STAGE_BASE);
-    if (srd && MODEL >= MODEL_LAMINAR && d.any_srd_rate) srd_rate_kernel<R, MODEL><<<cases, MAX_BLOCK, 0, st>>>(d, -1);
-    phase_first_cells_kernel<R, MODEL><<<fblocks, 256, 0, st>>>(d);
+    chain(tiled_stage_kernel<R, MODEL, FLUX>, dim3(grid), dim3(BT_THREADS), sm, st, d, STAGE_BASE);
+    if (srd && MODEL >= MODEL_LAMINAR && d.any_srd_rate) chain(srd_rate_kernel<R, MODEL>, dim3(cases), dim3(MAX_BLOCK), 0, st, d, -1);
+    chain(phase_first_cells_kernel<R, MODEL>, dim3(fblocks), dim3(256), 0, st, d);
     for (int stage = 1; stage <= 2; ++stage) {
-      if (srd) phase_srd_kernel<R, MODEL><<<cases, MAX_BLOCK, 0, st>>>(d, stage);
-      tiled_stage_kernel<R, MODEL, FLUX><<<grid, BT_THREADS, sm, st>>>(d, stage);
+      if (srd) chain(phase_srd_kernel<R, MODEL>, dim3(cases), dim3(MAX_BLOCK), 0, st, d, stage);
+      chain(tiled_stage_kernel<R, MODEL, FLUX>, dim3(grid), dim3(BT_THREADS), sm, st, d, stage);
     }
-    if (srd) phase_srd_kernel<R, MODEL><<<cases, MAX_BLOCK, 0, st>>>(d, 3);
-    phase_commit_kernel<<<kblocks, 128, 0, st>>>(d.ctl, cases, 0);
+    if (srd) chain(phase_srd_kernel<R, MODEL>, dim3(cases), dim3(MAX_BLOCK), 0, st, d, 3);
+    chain(phase_commit_kernel, dim3(kblocks), dim3(128), 0, st, d.ctl, cases, 0);
   }
   return cudaGetLastError();
 }
