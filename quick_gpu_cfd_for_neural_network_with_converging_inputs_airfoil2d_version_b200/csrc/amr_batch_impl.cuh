@@ -250,13 +250,16 @@ template <class R> class Batch final : public BatchBase {
       const uint64_t budget = c.hbm_bytes ? c.hbm_bytes : (uint64_t)4 << 30;
       cells = (long long)(budget / per_cell);
     }
+    const bool auto_faces = slots == 0;
     if (slots == 0) slots = 5 * cells;
     if (walls == 0) walls = cells / 8 + 64 * c.max_cases;
     if (terms == 0) terms = model_ == MODEL_EULER ? 1 : 6 * cells;
     if (srd == 0) srd = cells / 8 + 64 * c.max_cases;
     cap_cells_ = cells + c.max_cases;  // one closing entry per case
     cap_slots_ = slots;
-    cap_faces_ = slots;  // every face is listed by at least one cell
+    // every face is listed by at least one cell, so the slot count bounds the faces; a sized-from-
+    // cells arena assumes instead the ~2 faces per cell of 2-D quadtree meshes (2.5 with margin)
+    cap_faces_ = auto_faces ? std::min<long long>(slots, 5 * cells / 2 + 64ll * c.max_cases) : slots;
     cap_walls_ = walls;
     if (cap_faces_ >= (1ll << 30) || cap_walls_ >= (1ll << 30)) return fail(error, "arena too large for 32-bit record indices");
     cap_terms_ = std::max<long long>(terms, 1);
@@ -268,9 +271,11 @@ template <class R> class Batch final : public BatchBase {
     a_cells_ = RangeAlloc(cap_cells_);
     a_slots_ = RangeAlloc(cap_slots_);
     a_faces_ = RangeAlloc(cap_faces_);
-    cap_halo_ = 2 * cap_cells_;
-    cap_tface_ = 2 * cap_faces_ + 64;
-    cap_btiles_ = cap_cells_ / 16 + 4 * (long long)c.max_cases;
+    // block tiles serve only the tiled mode, which a batch reaches by asking for it or by autotuning
+    block_tiles_ = c.launch_mode == AMR_B200_LAUNCH_AUTO || c.launch_mode == AMR_B200_LAUNCH_TILED;
+    cap_halo_ = block_tiles_ ? 2 * cap_cells_ : 0;
+    cap_tface_ = block_tiles_ ? 2 * cap_faces_ + 64 : 0;
+    cap_btiles_ = block_tiles_ ? cap_cells_ / 16 + 4 * (long long)c.max_cases : 0;
     a_halo_ = RangeAlloc(cap_halo_);
     a_tface_ = RangeAlloc(cap_tface_);
     a_walls_ = RangeAlloc(cap_walls_);
@@ -317,12 +322,13 @@ template <class R> class Batch final : public BatchBase {
     ok = s_item_.alloc(cap_slots_, A, error, "slots") && f_case_.alloc(cap_faces_, A, error, "faces") &&
          f_own_.alloc(cap_faces_, A, error, "faces") && f_nb_.alloc(cap_faces_, A, error, "faces") &&
          f_meta_.alloc(cap_faces_, A, error, "faces") && f_len_.alloc(cap_faces_, A, error, "faces") &&
-         f_geo_.alloc(6 * cap_faces_, A, error, "faces") && fval_.alloc(SM_COLS * cap_faces_, A, error, "faces") &&
-         w_owner_.alloc(cap_walls_, A, error, "walls") && wval_.alloc(SM_COLS * cap_walls_, A, error, "walls") &&
+         f_geo_.alloc(6 * cap_faces_, A, error, "faces") && fval_.alloc(rec_stride() * cap_faces_, A, error, "faces") &&
+         w_owner_.alloc(cap_walls_, A, error, "walls") && wval_.alloc(rec_stride() * cap_walls_, A, error, "walls") &&
          live_end_.alloc(4, A, error, "ranges") && btiles_.alloc(cap_btiles_, A, error, "block tiles") &&
          bt_halo_.alloc(cap_halo_, A, error, "block tiles") && bt_face_.alloc(cap_tface_, A, error, "block tiles") &&
-         bt_floc_.alloc(cap_tface_, A, error, "block tiles") && s_loc_.alloc(cap_slots_, A, error, "slots") &&
-         w_ldon_.alloc(cap_walls_, A, error, "walls");
+         bt_floc_.alloc(cap_tface_, A, error, "block tiles") &&
+         s_loc_.alloc(block_tiles_ ? cap_slots_ : 0, A, error, "slots") &&
+         w_ldon_.alloc(block_tiles_ ? cap_walls_ : 0, A, error, "walls");
     if (!ok) return false;
     if (model_ >= MODEL_LAMINAR) {
       ok = crec_.alloc(CREC * nc, A, error, "scratch") && t_own_.alloc(cap_terms_, A, error, "terms") &&
@@ -358,8 +364,6 @@ template <class R> class Batch final : public BatchBase {
       return fail(error, "unknown launch mode");
     if (!cuda_ok(EngineOps<R>::tiled_setup(model_, flux_), error, "tiled kernel shared memory")) return false;
     mode_ = c.launch_mode == AMR_B200_LAUNCH_AUTO ? AMR_B200_LAUNCH_PERSISTENT : c.launch_mode;
-    // block tiles serve only the tiled mode, which a batch reaches by asking for it or by autotuning
-    block_tiles_ = c.launch_mode == AMR_B200_LAUNCH_AUTO || c.launch_mode == AMR_B200_LAUNCH_TILED;
     if (mode_ != AMR_B200_LAUNCH_PERSISTENT && block_ != PHASE_BLOCK)
       return fail(error, "the phase, split and tiled launch modes take block_threads 128");
     if (!configure_grid(error)) return false;
@@ -1706,6 +1710,11 @@ template <class R> class Batch final : public BatchBase {
     for (auto& c : cases_)
       if (c.live && c.cfg.srd_rate) return true;
     return false;
+  }
+
+  // values per stored face or wall record (the compact FP32 viscous format stores 8)
+  long long rec_stride() const {
+    return sizeof(R) == 4 && model_ >= MODEL_LAMINAR ? 8 : SM_COLS;
   }
 
   bool configure_grid(std::string* error) {
