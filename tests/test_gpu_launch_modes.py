@@ -151,3 +151,29 @@ def test_release_and_readmit_reuses_ranges(mode):
     fresh = run_batch([mix[2]], 64, 10, mode)
     assert np.array_equal(b.download(s), fresh[0])
 
+
+
+def test_fp32_laminar_split_close_to_phases_and_oracle():
+    """FP32 laminar model (AUSM+-up, Sutherland, outlet and reflecting sides, viscous wall model):
+    the split mode's compact records (net flux) stay within 1e-5 of the phase mode and within the
+    FP32 tolerance of the FP64 oracle."""
+    spec, mesh = built((0.04, 0.3, 0.1), profile='LF1', physics='laminar', law='sutherland', flux='ausm',
+                       kinds=('farfield', 'pressure-outlet', 'reflect', 'reflect'), mach=1.4, aoa=2.0)
+    params = spec.params()
+    u0 = cases.initial_state(mesh, spec.initial_primitive())
+    nsteps = 30
+    out = {}
+    for mode in ('split', 'phases'):
+        b = Batch(precision=32, model=_abi.MODEL_LAMINAR, sa=False, flux=_abi.FLUX_AUSMPUP, max_cases=2,
+                  max_cells=mesh.n_cells + 100, **MODES[mode])
+        s = b.admit(mesh, params, u0, case_control(1e30, nsteps, steady=False, mach=spec.mach, aoa=spec.aoa))
+        for _ in range(4):
+            b.advance(16)
+        st = b.status(s)
+        assert st['status'] == _abi.STATUS_MAXSTEPS and st['steps'] == nsteps, (mode, st)
+        assert mode in b.launch_config()
+        out[mode] = b.download(s)
+        b.destroy()
+    ref = Oracle(mesh, params).run(u0, 1e30, nsteps)
+    assert rel_err(out['split'], out['phases'], 4) <= 1e-5
+    assert rel_err(out['split'], ref['u'], 4) <= 2e-4
