@@ -197,6 +197,7 @@ def run_e2e(case_list, precision, steps, device=0, trials=32, block=0, grid=0, m
         u0 = cases.initial_state(mesh, spec.initial_primitive())
         items.append((mesh, spec.params(), u0, case_control(1e30, 10 ** 9, steady=False)))
         h2d += mesh_bytes(mesh, precision) + u0.nbytes * precision // 64
+    t_items = time.perf_counter()
     slots = b.admit_many(items)
     t_admit = time.perf_counter()
     adv, advances = 0, 0
@@ -218,7 +219,7 @@ def run_e2e(case_list, precision, steps, device=0, trials=32, block=0, grid=0, m
     b.destroy()
     return dict(value=cell_steps / seconds, seconds=seconds, h2d=h2d, d2h=d2h,
                 phases=dict(create=t_create - t0, admit=t_admit - t_create, advance=t_advance - t_admit,
-                            download=t_end - t_advance))
+                            download=t_end - t_advance, admit_host_inputs=t_items - t_create))
 
 
 def mesh_bytes(mesh, precision):
