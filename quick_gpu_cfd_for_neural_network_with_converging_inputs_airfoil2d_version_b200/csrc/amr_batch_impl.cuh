@@ -273,6 +273,9 @@ template <class R> class Batch final : public BatchBase {
     a_faces_ = RangeAlloc(cap_faces_);
     // block tiles serve only the tiled mode, which a batch reaches by asking for it or by autotuning
     block_tiles_ = c.launch_mode == AMR_B200_LAUNCH_AUTO || c.launch_mode == AMR_B200_LAUNCH_TILED;
+    // per-slot owner and geometry serve only the persistent and phase modes
+    slot_fluxes_ = c.launch_mode == AMR_B200_LAUNCH_AUTO || c.launch_mode == AMR_B200_LAUNCH_PERSISTENT ||
+                   c.launch_mode == AMR_B200_LAUNCH_PHASES;
     cap_halo_ = block_tiles_ ? 2 * cap_cells_ : 0;
     cap_tface_ = block_tiles_ ? 2 * cap_faces_ + 64 : 0;
     cap_btiles_ = block_tiles_ ? cap_cells_ / 16 + 4 * (long long)c.max_cases : 0;
@@ -300,7 +303,7 @@ template <class R> class Batch final : public BatchBase {
               c_flags_.alloc(nc, A, error, "cells") && c_slot_.alloc(nc, A, error, "cells") &&
               c_wall_.alloc(nc, A, error, "cells") && c_term_.alloc(nc, A, error, "cells") &&
               c_cx_.alloc(nc, A, error, "cells") && c_cy_.alloc(nc, A, error, "cells") &&
-              s_own_.alloc(cap_slots_, A, error, "slots") && s_nb_.alloc(cap_slots_, A, error, "slots") &&
+              s_own_.alloc(slot_fluxes_ ? cap_slots_ : 0, A, error, "slots") && s_nb_.alloc(cap_slots_, A, error, "slots") &&
               s_meta_.alloc(cap_slots_, A, error, "slots") && s_len_.alloc(cap_slots_, A, error, "slots") &&
               w_nx_.alloc(cap_walls_, A, error, "walls") && w_ny_.alloc(cap_walls_, A, error, "walls") &&
               w_len_.alloc(cap_walls_, A, error, "walls") && w_dist_.alloc(cap_walls_, A, error, "walls") &&
@@ -317,7 +320,7 @@ template <class R> class Batch final : public BatchBase {
               diag_cfg_.alloc(7 * c.max_cases, A, error, "diag") && case_tiles_.alloc(2 * c.max_cases, A, error, "diag") &&
               ddt_.alloc(2 * nc, A, error, "diag");
     if (!ok) return false;
-    if (!s_geo_.alloc(6 * cap_slots_, A, error, "slots")) return false;
+    if (!s_geo_.alloc(slot_fluxes_ ? 6 * cap_slots_ : 0, A, error, "slots")) return false;
     // face and wall records of the split launch mode
     ok = s_item_.alloc(cap_slots_, A, error, "slots") && f_case_.alloc(cap_faces_, A, error, "faces") &&
          f_own_.alloc(cap_faces_, A, error, "faces") && f_nb_.alloc(cap_faces_, A, error, "faces") &&
@@ -525,9 +528,9 @@ template <class R> class Batch final : public BatchBase {
   // grain), which sizes the staging arena; a larger case only takes a slower overflow path.
   size_t staged_bytes(size_t n, size_t nw, size_t ns, size_t nt, size_t nf, size_t ng, size_t gm, size_t ql,
                       size_t halo, size_t tface, bool tiles) const {
-    const size_t r = sizeof(R), n1 = n + 1, g1 = ng + 1, tl = tiles ? 1 : 0;
+    const size_t r = sizeof(R), n1 = n + 1, g1 = ng + 1, tl = tiles ? 1 : 0, sl = slot_fluxes_ ? 1 : 0;
     const size_t tables[] = {4 * n1, 4 * n1, 4 * n1, 4 * n1, 8 * n1, 8 * n1, 8 * n1, 8 * n1, 8 * n1, n1,
-                             model_ == MODEL_SA ? r * n1 : 0, 4 * ns, 4 * ns, 4 * ns, 4 * ns, r * ns, 6 * r * ns,
+                             model_ == MODEL_SA ? r * n1 : 0, 4 * ns * sl, 4 * ns, 4 * ns, 4 * ns, r * ns, 6 * r * ns * sl,
                              r * nw, r * nw, r * nw, r * nw, 8 * nw, 8 * nw, 4 * nw, 4 * nw, 4 * nt, 4 * nt, r * nt,
                              r * nt, 4 * nf, 4 * nf, 4 * nf, 4 * nf, r * nf, 6 * r * nf, 4 * halo, 4 * tface,
                              8 * tface, 4 * ns * tl, 4 * nw * tl, 4 * g1, 4 * gm, 4 * g1, 4 * g1, 4 * ql, 8 * gm, 8 * g1, 8 * g1,
@@ -810,8 +813,11 @@ template <class R> class Batch final : public BatchBase {
     c_flags[n] = 0;
     PVec<R> c_wd = pvu<R>(S, model_ == MODEL_SA ? n + 1 : 0);
     if (model_ == MODEL_SA) c_wd[n] = R(1);
-    PVec<int> s_own = pvu<int>(S, ns), s_nb = pvu<int>(S, ns), s_meta = pvu<int>(S, ns), s_item = pvu<int>(S, ns);
-    PVec<R> s_len = pvu<R>(S, ns), s_geo = pv<R>(S, 6 * ns, R(0));
+    // owner and geometry per slot serve only the per-slot flux modes (persistent, phases)
+    const bool sf = slot_fluxes_;
+    PVec<int> s_own = pvu<int>(S, sf ? ns : 0), s_nb = pvu<int>(S, ns), s_meta = pvu<int>(S, ns),
+              s_item = pvu<int>(S, ns);
+    PVec<R> s_len = pvu<R>(S, ns), s_geo = pv<R>(S, sf ? 6 * ns : 0, R(0));
     PVec<R> w_nx = pvu<R>(S, nw), w_ny = pvu<R>(S, nw), w_len = pvu<R>(S, nw), w_dist = pv<R>(S, nw, R(1));
     PVec<double> w_xm = pvu<double>(S, nw), w_ym = pvu<double>(S, nw);
     PVec<int> w_donor = pv<int>(S, nw, cb), w_owner = pvu<int>(S, nw);
@@ -838,12 +844,12 @@ template <class R> class Batch final : public BatchBase {
         const int other = own_left ? f.right : f.left;
         const int side = f.boundary;
         const int kind = side >= 0 ? kinds[side] : 0;
-        s_own[spos] = cb + (int)k;
+        if (sf) s_own[spos] = cb + (int)k;
         s_nb[spos] = other >= 0 ? cb + other : -1;
         s_meta[spos] = (own_left ? 1 : 0) | ((f.axis & 1) << 1) | ((side + 1) << 2) | ((kind & 15) << 5);
         s_len[spos] = (R)f.length;
         s_item[spos] = 2 * (fb + rec[fi]) + (own_left ? 1 : 0);  // record index and orientation
-        if (viscous) {
+        if (viscous && sf) {
           const amr_face_geometry_t& g = m->face_geometry[fi];
           R* geo = &s_geo[6 * spos];
           geo[0] = (R)g.dx;
@@ -862,21 +868,23 @@ template <class R> class Batch final : public BatchBase {
         w_len[wpos] = (R)w.length;
         w_xm[wpos] = (w.x0 + w.x1) * .5;
         w_ym[wpos] = (w.y0 + w.y1) * .5;
-        s_own[spos] = cb + (int)k;
+        if (sf) s_own[spos] = cb + (int)k;
         s_nb[spos] = -1;
         s_meta[spos] = SLOT_WALL;
         s_len[spos] = (R)w.length;
         s_item[spos] = wb + (int)wpos;
         w_owner[wpos] = cb + (int)k;
-        s_geo[6 * spos + 0] = (R)w.nx;
-        s_geo[6 * spos + 1] = (R)w.ny;
-        s_geo[6 * spos + 2] = R(1);
+        if (sf) {
+          s_geo[6 * spos + 0] = (R)w.nx;
+          s_geo[6 * spos + 1] = (R)w.ny;
+          s_geo[6 * spos + 2] = R(1);
+        }
         if (viscous) {
           const amr_wall_sample_t& smp = m->wall_samples[q];
           w_donor[wpos] = cb + smp.donor;
           w_dist[wpos] = (R)smp.distance;
           s_nb[spos] = cb + smp.donor;
-          s_geo[6 * spos + 2] = (R)smp.distance;
+          if (sf) s_geo[6 * spos + 2] = (R)smp.distance;
         }
       }
       if (viscous)
@@ -1892,6 +1900,7 @@ template <class R> class Batch final : public BatchBase {
   std::vector<char> reserved_;                     // slots reserved by an admission in progress
   long long pending_tiles_ = 0, pending_btiles_ = 0;
   bool block_tiles_ = true;  // cases carry block tiles (the batch may run the tiled mode)
+  bool slot_fluxes_ = true;  // slots carry owner and geometry (the batch may run a per-slot mode)
 };
 
 }  // namespace amrb

@@ -323,6 +323,8 @@ template <class R> int Batch<R>::autotune(int trials, std::string* error) {
   // (direct launches would penalise the multi-kernel modes by their host launch cost)
   for (int mode : {AMR_B200_LAUNCH_PERSISTENT, AMR_B200_LAUNCH_PHASES, AMR_B200_LAUNCH_SPLIT, AMR_B200_LAUNCH_TILED}) {
     if (mode == AMR_B200_LAUNCH_TILED && !block_tiles_) continue;  // the cases carry no block tiles
+    if ((mode == AMR_B200_LAUNCH_PERSISTENT || mode == AMR_B200_LAUNCH_PHASES) && !slot_fluxes_)
+      continue;  // the slots carry no owner or geometry
     for (int block : {128, 256}) {
       if (mode != AMR_B200_LAUNCH_PERSISTENT && block != PHASE_BLOCK) continue;
       mode_ = mode;
