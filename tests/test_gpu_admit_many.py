@@ -73,3 +73,27 @@ def test_bulk_reports_invalid_and_full_entries():
     alone = run([items[2]], 32, 'split', 1, 2, bulk=False)[1][0]
     assert np.array_equal(b.download(1), alone)
     b.destroy()
+
+
+def test_bulk_euler_srd_fp64_equals_sequential(golden):
+    """Non-trivial SRD neighbourhoods (Euler, no agglomeration) prepared on several threads: the
+    bulk admission computes bit for bit what one-by-one admissions compute."""
+    from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200.mesh import MeshArrays
+    from tests.test_gpu_launch_modes import built
+    mix = [(cases.CaseSpec(physics='euler', profile='LF1', mach=1.65, aoa=1.5),
+            MeshArrays.load(golden / 'mesh_naca0012_lf1_euler_srd.npz'))]
+    mix.append(built((0.02, 0.4, 0.12), profile='LF1', physics='euler', mach=1.8, aoa=3.0))
+    assert all(m.small_cells for _, m in mix)
+    items = items_of(mix + mix[:1], 20)
+    out = []
+    for bulk in (False, True):
+        b = Batch(precision=64, model=_abi.MODEL_EULER, sa=False, max_cases=4,
+                  max_cells=sum(m.n_cells for m, _, _, _ in items) + 100, **MODES['split'])
+        slots = b.admit_many(items, threads=3) if bulk else [b.admit(*it) for it in items]
+        for _ in range(2):
+            b.advance(16)
+        out.append((slots, [b.status(s)['steps'] for s in slots], [b.download(s) for s in slots]))
+        b.destroy()
+    assert out[0][0] == out[1][0] and out[0][1] == out[1][1] == [20] * 3
+    for a, c in zip(out[0][2], out[1][2]):
+        assert np.array_equal(a, c)
