@@ -1065,6 +1065,10 @@ template <class R> class Batch final : public BatchBase {
                      &j.error, "control upload"))
           j.status = 1;
       }
+    // a case that failed after its fill began may have written its ranges' owner markers: mark
+    // them free again (as release does), so no later case inherits those cells, faces or walls
+    for (AdmitJob& j : jobs)
+      if (j.status != 0 && j.reserved) unmark_ranges(j.hc);
     std::string err;
     const bool synced = cuda_ok(cudaStreamSynchronize(stream_), &err, "admit sync");
     for (std::unique_ptr<Stager>& s : stagers_) {
@@ -1104,9 +1108,7 @@ template <class R> class Batch final : public BatchBase {
     cudaMemcpyAsync(ctl_.p + slot, &h_ctl_[slot], sizeof(CaseCtl), cudaMemcpyHostToDevice, stream_);
     // the freed cell range no longer belongs to any case
     HostCase<R>& hc = cases_[slot];
-    cudaMemsetAsync(c_case_.p + hc.cells.b, 0xff, sizeof(int) * hc.cells.n, stream_);
-    if (hc.faces.n) cudaMemsetAsync(f_case_.p + hc.faces.b, 0xff, sizeof(int) * hc.faces.n, stream_);
-    if (hc.walls.n) cudaMemsetAsync(w_owner_.p + hc.walls.b, 0xff, sizeof(int) * hc.walls.n, stream_);
+    unmark_ranges(hc);
     cudaStreamSynchronize(stream_);
     release_ranges(hc);
     hc = HostCase<R>();
@@ -1532,6 +1534,13 @@ template <class R> class Batch final : public BatchBase {
     for (auto& c : cases_)
       if (c.live) s += (long long)c.tiles.size();
     return s;
+  }
+
+  // Marks a case's cells, faces and walls as belonging to no case (asynchronous on stream_).
+  void unmark_ranges(const HostCase<R>& hc) {
+    if (hc.cells.n) cudaMemsetAsync(c_case_.p + hc.cells.b, 0xff, sizeof(int) * hc.cells.n, stream_);
+    if (hc.faces.n) cudaMemsetAsync(f_case_.p + hc.faces.b, 0xff, sizeof(int) * hc.faces.n, stream_);
+    if (hc.walls.n) cudaMemsetAsync(w_owner_.p + hc.walls.b, 0xff, sizeof(int) * hc.walls.n, stream_);
   }
 
   void release_ranges(HostCase<R>& hc) {
