@@ -97,3 +97,27 @@ def test_bulk_euler_srd_fp64_equals_sequential(golden):
     assert out[0][0] == out[1][0] and out[0][1] == out[1][1] == [20] * 3
     for a, c in zip(out[0][2], out[1][2]):
         assert np.array_equal(a, c)
+
+
+def test_bulk_no_room_by_cells_and_readmit_into_freed_ranges():
+    """A batch with cells for two of three cases: the third entry finds no room (3) while the
+    others are admitted; after a release, a bulk re-admission reuses the freed ranges and computes
+    exactly what the case computes alone.  An empty request list admits nothing."""
+    mix = sa_mix()
+    items = items_of(mix, 8)
+    cells = sorted(m.n_cells for m, _, _, _ in items)
+    b = Batch(precision=32, model=_abi.MODEL_LAMINAR, sa=True, max_cases=4,
+              max_cells=cells[1] + cells[2] + 8, **MODES['split'])
+    assert b.admit_many([]) == []
+    big_two = sorted(range(3), key=lambda i: items[i][0].n_cells)[1:]
+    small = min(range(3), key=lambda i: items[i][0].n_cells)
+    first = b.admit_many([items[i] for i in big_two] + [items[small]], threads=2)
+    assert first[:2] == [0, 1] and first[2] is None
+    b.release(first[0])
+    again = b.admit_many([items[small]], threads=2)
+    assert again == [0]
+    for _ in range(2):
+        b.advance(16)
+    alone = run([items[small]], 32, 'split', 1, 1, bulk=False)[1][0]
+    assert np.array_equal(b.download(0), alone)
+    b.destroy()
