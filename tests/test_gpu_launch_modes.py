@@ -177,3 +177,34 @@ def test_fp32_laminar_split_close_to_phases_and_oracle():
     ref = Oracle(mesh, params).run(u0, 1e30, nsteps)
     assert rel_err(out['split'], out['phases'], 4) <= 1e-5
     assert rel_err(out['split'], ref['u'], 4) <= 2e-4
+
+
+def test_fp32_euler_srd_split_alone_in_mix_and_close_to_phases_and_oracle(golden):
+    """FP32 Euler with non-trivial SRD neighbourhoods: the split mode is bit-identical alone and
+    beside another case, within 1e-5 of the phase mode and within the FP32 tolerance of the FP64
+    oracle."""
+    spec = cases.CaseSpec(physics='euler', profile='LF1', mach=1.65, aoa=1.5)
+    mesh = MeshArrays.load(golden / 'mesh_naca0012_lf1_euler_srd.npz')
+    other = built((0.02, 0.4, 0.12), profile='LF1', physics='euler', mach=1.8, aoa=3.0)
+    params = spec.params()
+    nsteps = 40
+
+    def run(mode, with_other):
+        items = [(spec, mesh)] + ([other] if with_other else [])
+        b = Batch(precision=32, model=_abi.MODEL_EULER, sa=False, max_cases=2,
+                  max_cells=sum(m.n_cells for _, m in items) + 100, **MODES[mode])
+        slots = [b.admit(m, s.params(), cases.initial_state(m, s.initial_primitive()),
+                         case_control(1e30, nsteps, steady=False, mach=s.mach, aoa=s.aoa)) for s, m in items]
+        for _ in range(4):
+            b.advance(16)
+        st = b.status(slots[0])
+        assert st['status'] == _abi.STATUS_MAXSTEPS and st['steps'] == nsteps, (mode, st)
+        u = b.download(slots[0])
+        b.destroy()
+        return u
+
+    alone = run('split', False)
+    assert np.array_equal(alone, run('split', True))
+    ref = Oracle(mesh, params).run(cases.initial_state(mesh, spec.initial_primitive()), 1e30, nsteps)
+    assert rel_err(alone, run('phases', False), 4) <= 1e-5
+    assert rel_err(alone, ref['u'], 4) <= 2e-4
