@@ -97,6 +97,7 @@ template <class R> struct Dev {
   const CaseCfg<R>* cfg;
   const Tile* tiles;
   int n_tiles, n_cases;
+  int fused_first;  // split mode: stage 1 reads U + dt R0 in place of a stored first update
   // cells
   const int* c_case;
   const double* c_vol;
@@ -243,7 +244,8 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* b, unsigned long long 
 
 template <class R> struct Prim { R rho, u, v, p; };
 
-template <class R> __device__ __forceinline__ Prim<R> prim(const R* U, long long n, int k, R g) {
+// U: the state's SoA array, or any object whose [i] yields entry i of such an array (FusedIn).
+template <class R, class In> __device__ __forceinline__ Prim<R> prim(const In& U, long long n, int k, R g) {
   Prim<R> w;
   const R rho = U[k], mx = U[n + k], my = U[2 * n + k], e = U[3 * n + k];
   w.rho = rho;
@@ -253,10 +255,20 @@ template <class R> __device__ __forceinline__ Prim<R> prim(const R* U, long long
   return w;
 }
 
-template <class R> __device__ __forceinline__ bool prim_ok(const R* U, long long n, int k, const Prim<R>& w) {
+template <class R, class In> __device__ __forceinline__ bool prim_ok(const In& U, long long n, int k, const Prim<R>& w) {
   const R mx = U[n + k], my = U[2 * n + k], e = U[3 * n + k];
   return isfinite(w.rho) && w.rho > R(0) && isfinite(mx) && isfinite(my) && isfinite(e) && isfinite(w.p) && w.p > R(0);
 }
+
+// The first stage's input U1 = U + dt R0, formed where it is read (split mode, viscous models
+// without SRD, whose first update has no other effect), with the expression the first-update
+// kernel stores.
+template <class R> struct FusedIn {
+  const R* U;
+  const R* R0;
+  R dt;
+  __device__ __forceinline__ R operator[](long long i) const { return U[i] + dt * R0[i]; }
+};
 
 __device__ __forceinline__ void atomic_min_dt(unsigned long long* slot, double v) {
   atomicMin(slot, (unsigned long long)__double_as_longlong(v));
@@ -342,8 +354,8 @@ template <class R, int MODEL> __device__ __forceinline__ void load_cell_record(c
 // With soa the per-cell fields go to the SoA scratch arrays; with rec (split mode) they also go
 // to the cell's packed record: state 0-4, gradient 5-8, mu 9, eddy 10, SA phi gradient 11-12,
 // SA diffusion 13.
-template <class R, int MODEL>
-__device__ __forceinline__ bool grad_finish(const Dev<R>& d, const CaseCfg<R>& cf, int k, const R* Uin, const R* gr,
+template <class R, int MODEL, class In>
+__device__ __forceinline__ bool grad_finish(const Dev<R>& d, const CaseCfg<R>& cf, int k, const In& Uin, const R* gr,
                                             const R* sg, bool soa = true, R* rec = nullptr, bool src_out = true) {
   const long long n = d.ncap;
   const Prim<R> w = prim(Uin, n, k, cf.gamma);
@@ -391,8 +403,8 @@ __device__ __forceinline__ bool grad_finish(const Dev<R>& d, const CaseCfg<R>& c
 
 // LSQ contribution of one gradient term of cell k (reference src/static_amr2d_viscous.cpp:170-173,
 // src/static_amr2d_sa.cpp:75-76): c[0..3] velocity, c[4..7] SA phi and density.
-template <class R, int MODEL>
-__device__ __forceinline__ void term_values(const Dev<R>& d, const CaseCfg<R>& cf, int q, int k, const R* Uin, R* c) {
+template <class R, int MODEL, class In>
+__device__ __forceinline__ void term_values(const Dev<R>& d, const CaseCfg<R>& cf, int q, int k, const In& Uin, R* c) {
   const long long n = d.ncap;
   const int src = __ldg(d.t_src + q);
   const R x = __ldg(d.t_x + q), y = __ldg(d.t_y + q);
@@ -725,9 +737,9 @@ template <class R> struct Cols {
 // Per-cell end of the F phase: in-order sums of the cell's slot values (faces [a, e) in CSR order,
 // then walls [e, b)), residual, cell dt (base stage) and the stage update.  get(q, col) yields
 // the 12 values of slot q with the flux columns signed for cell k.  Returns the cell dt.
-template <class R, int MODEL, class Get>
+template <class R, int MODEL, class Get, class In>
 __device__ __forceinline__ double finish_cell(const Dev<R>& d, const CaseCfg<R>& cf, int cs, int k, int stage, int a,
-                                              int e, int b, const Get& get, const R* Uin, R* Ub, R* Un, bool& bad) {
+                                              int e, int b, const Get& get, const In& Uin, R* Ub, R* Un, bool& bad) {
   const long long n = d.ncap;
   const R g = cf.gamma;
   const bool base = stage == STAGE_BASE;
@@ -1271,6 +1283,26 @@ __global__ void __launch_bounds__(MAX_BLOCK) phase_first_cells_kernel(Dev<R> d) 
   }
 }
 
+// The first update's control part alone, one thread per case (split mode with fused_first: the
+// state part, U1 = U + dt R0, is formed where the stage-1 kernels read it).  Same decisions as
+// phase_first_cells_kernel makes at a case's first cell.
+template <class R>
+__global__ void __launch_bounds__(128) dt_cases_kernel(Dev<R> d) {
+  chain_begin();
+  const int cs = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cs >= d.n_cases) return;
+  const CaseCtl& c = d.ctl[cs];
+  if (!c.live || !c.active) return;
+  double dt;
+  int fatal;
+  if (choose_dt(c, d.cfg[cs].dt_fixed, &dt, &fatal)) {
+    d.ctl[cs].dt_trial = dt;
+    if (!c.retrying) d.ctl[cs].attempt = 0;
+  } else {
+    d.ctl[cs].fatal = fatal;
+  }
+}
+
 // stage 1: SRD of U1, stage 2: of U2, stage 3: of the final candidate with the admissibility check.
 template <class R, int MODEL>
 __global__ void __launch_bounds__(MAX_BLOCK) phase_srd_kernel(Dev<R> d, int stage) {
@@ -1392,18 +1424,22 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::cell) grad_cells_ker
     const CaseCtl& c = d.ctl[cs];
     if (skip_case(c, rule)) continue;
     const CaseCfg<R>& cf = d.cfg[cs];
-    const R* Uin = stage_input(d, stage, c.cur);
-    R gr[4] = {0, 0, 0, 0}, sg[4] = {0, 0, 0, 0};
-    for (int q = d.c_term[k]; q < d.c_term[k + 1]; ++q) {
-      R t[8];
-      term_values<R, MODEL>(d, cf, q, k, Uin, t);
-      for (int v = 0; v < 4; ++v) gr[v] += t[v];
-      if (MODEL == MODEL_SA)
-        for (int v = 0; v < 4; ++v) sg[v] += t[4 + v];
-    }
-    // the packed record feeds the item kernel; the SoA copies only the residual-mode loads
-    if (!grad_finish<R, MODEL>(d, cf, k, Uin, gr, sg, stage == STAGE_DIAG, d.crec + CREC * (long long)k))
-      atomicOr(&d.ctl[cs].bad, 1);
+    const auto cell = [&](const auto& Uin) {
+      R gr[4] = {0, 0, 0, 0}, sg[4] = {0, 0, 0, 0};
+      for (int q = d.c_term[k]; q < d.c_term[k + 1]; ++q) {
+        R t[8];
+        term_values<R, MODEL>(d, cf, q, k, Uin, t);
+        for (int v = 0; v < 4; ++v) gr[v] += t[v];
+        if (MODEL == MODEL_SA)
+          for (int v = 0; v < 4; ++v) sg[v] += t[4 + v];
+      }
+      // the packed record feeds the item kernel; the SoA copies only the residual-mode loads
+      return grad_finish<R, MODEL>(d, cf, k, Uin, gr, sg, stage == STAGE_DIAG, d.crec + CREC * (long long)k);
+    };
+    const bool ok = d.fused_first && stage == STAGE_1
+                        ? cell(FusedIn<R>{state_buf(d, c.cur), d.R0, (R)c.dt_trial})
+                        : cell(stage_input(d, stage, c.cur));
+    if (!ok) atomicOr(&d.ctl[cs].bad, 1);
   }
 }
 
@@ -1485,9 +1521,14 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::gather) gather_kerne
       const CaseCtl& c = d.ctl[cs];
       const int a = d.c_slot[k], b = d.c_slot[k + 1];
       const int e = b - (d.c_wall[k + 1] - d.c_wall[k]);
-      cell_dt = finish_cell<R, MODEL>(d, d.cfg[cs], cs, k, stage, a, e, b,
-                                      ItemSlots<R, MODEL>{&d, base || stage == STAGE_DIAG},
-                                      stage_input(d, stage, c.cur), state_buf(d, c.cur), state_buf(d, c.cur ^ 1), bad);
+      const ItemSlots<R, MODEL> get{&d, base || stage == STAGE_DIAG};
+      if (d.fused_first && stage == STAGE_1)
+        cell_dt = finish_cell<R, MODEL>(d, d.cfg[cs], cs, k, stage, a, e, b, get,
+                                        FusedIn<R>{state_buf(d, c.cur), d.R0, (R)c.dt_trial}, state_buf(d, c.cur),
+                                        state_buf(d, c.cur ^ 1), bad);
+      else
+        cell_dt = finish_cell<R, MODEL>(d, d.cfg[cs], cs, k, stage, a, e, b, get, stage_input(d, stage, c.cur),
+                                        state_buf(d, c.cur), state_buf(d, c.cur ^ 1), bad);
       if (bad && stage != STAGE_DIAG) atomicOr(&d.ctl[cs].bad, 1);
     }
     if (base) {

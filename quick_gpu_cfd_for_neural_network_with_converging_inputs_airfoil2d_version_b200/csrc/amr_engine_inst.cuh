@@ -104,10 +104,16 @@ static cudaError_t launch_split_t(const Dev<R>& d, bool srd, int trials, int mod
   const int fblocks = (int)std::min<long long>((ncap + 255) / 256, (long long)sms * 8);
   const int cases = d.n_cases;
   const int kblocks = (cases + 127) / 128;
+  // Viscous models without SRD: the first update only adds dt R0, so the stage-1 kernels form
+  // U1 where they read it and one thread per case makes the update's control decisions.
+  // (Euler reads U1 in the face kernel; SRD changes U1 between the update and stage 1.)
+  const bool fused = MODEL >= MODEL_LAMINAR && !srd;
+  Dev<R> dd = d;
+  dd.fused_first = fused ? 1 : 0;
   auto stage_seq = [&](int stage) {
-    if (MODEL >= MODEL_LAMINAR) chain(grad_cells_kernel<R, MODEL>, dim3(cblocks), dim3(B), 0, st, d, stage);
-    chain(item_kernel<R, MODEL, FLUX>, dim3(iblocks), dim3(B), 0, st, d, stage);
-    chain(gather_kernel<R, MODEL>, dim3(gblocks), dim3(B), 0, st, d, stage);
+    if (MODEL >= MODEL_LAMINAR) chain(grad_cells_kernel<R, MODEL>, dim3(cblocks), dim3(B), 0, st, dd, stage);
+    chain(item_kernel<R, MODEL, FLUX>, dim3(iblocks), dim3(B), 0, st, dd, stage);
+    chain(gather_kernel<R, MODEL>, dim3(gblocks), dim3(B), 0, st, dd, stage);
   };
   if (mode == MODE_RESIDUAL) {
     stage_seq(STAGE_DIAG);
@@ -117,7 +123,10 @@ static cudaError_t launch_split_t(const Dev<R>& d, bool srd, int trials, int mod
   for (int t = 0; t < trials; ++t) {
     stage_seq(STAGE_BASE);
     if (srd && MODEL >= MODEL_LAMINAR && d.any_srd_rate) chain(srd_rate_kernel<R, MODEL>, dim3(cases), dim3(MAX_BLOCK), 0, st, d, -1);
-    chain(phase_first_cells_kernel<R, MODEL>, dim3(fblocks), dim3(256), 0, st, d);
+    if (fused)
+      chain(dt_cases_kernel<R>, dim3(kblocks), dim3(128), 0, st, d);
+    else
+      chain(phase_first_cells_kernel<R, MODEL>, dim3(fblocks), dim3(256), 0, st, d);
     for (int stage = 1; stage <= 2; ++stage) {
       if (srd) chain(phase_srd_kernel<R, MODEL>, dim3(cases), dim3(MAX_BLOCK), 0, st, d, stage);
       stage_seq(stage);
