@@ -38,7 +38,7 @@ SOLVE_STEPS = 5000  # steps per solve of the batched workload
 # DRAM bytes (read + write) of one split-mode trial of the 256-case workload, summed over its
 # kernels from one ncu capture (profiles/split_trial_f32_sa_256cases.md; cold cache, so an upper
 # bound of a warm trial).  Reported as roofline.traffic when the run matches that configuration.
-SPLIT_256_TRAFFIC_PER_STEP = 3.1200e9
+SPLIT_256_TRAFFIC_PER_STEP = 2.7783e9
 
 
 def peaks():
