@@ -208,3 +208,30 @@ def test_fp32_euler_srd_split_alone_in_mix_and_close_to_phases_and_oracle(golden
     ref = Oracle(mesh, params).run(cases.initial_state(mesh, spec.initial_primitive()), 1e30, nsteps)
     assert rel_err(alone, run('phases', False), 4) <= 1e-5
     assert rel_err(alone, ref['u'], 4) <= 2e-4
+
+
+def test_split_first_update_in_place_rejections_and_fatal_match_oracle(golden):
+    """Split mode, SA without SRD (the stage-1 kernels form U1 = U + dt R0 in place): an oversize
+    fixed dt is halved and retried exactly as on the CPU; 21 rejections end with status 5 and a
+    dt underflow with status 4, the accepted state kept."""
+    mesh = MeshArrays.load(golden / 'mesh_naca2412_lf1_sa.npz')
+    assert not mesh.small_cells
+    opts = default_options(**MODES['split'])
+    spec = cases.CaseSpec(physics='sa', profile='LF1', mach=1.65, aoa=1.5, dt_fixed=0.02)
+    u0 = cases.initial_state(mesh, spec.initial_primitive())
+    ref = Oracle(mesh, spec.params()).run(u0, 1e30, 6)
+    s = StaticAmrGpu.create(mesh, spec.params(), u0, options=opts)
+    assert s.advance(1e30, 6) == 1 and 'status 3' in s.last_error
+    assert 'split' in s.launch_config()
+    assert (s.steps, s.rejected, s.time) == (ref['steps'], ref['rejected'], ref['time']) and ref['rejected'] > 0
+    assert rel_err(s.download(), ref['u'], mesh.nv) <= TOL
+    spec5 = cases.CaseSpec(physics='sa', profile='LF1', mach=1.65, aoa=1.5, dt_fixed=1e10)
+    ref5 = Oracle(mesh, spec5.params()).run(u0, 1e12, 5)
+    assert 'after 21 trials' in ref5['error']
+    s = StaticAmrGpu.create(mesh, spec5.params(), u0, options=opts)
+    assert s.advance(1e12, 5) == 1 and 'status 5' in s.last_error
+    assert s.rejected == ref5['rejected'] == 21 and np.array_equal(s.download(), u0)
+    spec4 = cases.CaseSpec(physics='sa', profile='LF1', mach=1.65, aoa=1.5, dt_fixed=1e-300)
+    s = StaticAmrGpu.create(mesh, spec4.params(), u0, time=1.0, options=opts)
+    assert s.advance(2.0, 5) == 1 and 'status 4' in s.last_error
+    assert np.array_equal(s.download(), u0)
