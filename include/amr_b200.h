@@ -238,10 +238,12 @@ int amr_gpu_diagnostics(amr_gpu_session* session, const double region[4], double
  * stream is a cudaStream_t (NULL: the default stream).  The scratch (primitives and face fluxes)
  * lives in one static device array of 1.8 MB that every GPU loading the library holds until the
  * process exits, so meshes are limited to 16384 cells and 40960 faces; larger ones are rejected
- * with an error.  The first call on a device looks up that array's device address, so make it
- * before any stream capture.  All calls on a device share the array: calls whose kernels
- * overlap on the GPU (other streams or host threads) race.  Synchronises `stream`; returns 1
- * with a message for a nonphysical state, like amr_gpu_residual. */
+ * with an error.  Every call looks up that array's device address on the current device and
+ * synchronises `stream` to read its status word, so no call may be made while a stream is being
+ * captured.  All calls on a device share the array: calls whose kernels overlap on the GPU (other
+ * streams or host threads) race, so serialise them.  Returns 1 with a message for a nonphysical
+ * state, like amr_gpu_residual, and for mesh records whose indices fall outside the arrays
+ * passed (face cells, boundary side or axis, a cell's face range, face ids, wall ranges). */
 int amr_euler_residual_static(const amr_cell_t* cells, uint64_t n_cells, const amr_face_t* faces, uint64_t n_faces,
                               const amr_wall_t* walls, uint64_t n_walls, const uint64_t* face_offsets,
                               const uint64_t* cell_faces, const amr_boundary_t* boundaries, const amr_params_t* params,

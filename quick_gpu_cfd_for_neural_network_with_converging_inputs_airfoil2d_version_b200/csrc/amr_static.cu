@@ -38,8 +38,10 @@ constexpr uint64_t kScratchDoubles = 4 * (kMaxCells + kMaxFaces) + 2;
 // GPU (different streams, or different host threads on one device) race on it.
 static __device__ __align__(256) double g_residual_scratch[kScratchDoubles];
 
-constexpr int kMaxDevices = 64;
-double* g_scratch_address[kMaxDevices] = {nullptr};
+// Status bits the kernels raise: a nonphysical state or flux, and a mesh record whose indices
+// point outside the arrays the caller passed (the access is skipped, nothing is read there).
+constexpr int kBadState = 1;
+constexpr int kBadMesh = 2;
 
 struct StaticParams {
   double gamma, mco;
@@ -48,7 +50,8 @@ struct StaticParams {
   Bnd<double> bnd[4];
 };
 
-__device__ __forceinline__ void flag_bad(int* status) { atomicOr(status, 1); }
+__device__ __forceinline__ void flag_bad(int* status) { atomicOr(status, kBadState); }
+__device__ __forceinline__ void flag_mesh(int* status) { atomicOr(status, kBadMesh); }
 
 __global__ void static_primitive_kernel(const double* __restrict__ u, uint64_t n, double gamma, double* __restrict__ w,
                                         int* status) {
@@ -69,6 +72,11 @@ __global__ void static_face_kernel(const amr_face_t* __restrict__ faces, uint64_
   const uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (q >= nf) return;
   const amr_face_t f = faces[q];
+  if (f.left >= (int64_t)n || f.right >= (int64_t)n || (f.left < 0 && f.right < 0) || f.boundary < -1 || f.boundary > 3 ||
+      (f.boundary < 0 && (f.left < 0 || f.right < 0)) || (f.axis != 0 && f.axis != 1)) {
+    flag_mesh(status);
+    return;
+  }
   const int inside = f.left >= 0 ? f.left : f.right;
   const int la = f.left >= 0 ? f.left : inside, rb = f.right >= 0 ? f.right : inside;
   double a[4], b[4];
@@ -103,14 +111,26 @@ __global__ void static_face_kernel(const amr_face_t* __restrict__ faces, uint64_
 }
 
 __global__ void static_gather_kernel(const amr_cell_t* __restrict__ cells, uint64_t n, const amr_face_t* __restrict__ faces,
-                                     uint64_t nf, const amr_wall_t* __restrict__ walls, const uint64_t* __restrict__ offsets,
-                                     const uint64_t* __restrict__ cell_faces, const double* __restrict__ w,
-                                     const double* __restrict__ flux, double* __restrict__ r) {
+                                     uint64_t nf, const amr_wall_t* __restrict__ walls, uint64_t nw,
+                                     const uint64_t* __restrict__ offsets, const uint64_t* __restrict__ cell_faces,
+                                     const double* __restrict__ w, const double* __restrict__ flux, double* __restrict__ r,
+                                     int* status) {
   const uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (k >= n) return;
   const amr_cell_t c = cells[k];
+  // cell_faces holds offsets[n] entries, so every position below offsets[n] may be read
+  const uint64_t begin = offsets[k], end = offsets[k + 1], total = offsets[n];
+  if (begin > end || end > total || c.wall_begin > nw || c.wall_count > nw - c.wall_begin) {
+    flag_mesh(status);
+    return;
+  }
+  for (uint64_t pos = begin; pos < end; ++pos)
+    if (cell_faces[pos] >= nf) {
+      flag_mesh(status);
+      return;
+    }
   double sum[4] = {0, 0, 0, 0};
-  for (uint64_t pos = offsets[k]; pos < offsets[k + 1]; ++pos) {
+  for (uint64_t pos = begin; pos < end; ++pos) {
     const uint64_t face = cell_faces[pos];
     const double sign = faces[face].left == (int)k ? 1.0 : -1.0;
     for (int v = 0; v < 4; ++v) sum[v] += sign * flux[v * nf + face];
@@ -158,20 +178,13 @@ extern "C" int amr_euler_residual_static(const amr_cell_t* cells, uint64_t n_cel
     put(error, error_size, "invalid static residual parameters");
     return 1;
   }
-  int device = 0;
-  if (!check(cudaGetDevice(&device), error, error_size, "cudaGetDevice")) return 1;
-  if (device < 0 || device >= kMaxDevices) {
-    put(error, error_size, "device ordinal out of range");
-    return 1;
-  }
-  // Set-up, once per device, with that device current: the device address of the scratch array
-  // (the array's name in host code is only a host-side handle).
-  if (!g_scratch_address[device]) {
-    void* address = nullptr;
-    if (!check(cudaGetSymbolAddress(&address, g_residual_scratch), error, error_size, "cudaGetSymbolAddress")) return 1;
-    g_scratch_address[device] = static_cast<double*>(address);
-  }
-  double* scratch = g_scratch_address[device];
+  // The device address of the scratch array on the current device (the array's name in host code
+  // is only a host-side handle).  It is looked up on every call rather than cached: the lookup is
+  // cheap once the module is loaded, two host threads cannot race on a cache, and a device reset
+  // (which reloads the module, possibly elsewhere) cannot leave a stale address behind.
+  void* address = nullptr;
+  if (!check(cudaGetSymbolAddress(&address, g_residual_scratch), error, error_size, "cudaGetSymbolAddress")) return 1;
+  double* scratch = static_cast<double*>(address);
   double* w = scratch;                        // 4 * n_cells
   double* flux = scratch + 4 * kMaxCells;     // 4 * n_faces
   int* status = reinterpret_cast<int*>(scratch + 4 * (kMaxCells + kMaxFaces));
@@ -201,14 +214,18 @@ extern "C" int amr_euler_residual_static(const amr_cell_t* cells, uint64_t n_cel
   const int T = 128;
   static_primitive_kernel<<<(unsigned)((n_cells + T - 1) / T), T, 0, st>>>(u, n_cells, p.gamma, w, status);
   static_face_kernel<<<(unsigned)((n_faces + T - 1) / T), T, 0, st>>>(faces, n_faces, n_cells, w, sp, flux, status);
-  static_gather_kernel<<<(unsigned)((n_cells + T - 1) / T), T, 0, st>>>(cells, n_cells, faces, n_faces, walls, face_offsets,
-                                                                        cell_faces, w, flux, r);
+  static_gather_kernel<<<(unsigned)((n_cells + T - 1) / T), T, 0, st>>>(cells, n_cells, faces, n_faces, walls, n_walls,
+                                                                        face_offsets, cell_faces, w, flux, r, status);
   if (!check(cudaGetLastError(), error, error_size, "static residual launch")) return 1;
   int host_status = 0;
   if (!check(cudaMemcpyAsync(&host_status, status, sizeof(int), cudaMemcpyDeviceToHost, st), error, error_size,
              "status read-back") ||
       !check(cudaStreamSynchronize(st), error, error_size, "static residual sync"))
     return 1;
+  if (host_status & kBadMesh) {
+    put(error, error_size, "mesh record index out of range (face cell/boundary/axis, cell face range, face id or wall range)");
+    return 1;
+  }
   if (host_status) {
     put(error, error_size, "nonphysical state or nonfinite face flux");
     return 1;

@@ -1,6 +1,6 @@
 """Generates the golden fixtures in tests/golden/ (run in a container that has the reference).
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py [--reference <reference checkout>]  (default: beside this repository)
 
 Writes
   examples.npz      the reference's ten example contours (examples/G*.csv) prepared by the
@@ -94,7 +94,7 @@ class SettingsSpec(cases.CaseSpec):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--reference', default='/root/reference')
+    ap.add_argument('--reference', default=str(pathlib.Path(__file__).resolve().parents[3] / 'reference'))
     args = ap.parse_args()
     ref = pathlib.Path(args.reference)
     sys.path.insert(0, str(ref))

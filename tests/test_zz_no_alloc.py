@@ -72,3 +72,30 @@ def test_static_residual_rejects_meshes_beyond_capacity(golden):
     st = lib().amr_euler_residual_static(fake, 16385, fake, 1, None, 0, fake, fake, mesh.boundaries.ctypes.data,
                                          C.addressof(params), fake, fake, None, err, len(err))
     assert st == 1 and 'capacity' in err.value.decode()
+
+
+def test_static_residual_reports_out_of_range_mesh_indices(golden):
+    """A face whose boundary side is not 0..3 and a cell whose wall range runs past n_walls are
+    skipped on the device (nothing is read through them) and returned as an error."""
+    import torch
+    mesh = MeshArrays.load(golden / 'mesh_naca0012_lf1_euler_srd.npz')
+    spec = cases.CaseSpec(physics='euler', profile='LF1', mach=1.65, aoa=1.5)
+    params = spec.params()
+    u0 = cases.initial_state(mesh, spec.initial_primitive())
+    for table, field, value in (('faces', 'boundary', 7), ('cells', 'wall_count', mesh.n_walls + 5)):
+        broken = getattr(mesh, table).copy()
+        broken[field][3] = value
+        bufs = {name: device_copy(broken if name == table else getattr(mesh, name))
+                for name in ('cells', 'faces', 'walls', 'face_offsets', 'cell_faces')}
+        d_u = device_copy(u0)
+        d_r = torch.zeros(4 * mesh.n_cells, dtype=torch.float64, device='cuda')
+        err = errbuf()
+        st = lib().amr_euler_residual_static(
+            bufs['cells'].data_ptr(), mesh.n_cells, bufs['faces'].data_ptr(), mesh.n_faces, bufs['walls'].data_ptr(),
+            mesh.n_walls, bufs['face_offsets'].data_ptr(), bufs['cell_faces'].data_ptr(), mesh.boundaries.ctypes.data,
+            C.addressof(params), d_u.data_ptr(), d_r.data_ptr(), None, err, len(err))
+        assert st == 1 and 'out of range' in err.value.decode(), (table, err.value.decode())
+    # a well-formed call afterwards still succeeds (the status word is cleared per call)
+    bufs = {name: device_copy(getattr(mesh, name)) for name in ('cells', 'faces', 'walls', 'face_offsets', 'cell_faces')}
+    r = static_residual(mesh, params, bufs, u0)
+    assert np.isfinite(r).all()
