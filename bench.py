@@ -1,16 +1,29 @@
 """Benchmark of the static-AMR explicit time step on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload batched|plain]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload batched|accuracy|time-accurate|serve]
 
-One step = one SSP-RK3 step (one trial) of every case in the batch.  Workload `batched` (the
-default): 256 SA-neg/Sutherland cases, HLLC, FP32 state (FP64 dt/norms/loads), half LF1 and half
-LF2 meshes, each case with its own seeded Mach ~ U[1.2, 2.0] and AoA ~ U[-3, 5] deg.  `value` is
-whole-job accepted cell-steps per second timed with CUDA events on the engine's launch stream;
-`e2e` is the same work through the C ABI from host buffers (mesh + state upload, the steps, state
-download) timed on the host clock.  Beside it: the plain FP64 session on the same meshes and the
-reference CPU core (oracle/_ref, all host threads) on a bounded sample.
+One step = one SSP-RK3 step (one trial) of every case in the batch.
+
+Workload `batched` (the default): 256 seeded NACA 4-digit airfoils (m~U[0,0.06], p~U[0.2,0.6],
+t~U[0.08,0.15]; a draw the mesh builder rejects is redrawn and counted), half on LF1 and half on
+LF2 meshes, SA-neg with Sutherland viscosity, HLLC, M~U[1.2,2.0], AoA~U[-3,5] deg, FP32 state with
+FP64 dt, norms and loads.  `value` is whole-job accepted cell-steps per second over exactly K timed
+steps, CUDA events on the engine's launch stream; `e2e` is the same work through the C ABI from
+host buffers (batch creation, mesh and state upload, the K steps, download of every state) on the
+host clock.  Beside it: a measured 5000-step solve of the same batch (solves/s), the plain FP64
+session on the same meshes, the plain FP64 inviscid Euler+SRD NACA 0012 LF1 case (200 steps) with
+the reference CPU core at 1 thread and at all host threads, and the reference CPU core on a
+bounded sample of the workload.
+
+Workload `accuracy`: NACA 2412 on LF2, SA, run to the steady criteria or 20000 steps in FP64 and in
+FP32, with the CL/CD/CM and per-field errors of the FP32 form.  `time-accurate`: 128 seeded LF2
+cases, laminar with constant viscosity, AUSM+-up, pressure outlet on xmax, integrated to t*=1 in
+FP32 and FP64, with the per-cell errors of rho, u, v, p.  `serve`: the served form (Poisson
+arrivals, continuous batching, p50/p99 latency).
 """
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -19,6 +32,7 @@ import select
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 import numpy as np
@@ -26,19 +40,21 @@ import numpy as np
 ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200 import _abi, cases  # noqa: E402
+from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200 import _abi, cases, runs, workloads  # noqa: E402
 from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200.batch import Batch, case_control  # noqa: E402
 from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200.mesh import MeshArrays  # noqa: E402
 from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200.session import StaticAmrGpu, default_options  # noqa: E402
 
 METRIC = 'solves/s & cell-steps/s at |ΔCL|,|ΔCD|≤1e-4 vs plain FP64; p50/p99 latency'
 GOLDEN = ROOT / 'tests' / 'golden'
-MESHES = {'LF1': GOLDEN / 'mesh_naca2412_lf1_sa.npz', 'LF2': GOLDEN / 'mesh_naca2412_lf2_sa.npz'}
 SOLVE_STEPS = 5000  # steps per solve of the batched workload
-# DRAM bytes (read + write) of one split-mode trial of the 256-case workload, summed over its
-# kernels from one ncu capture (profiles/split_trial_f32_sa_256cases.md; cold cache, so an upper
-# bound of a warm trial).  Reported as roofline.traffic when the run matches that configuration.
-SPLIT_256_TRAFFIC_PER_STEP = 2.7783e9
+# DRAM bytes (read + write) of one step of the default workload (256 cases, split launch mode),
+# summed over the step's kernel launches from an ncu capture of `bench.py --profile split`
+# (dram__bytes_read.sum + dram__bytes_write.sum, caches flushed before every launch, so it bounds
+# the warm traffic from above).  It comes from that separate capture, not from the timed run.
+SPLIT_256_TRAFFIC_PER_STEP = None
+TRAFFIC_SOURCE = ('ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum over the 11 launches of one step of '
+                  '`bench.py --profile split --cases 256` (separate capture, cold cache)')
 
 
 def peaks():
@@ -61,17 +77,82 @@ def algorithmic_bytes(mesh, s=4, sg=4):
     c_term = 4 + 2 * sg
     srd = 0
     if mesh.small_cells:
-        for k in range(n):
-            size = int(mesh.group_offsets[k + 1] - mesh.group_offsets[k])
-            if size > 1:
-                srd += 16 * size
+        sizes = np.diff(mesh.group_offsets.astype(np.int64))
+        srd = 16 * int(sizes[sizes > 1].sum())
     return 8 * nv * s * n + 3 * (n * c_cell + nf * c_face + nw * c_wall + T * c_term + srd)
 
 
+def _cuda_pci_bus_id(device):
+    try:
+        rt = ctypes.CDLL('libcudart.so.12')
+        buf = ctypes.create_string_buffer(64)
+        if rt.cudaDeviceGetPCIBusId(buf, 64, int(device)) == 0:
+            return buf.value.decode()
+    except OSError:
+        pass
+    return None
+
+
+class NvmlSampler:
+    """SM clock and clock-event reasons read through NVML every `interval_s` while entered.  It is
+    entered around the timed region itself, which at the driver's step counts lasts only tens of
+    milliseconds (too short for nvidia-smi's sampling)."""
+    REASONS = {8: 'hw_slowdown', 64: 'hw_thermal_slowdown', 32: 'sw_thermal_slowdown', 4: 'sw_power_cap',
+               128: 'hw_power_brake_slowdown'}
+
+    def __init__(self, device, interval_s=0.0005):
+        self.device = device
+        self.interval_s = interval_s
+        self.samples = []
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._thread = None
+        self._h = None
+
+    def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            bus = _cuda_pci_bus_id(self.device)
+            self._h = (pynvml.nvmlDeviceGetHandleByPciBusId(bus) if bus else pynvml.nvmlDeviceGetHandleByIndex(self.device))
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM))
+            self._nvml = pynvml
+            self._thread = threading.Thread(target=self._loop, daemon=True)
+            self._thread.start()
+        except Exception:
+            self._h = None
+        return self
+
+    def _loop(self):
+        nv = self._nvml
+        while not self._stop.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM)
+                reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                self.samples.append((float(mhz), int(reasons)))
+            except Exception:
+                break
+            time.sleep(self.interval_s)
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thread:
+            self._thread.join(timeout=5)
+
+    def summary(self):
+        sm = [s for s, _ in self.samples]
+        reasons = set()
+        for _, bits in self.samples:
+            for bit, name in self.REASONS.items():
+                if bits & bit:
+                    reasons.add(name)
+        return dict(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=self.max_mhz, reasons=sorted(reasons),
+                    samples=len(sm), source='NVML, timed region only')
+
+
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every `interval_ms` while entered (the
-    batched bench enters it for the warm-up and timed loop only, so idle set-up time, when the
-    GPU drops its clocks, does not count)."""
+    """nvidia-smi clocks and throttle reasons sampled every `interval_ms` while entered (used
+    around the longer legs: warm-up, timed loop and the full solve)."""
     FIELDS = 'index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,' \
              'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap'
 
@@ -119,20 +200,7 @@ class ClockSampler:
                 if val.lower() == 'active':
                     reasons.add(name)
         return dict(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=mx, reasons=sorted(reasons),
-                    samples=len(sm))
-
-
-def batched_cases(ncases, seed=20261203):
-    rng = np.random.default_rng(seed)
-    meshes = {k: MeshArrays.load(v) for k, v in MESHES.items()}
-    out = []
-    for i in range(ncases):
-        profile = 'LF1' if i % 2 == 0 else 'LF2'
-        mach, aoa = float(rng.uniform(1.2, 2.0)), float(rng.uniform(-3.0, 5.0))
-        spec = cases.CaseSpec(naca=(0.02, 0.4, 0.12), profile=profile, physics='sa', mach=mach, aoa=aoa)
-        mesh = meshes[profile].with_physics(boundaries=spec.boundary_records())
-        out.append((spec, mesh))
-    return out
+                    samples=len(sm), source='nvidia-smi, warm-up + timed loop + full solve')
 
 
 def parse_launch(cfg):
@@ -144,23 +212,26 @@ def parse_launch(cfg):
     return block, grid, mode
 
 
-def run_batched(case_list, precision, steps, warmup, device=0, trials=32, block=0, grid=0, tune=True, clock=None):
-    """Admit every case, autotune, warm up, then time `steps` trials with CUDA events on the
-    engine stream.  Accepted cell-steps are counted per case from the device counters.  `clock`
-    (a ClockSampler) samples the warm-up and timed loop."""
-    total_cells = sum(m.n_cells for _, m in case_list)
-    b = Batch(precision=precision, model=_abi.MODEL_LAMINAR, sa=True, max_cases=len(case_list),
-              max_cells=total_cells + 64, device=device, block_threads=block, grid_blocks=grid)
-    slots = []
-    for spec, mesh in case_list:
-        u0 = cases.initial_state(mesh, spec.initial_primitive())
-        s = b.admit(mesh, spec.params(), u0, case_control(1e30, 10 ** 9, steady=False, mach=spec.mach, aoa=spec.aoa))
-        assert s is not None, 'arena too small'
-        slots.append(s)
-    if tune:
-        b.autotune(4)
-    if clock is not None:
-        clock.__enter__()
+def new_batch(case_list, precision, device=0, block=0, grid=0, mode=0):
+    kw = workloads.batch_kwargs(case_list)
+    return Batch(precision=precision, device=device, block_threads=block, grid_blocks=grid, launch_mode=mode, **kw)
+
+
+def admit_all(b, case_list, steps_cap=10 ** 9):
+    items = [(m, s.params(), cases.initial_state(m, s.initial_primitive()),
+              case_control(1e30, steps_cap, steady=False, mach=s.mach, aoa=s.aoa)) for s, m in case_list]
+    slots = b.admit_many(items)
+    assert all(s is not None for s in slots), 'arena too small'
+    return slots
+
+
+def run_batched(case_list, precision, steps, warmup, device=0, trials=32):
+    """Admit every case, autotune, warm up, then time exactly `steps` trials with CUDA events on the
+    engine stream.  Accepted cell-steps are counted per case from the device counters.  The NVML
+    sampler covers the timed loop alone."""
+    b = new_batch(case_list, precision, device)
+    slots = admit_all(b, case_list)
+    b.autotune(4)
     done = 0
     while done < warmup:
         k = min(trials, warmup - done)
@@ -169,28 +240,51 @@ def run_batched(case_list, precision, steps, warmup, device=0, trials=32, block=
     before = [b.status(s)['steps'] for s in slots]
     launches0 = b.kernel_launches
     dev_seconds, adv, advances = 0.0, 0, 0
-    while adv < steps:
-        k = min(trials, steps - adv)
-        b.advance(k)
-        dev_seconds += b.last_advance_seconds
-        adv += k
-        advances += 1
-    if clock is not None:
-        clock.__exit__(None, None, None)
+    with NvmlSampler(device) as nvml:
+        while adv < steps:
+            k = min(trials, steps - adv)
+            b.advance(k)
+            dev_seconds += b.last_advance_seconds
+            adv += k
+            advances += 1
     status = [b.status(s) for s in slots]
     cell_steps = sum(m.n_cells * (st['steps'] - b0) for (_, m), st, b0 in zip(case_list, status, before))
     return dict(batch=b, slots=slots, dev_seconds=dev_seconds, launches=b.kernel_launches - launches0,
-                cell_steps=cell_steps, status=status, config=b.launch_config(), advances=advances)
+                cell_steps=cell_steps, status=status, config=b.launch_config(), advances=advances, nvml=nvml.summary())
+
+
+def run_solve(case_list, nsteps, device, block, grid, mode, trials=32):
+    """A full solve of the batch: every case from its freestream start to `nsteps` accepted steps,
+    device time from CUDA events; solves/s = cases / that time (measured, not extrapolated)."""
+    b = new_batch(case_list, 32, device, block, grid, mode)
+    try:
+        slots = admit_all(b, case_list, nsteps)
+        t0 = time.perf_counter()
+        dev = 0.0
+        polls = 0
+        while True:
+            b.advance(trials)
+            dev += b.last_advance_seconds
+            polls += 1
+            st = [b.status(s) for s in slots]
+            if all(x['status'] == _abi.STATUS_MAXSTEPS for x in st) or polls > nsteps:
+                break
+        wall = time.perf_counter() - t0
+        steps = [x['steps'] for x in st]
+        cell_steps = sum(m.n_cells * x for (_, m), x in zip(case_list, steps))
+        return dict(steps_per_solve=nsteps, cases=len(case_list), device_seconds=dev, host_seconds=wall,
+                    solves_per_s=len(case_list) / dev, cell_steps_per_s=cell_steps / dev,
+                    all_cases_completed=all(x == nsteps for x in steps), rejected=sum(x['rejected'] for x in st))
+    finally:
+        b.destroy()
 
 
 def run_e2e(case_list, precision, steps, device=0, trials=32, block=0, grid=0, mode=0):
     """The same work end to end through the C ABI from host buffers: batch creation, mesh and
-    state upload of every case (one bulk admission), `steps` trials with a control read-back per launch, and the
-    download of every final state; host wall clock."""
+    state upload of every case (one bulk admission), `steps` trials with a control read-back per
+    launch, and the download of every final state; host wall clock."""
     t0 = time.perf_counter()
-    total_cells = sum(m.n_cells for _, m in case_list)
-    b = Batch(precision=precision, model=_abi.MODEL_LAMINAR, sa=True, max_cases=len(case_list),
-              max_cells=total_cells + 64, device=device, block_threads=block, grid_blocks=grid, launch_mode=mode)
+    b = new_batch(case_list, precision, device, block, grid, mode)
     t_create = time.perf_counter()
     items, h2d = [], 0
     for spec, mesh in case_list:
@@ -234,55 +328,101 @@ def mesh_bytes(mesh, precision):
     return cells + slots + walls + terms
 
 
+def time_plain(spec, mesh, steps):
+    """The plain FP64 session on one case: a first session warms up (graph capture, autotune); a
+    second, with the chosen launch, runs `steps` steps timed by CUDA events."""
+    u0 = cases.initial_state(mesh, spec.initial_primitive())
+    w = StaticAmrGpu.create(mesh, spec.params(), u0)
+    w.advance(1e30, 64)
+    cfg = w.launch_config()
+    w.destroy()
+    block, grid, mode = parse_launch(cfg)
+    s = StaticAmrGpu.create(mesh, spec.params(), u0, options=default_options(block_threads=block, grid_blocks=grid,
+                                                                             launch_mode=mode))
+    s.advance(1e30, steps)
+    st = s.stats()
+    sec = st['advance_event_seconds']
+    out = dict(cells=mesh.n_cells, steps=s.steps, seconds=sec, us_per_step=1e6 * sec / s.steps,
+               cell_steps_per_s=mesh.n_cells * s.steps / sec, config=cfg, polls=st['status_polls'])
+    s.destroy()
+    return out
+
+
 def plain_fp64(case_list, steps):
-    """The plain FP64 session on one case of each profile: accepted cell-steps per device second.
-    A first session warms up (graph capture, autotune); the timed session runs `steps` steps."""
+    """The plain FP64 session on the first case of each profile of the workload."""
     res = {}
     for profile in ('LF1', 'LF2'):
         spec, mesh = [c for c in case_list if c[0].profile == profile][0]
-        u0 = cases.initial_state(mesh, spec.initial_primitive())
-        w = StaticAmrGpu.create(mesh, spec.params(), u0)
-        w.advance(1e30, 64)
-        cfg = w.launch_config()
-        w.destroy()
-        block, grid, mode = parse_launch(cfg)
-        s = StaticAmrGpu.create(mesh, spec.params(), u0,
-                                options=default_options(block_threads=block, grid_blocks=grid, launch_mode=mode))
-        s.advance(1e30, steps)
-        st = s.stats()
-        sec = st['advance_event_seconds']
-        res[profile] = dict(cells=mesh.n_cells, steps=s.steps, seconds=sec, us_per_step=1e6 * sec / s.steps,
-                            cell_steps_per_s=mesh.n_cells * s.steps / sec, config=cfg, polls=st['status_polls'])
-        s.destroy()
+        res[profile] = time_plain(spec, mesh, steps)
     return res
 
 
-def cpu_reference(case_list, steps_lf1, steps_lf2, threads):
-    """Reference CPU core (oracle/_ref, OpenMP) on one case of each profile, in a subprocess so the
-    OpenMP thread count is fixed before the runtime loads."""
-    code = f'''
-import json, sys
-sys.path.insert(0, {str(ROOT)!r})
-from bench import batched_cases
-from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200 import cases
-from oracle.oracle import RefCase
-cl = batched_cases(2)
-out = {{}}
-for (spec, mesh), n in zip(cl, ({steps_lf1}, {steps_lf2})):
-    rc = RefCase.from_mesh(mesh, spec.params(), kind='omp')
-    u0 = cases.initial_state(mesh, spec.initial_primitive())
-    sec, r = rc.run_timed(u0, 1e30, n)
-    out[spec.profile] = dict(cells=mesh.n_cells, steps=r['steps'], seconds=sec)
-print(json.dumps(out))
-'''
+def _ref_subprocess(code, threads):
+    """Runs `code` in a fresh interpreter with the OpenMP thread count fixed before the runtime loads;
+    returns the JSON object of its last output line."""
     env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND='false')
     r = subprocess.run([sys.executable, '-c', code], capture_output=True, text=True, env=env, cwd=str(ROOT))
     if r.returncode:
         raise RuntimeError(r.stderr[-2000:])
-    d = json.loads(r.stdout.strip().splitlines()[-1])
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def cpu_reference(steps_lf1, steps_lf2, threads, seed):
+    """The reference CPU core (oracle/_ref, OpenMP build) on the first LF1 and the first LF2 case of
+    the workload's draws, meshes built by the reference builder; cell-steps per second."""
+    code = f'''
+import json, sys
+sys.path.insert(0, {str(ROOT)!r})
+from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200 import airfoils, cases, workloads
+from oracle.oracle import RefCase
+out = {{}}
+for spec, n in zip(workloads.batched_sa_specs(2, {seed}), ({steps_lf1}, {steps_lf2})):
+    x, y, pt = airfoils.naca4(*spec.naca)
+    rc = RefCase.build(spec, x, y, pt, kind='omp')
+    u0 = rc.initial(spec.initial_primitive())
+    sec, r = rc.run_timed(u0, 1e30, n)
+    out[spec.profile] = dict(cells=rc.counts['n'], steps=r['steps'], seconds=sec)
+print(json.dumps(out))
+'''
+    d = _ref_subprocess(code, threads)
     cell_steps = sum(v['cells'] * v['steps'] for v in d.values())
     seconds = sum(v['seconds'] for v in d.values())
     return cell_steps / seconds, d
+
+
+def config1_leg(steps=200):
+    """Plain FP64 inviscid Euler + SRD, NACA 0012 LF1 (the reference's CPU-runnable case), 200 steps:
+    the FP64 session on the GPU beside the reference CPU core at 1 thread (the reference driver's
+    default, OMP_NUM_THREADS=1) and at every host thread."""
+    mesh = MeshArrays.load(GOLDEN / 'mesh_naca0012_lf1_euler_srd.npz')
+    spec = cases.CaseSpec(physics='euler', profile='LF1', mach=1.65, aoa=1.5)
+    gpu = time_plain(spec, mesh, steps)
+    code = f'''
+import json, sys
+sys.path.insert(0, {str(ROOT)!r})
+from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200 import cases
+from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200.mesh import MeshArrays
+from oracle.oracle import RefCase
+mesh = MeshArrays.load({str(GOLDEN / 'mesh_naca0012_lf1_euler_srd.npz')!r})
+spec = cases.CaseSpec(physics='euler', profile='LF1', mach=1.65, aoa=1.5)
+rc = RefCase.from_mesh(mesh, spec.params(), kind=sys.argv[1] if len(sys.argv) > 1 else 'KIND')
+u0 = cases.initial_state(mesh, spec.initial_primitive())
+rc.run_timed(u0, 1e30, 5)
+sec, r = rc.run_timed(u0, 1e30, {steps})
+print(json.dumps(dict(cells=mesh.n_cells, steps=r['steps'], seconds=sec)))
+'''
+    threads = os.cpu_count() or 1
+    one = _ref_subprocess(code.replace("'KIND'", "'serial'"), 1)
+    allc = _ref_subprocess(code.replace("'KIND'", "'omp'"), threads)
+    cpu = {}
+    for name, d, t in (('1_thread', one, 1), ('all_threads', allc, threads)):
+        cpu[name] = dict(threads=t, ms_per_step=1e3 * d['seconds'] / d['steps'],
+                         cell_steps_per_s=d['cells'] * d['steps'] / d['seconds'])
+    return dict(workload='plain-fp64-euler-srd-naca0012-lf1', cells=mesh.n_cells, steps=steps,
+                gpu=dict(us_per_step=gpu['us_per_step'], cell_steps_per_s=gpu['cell_steps_per_s'], launch=gpu['config']),
+                cpu_reference=cpu, cpu=cpu_model(),
+                gpu_over_cpu_1_thread=gpu['cell_steps_per_s'] / cpu['1_thread']['cell_steps_per_s'],
+                gpu_over_cpu_all_threads=gpu['cell_steps_per_s'] / cpu['all_threads']['cell_steps_per_s'])
 
 
 def cpu_model():
@@ -316,31 +456,45 @@ def dist_max(value, world):
     return float(t.item())
 
 
+def dist_sum(value, world):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def dist_barrier(world):
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
 
 
+def rank_seed(rank):
+    return workloads.SEED + 1000 * rank
+
+
 def reference_arm(args, rank, world):
     """--impl reference: the reference CPU implementation (oracle/_ref with all host threads) on
-    the same workload, each step a bounded sample (one LF1 + one LF2 case)."""
+    the same workload, each step a bounded sample (the first LF1 and LF2 cases of the draws)."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    case_list = batched_cases(2)
     n_lf1, n_lf2 = 40, 20
     values = []
     for _ in range(max(1, args.warmup)):
-        cpu_reference(case_list, 4, 2, threads)
+        cpu_reference(4, 2, threads, rank_seed(0))
     for _ in range(args.steps):
-        v, detail = cpu_reference(case_list, n_lf1, n_lf2, threads)
+        v, detail = cpu_reference(n_lf1, n_lf2, threads, rank_seed(0))
         values.append(v)
     value = statistics.median(values)
     line = dict(metric=METRIC, impl='reference', value=value, unit='cell-steps/s', n_gpus=args.gpus,
                 steps=args.steps, warmup=args.warmup, higher_is_better=True, scaling='weak', vs_baseline=None,
                 dtype='f64', data='synthetic',
-                config=dict(workload='batched-sa-fp32-256', sample=f'1 LF1 x {n_lf1} + 1 LF2 x {n_lf2} steps per step'),
+                config=dict(workload='batched-sa-fp32-%d' % args.cases,
+                            sample=f'1 LF1 x {n_lf1} + 1 LF2 x {n_lf2} steps per step (first draws of the workload)'),
                 cpu_baseline=dict(value=value, unit='cell-steps/s', cores=threads, kind='reference',
                                   sample=f'1 LF1 ({detail["LF1"]["cells"]} cells) x {n_lf1} steps + 1 LF2 '
                                          f'({detail["LF2"]["cells"]} cells) x {n_lf2} steps', cpu=cpu_model()),
@@ -349,8 +503,8 @@ def reference_arm(args, rank, world):
 
 
 def run_serving(args, rank, world, local):
-    """--serve: the served form.  Poisson request arrivals (seeded), host mesh builds on a thread
-    pool, admission while the arena has room, device steady-rule retirement or the step cap.
+    """--workload serve: the served form.  Poisson request arrivals (seeded), host mesh builds on a
+    thread pool, admission by free device memory, device steady-rule retirement or the step cap.
     Each rank serves its shard on its own GPU; rank 0 prints one JSON line."""
     from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200 import serve
     reqs = serve.poisson_requests(args.requests, args.rate, args.seed)
@@ -377,14 +531,80 @@ def run_serving(args, rank, world, local):
     dist_barrier(world)
 
 
-def dist_sum(value, world):
-    if world == 1:
-        return value
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([float(value)], dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+def accuracy_leg(args):
+    """NACA 2412 LF2 SA to the steady criteria or 20000 steps, FP64 and FP32: loads at every check
+    and of the final states, and the per-field error of the FP32 final state."""
+    w = workloads.naca2412_lf2_sa()
+    spec, mesh = w.items[0]
+    ctl = runs.steady_control(max_steps=args.accuracy_steps)
+    out = {}
+    for prec in (64, 32):
+        res, sec = runs.solve(w.items, prec, ctl)
+        r = res[0]
+        out[prec] = dict(status=r['status'], steps=r['steps'], time=r['time'], converged=r['converged'],
+                         checks=r['checks'], last_check=dict(cl=r['cl'], cd=r['cd'], cm=r['cm']),
+                         final_state_loads=runs.loads_of_state(spec, mesh, r['u']), device_seconds=sec, u=r['u'])
+    e_check = runs.load_errors(out[32]['last_check'], out[64]['last_check'])
+    e_final = runs.load_errors(out[32]['final_state_loads'], out[64]['final_state_loads'])
+    fields = runs.field_errors(out[32]['u'], out[64]['u'], mesh.nv)
+    for p in out.values():
+        p.pop('u')
+    line = dict(workload='accuracy-naca2412-lf2-sa', cells=mesh.n_cells, max_steps=args.accuracy_steps,
+                fp64=out[64], fp32=out[32], load_error_last_check=e_check, load_error_final_state=e_final,
+                field_error_final_state=fields,
+                note='FP32 and FP64 end at the same step count; their final times differ by the dt history')
+    print(json.dumps(line), flush=True)
+
+
+def time_accurate_leg(args):
+    """128 seeded LF2 laminar AUSM+-up cases with a pressure outlet, to t*=1, FP32 against FP64:
+    per-cell errors of rho, u, v, p (largest over the cases of each measure)."""
+    w = workloads.time_accurate_laminar(args.ta_cases)
+    res32, s32 = runs.solve(w.items, 32, runs.fixed_time(1.0))
+    res64, s64 = runs.solve(w.items, 64, runs.fixed_time(1.0))
+    worst = {}
+    per_case = []
+    for (spec, mesh), a, b in zip(w.items, res32, res64):
+        e = runs.field_errors(a['u'], b['u'], mesh.nv)
+        per_case.append(dict(mach=spec.mach, aoa=spec.aoa, steps32=a['steps'], steps64=b['steps'],
+                             time32=a['time'], time64=b['time'], max_rel=max(v['max_rel'] for v in e.values())))
+        for name, v in e.items():
+            cur = worst.setdefault(name, dict(max_abs=0.0, max_rel=0.0, rms_rel=0.0))
+            for k in cur:
+                cur[k] = max(cur[k], v[k])
+    cs32 = sum(m.n_cells * r['steps'] for (_, m), r in zip(w.items, res32))
+    cs64 = sum(m.n_cells * r['steps'] for (_, m), r in zip(w.items, res64))
+    line = dict(w.describe(), tend=1.0,
+                fp32=dict(device_seconds=s32, cell_steps_per_s=cs32 / s32,
+                          all_finished=all(r['time'] == 1.0 for r in res32), rejected=sum(r['rejected'] for r in res32)),
+                fp64=dict(device_seconds=s64, cell_steps_per_s=cs64 / s64,
+                          all_finished=all(r['time'] == 1.0 for r in res64), rejected=sum(r['rejected'] for r in res64)),
+                steps=dict(min=min(r['steps'] for r in res64), max=max(r['steps'] for r in res64)),
+                field_error_worst_case=worst,
+                worst_cases=sorted(per_case, key=lambda c: -c['max_rel'])[:3])
+    print(json.dumps(line), flush=True)
+
+
+def profile_leg(args, local):
+    """--profile MODE: only the timed batched loop with a fixed launch mode (for ncu)."""
+    case_list = workloads.batched_sa(args.cases, seed=rank_seed(0)).items
+    mode = {'phases': _abi.LAUNCH_PHASES, 'split': _abi.LAUNCH_SPLIT,
+            'tiled': _abi.LAUNCH_TILED}.get(args.profile, _abi.LAUNCH_PERSISTENT)
+    b = new_batch(case_list, args.precision, local, args.block, 0, mode)
+    admit_all(b, case_list)
+    done = 0
+    while done < args.warmup:
+        k = min(32, args.warmup - done)
+        b.advance(k)
+        done += k
+    done, sec = 0, 0.0
+    while done < args.steps:
+        k = min(32, args.steps - done)
+        b.advance(k)
+        sec += b.last_advance_seconds
+        done += k
+    print(json.dumps(dict(profile=args.profile, cases=len(case_list), precision=args.precision, block=args.block,
+                          launch=b.launch_config(), ms_per_step=1e3 * sec / max(1, args.steps))))
 
 
 def main():
@@ -393,101 +613,102 @@ def main():
     ap.add_argument('--steps', type=int, default=320)
     ap.add_argument('--warmup', type=int, default=64)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--workload', default='batched', choices=['batched', 'accuracy', 'time-accurate', 'serve'])
     ap.add_argument('--cases', type=int, default=256)
     ap.add_argument('--no-cpu', action='store_true')
+    ap.add_argument('--no-solve', action='store_true', help='skip the measured full-solve leg')
     ap.add_argument('--profile', choices=['persistent', 'phases', 'split', 'tiled'], default=None,
                     help='only the timed batched loop, with this launch mode and --block (for ncu)')
     ap.add_argument('--block', type=int, default=128)
     ap.add_argument('--precision', type=int, default=32, choices=[32, 64])
-    ap.add_argument('--serve', action='store_true', help='the served form: Poisson arrivals, p50/p99 latency')
+    ap.add_argument('--serve', action='store_true', help='same as --workload serve')
     ap.add_argument('--requests', type=int, default=200)
     ap.add_argument('--rate', type=float, default=50.0)
     ap.add_argument('--max-steps', type=int, default=3000)
     ap.add_argument('--serve-cases', type=int, default=512)
-    ap.add_argument('--seed', type=int, default=20261203)
+    ap.add_argument('--seed', type=int, default=workloads.SEED)
+    ap.add_argument('--accuracy-steps', type=int, default=20000)
+    ap.add_argument('--ta-cases', type=int, default=128)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank, world, local = dist_setup(args.gpus)
     if args.impl == 'reference':
         reference_arm(args, rank, world)
         return
-    if args.serve:
+    if args.serve or args.workload == 'serve':
         run_serving(args, rank, world, local)
         return
-    case_list = batched_cases(args.cases, seed=20261203 + rank)
-    if args.profile:
-        mode = {'phases': _abi.LAUNCH_PHASES, 'split': _abi.LAUNCH_SPLIT,
-                'tiled': _abi.LAUNCH_TILED}.get(args.profile, _abi.LAUNCH_PERSISTENT)
-        b = Batch(precision=args.precision, model=_abi.MODEL_LAMINAR, sa=True, max_cases=len(case_list),
-                  max_cells=sum(m.n_cells for _, m in case_list) + 64, device=local, block_threads=args.block,
-                  launch_mode=mode)
-        for spec, mesh in case_list:
-            b.admit(mesh, spec.params(), cases.initial_state(mesh, spec.initial_primitive()),
-                    case_control(1e30, 10 ** 9, steady=False))
-        done = 0
-        while done < args.warmup:
-            k = min(32, args.warmup - done)
-            b.advance(k)
-            done += k
-        done, sec = 0, 0.0
-        while done < args.steps:
-            k = min(32, args.steps - done)
-            b.advance(k)
-            sec += b.last_advance_seconds
-            done += k
-        print(json.dumps(dict(profile=args.profile, cases=len(case_list), precision=args.precision, block=args.block,
-                              launch=b.launch_config(), ms_per_step=1e3 * sec / max(1, args.steps))))
+    if args.workload == 'accuracy':
+        if rank == 0:
+            accuracy_leg(args)
         return
+    if args.workload == 'time-accurate':
+        if rank == 0:
+            time_accurate_leg(args)
+        return
+    if args.profile:
+        profile_leg(args, local)
+        return
+    work = workloads.batched_sa(args.cases, seed=rank_seed(rank))
+    case_list = work.items
     hbm, peak_kind = peaks()
     dist_barrier(world)
-    clk = ClockSampler(local, interval_ms=50)
-    r = run_batched(case_list, 32, args.steps, args.warmup, device=local, clock=clk)
+    clk = ClockSampler(local, interval_ms=100)
+    clk.__enter__()
+    r = run_batched(case_list, 32, args.steps, args.warmup, device=local)
     dev_seconds = dist_max(r['dev_seconds'], world)
-    cell_steps = r['cell_steps']
-    value = cell_steps * world / dev_seconds
+    cell_steps = dist_sum(r['cell_steps'], world)
+    value = cell_steps / dev_seconds
     cfg = r['config']
     block, grid, mode = parse_launch(cfg)
+    solve = None if args.no_solve else run_solve(case_list, SOLVE_STEPS, local, block, grid, mode)
+    clk.__exit__(None, None, None)
     # the device-timed batch is freed after the end-to-end run, so that its teardown in the driver
     # does not overlap (and slow) the end-to-end run's own batch creation
     e2e = run_e2e(case_list, 32, args.steps, device=local, block=block, grid=grid, mode=mode)
     r.pop('batch').destroy()
-    e2e_value = e2e['value'] * world
-    # roofline of the persistent kernel: algorithmic bytes per launch / launch duration
+    e2e_value = dist_sum(e2e['value'], world)
+    # roofline of the step: algorithmic bytes per launch / launch duration (CUDA events)
     bytes_per_step = sum(algorithmic_bytes(m) for _, m in case_list)
     per_launch = r['dev_seconds'] / r['advances']
-    achieved = bytes_per_step * (args.steps / r['advances']) / per_launch / 1e9
-    mean_cells = sum(m.n_cells for _, m in case_list) / len(case_list)
+    steps_per_launch = args.steps / r['advances']
+    achieved = bytes_per_step * steps_per_launch / per_launch / 1e9
+    traffic = (SPLIT_256_TRAFFIC_PER_STEP * steps_per_launch
+               if SPLIT_256_TRAFFIC_PER_STEP and 'mode=split' in cfg and args.cases == 256 else None)
+    desc = work.describe()
     line = dict(metric=METRIC, value=value, unit='cell-steps/s', n_gpus=world, steps=args.steps, warmup=args.warmup,
                 ms_per_step=1e3 * dev_seconds / args.steps, higher_is_better=True, scaling='weak', vs_baseline=None,
                 dtype='f32', data='synthetic',
-                config=dict(workload='batched-sa-fp32-256', cases=args.cases * world,
-                            meshes='NACA 2412 LF1 (%d cells) / LF2 (%d cells), 1:1, replicated with seeded M~U[1.2,2], '
-                                   'AoA~U[-3,5]' % (case_list[0][1].n_cells, case_list[1][1].n_cells),
-                            cells=sum(m.n_cells for _, m in case_list), solve_steps=SOLVE_STEPS,
-                            solves_per_s=value / mean_cells / SOLVE_STEPS,
+                config=dict(workload=desc['workload'], cases=args.cases * world, cells=desc['cells'],
+                            profiles=desc['profiles'], seed=desc['seed'], redraws=desc['redraws'],
+                            meshes='seeded NACA 4-digit draws m~U[0,0.06] p~U[0.2,0.6] t~U[0.08,0.15], LF1:LF2 1:1, '
+                                   'M~U[1.2,2], AoA~U[-3,5], SA-neg + Sutherland, HLLC, native mesh builder',
+                            solve_steps=SOLVE_STEPS,
                             l2='working set > L2 (no flush needed)', launch=cfg, parallelism='replicas'),
                 roofline=dict(bound='hbm', achieved=achieved, peak=hbm, unit='GB/s', frac=achieved / hbm,
-                              peak_kind=peak_kind,
-                              traffic=(SPLIT_256_TRAFFIC_PER_STEP * args.steps / r['advances']
-                                       if 'mode=split' in cfg and args.cases == 256 else None),
-                              traffic_scope='DRAM bytes per launch (a graph of steps_per_launch steps), ncu, cold cache',
-                              bytes_per_step=bytes_per_step,
-                              launch_ms=1e3 * per_launch, steps_per_launch=args.steps / r['advances']),
+                              peak_kind=peak_kind, traffic=traffic,
+                              traffic_source=TRAFFIC_SOURCE if traffic else None,
+                              bytes_per_step=bytes_per_step, launch_ms=1e3 * per_launch,
+                              steps_per_launch=steps_per_launch),
                 e2e=dict(value=e2e_value, unit='cell-steps/s', h2d_bytes_per_step=e2e['h2d'] / args.steps,
                          d2h_bytes_per_step=e2e['d2h'] / args.steps, seconds=e2e['seconds'],
                          phases_seconds=e2e['phases']),
-                gpu_launches=r['launches'], clocks=clk.summary(),
+                gpu_launches=r['launches'], clocks=r['nvml'], clocks_under_load=clk.summary(),
                 rejected=sum(st['rejected'] for st in r['status']))
+    if solve is not None:
+        line['solve'] = dict(solve, note='measured: every case run from its freestream start to %d steps' % SOLVE_STEPS)
+        line['config']['solves_per_s'] = solve['solves_per_s']
     if rank == 0:
         plain = plain_fp64(case_list, 256)
         pv = sum(p['cells'] * p['steps'] for p in plain.values()) / sum(p['seconds'] for p in plain.values())
         line['plain_fp64'] = dict(cell_steps_per_s=pv, per_profile=plain, batched_over_plain=value / world / pv)
         if not args.no_cpu:
             threads = os.cpu_count() or 1
-            cv, detail = cpu_reference(case_list, 400, 200, threads)
+            cv, detail = cpu_reference(400, 200, threads, rank_seed(0))
             line['cpu_baseline'] = dict(value=cv, unit='cell-steps/s', cores=threads, kind='reference',
-                                        sample='1 LF1 x 400 steps + 1 LF2 x 200 steps of the workload (reference CPU '
-                                               'core, OpenMP)', cpu=cpu_model(), detail=detail)
+                                        sample='first LF1 draw x 400 steps + first LF2 draw x 200 steps of the workload '
+                                               '(reference CPU core, OpenMP)', cpu=cpu_model(), detail=detail)
+            line['config1'] = config1_leg()
         print(json.dumps(line), flush=True)
     dist_barrier(world)
 

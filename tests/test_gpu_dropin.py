@@ -31,13 +31,13 @@ def write_inputs(golden, folder, mode, backend, profile='LF1'):
     (folder / 'patches.csv').write_text('edge,patch\n' + ''.join(f'{j},{int(p)}\n' for j, p in enumerate(z['patches'][a:b])))
 
 
-def run(golden, tmp_path, mode, backend):
-    folder = tmp_path / f'{mode}_{backend}'
+def run(golden, tmp_path, mode, backend, profile='LF1'):
+    folder = tmp_path / f'{mode}_{backend}_{profile}'
     (folder / 'internal').mkdir(parents=True)
-    write_inputs(golden, folder, mode, backend)
+    write_inputs(golden, folder, mode, backend, profile)
     cmd = [str(BIN), '--settings', str(folder / 'settings.txt'), '--geometry', str(folder / 'airfoil.csv'),
            '--patches', str(folder / 'patches.csv'), '--out', str(folder / 'internal' / 'flow')]
-    p = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
+    p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
     assert p.returncode == 0, p.stdout + p.stderr
     return json.loads((folder / 'internal' / 'flow.result.json').read_text())
 
