@@ -309,7 +309,9 @@ typedef struct amr_batch amr_batch;
 
 int amr_batch_create(const amr_batch_config_t* config, amr_batch** out, char* error, uint64_t error_size);
 /* Admits one case; *slot receives its id.  Returns 3 (no room) when the arena lacks cells,
- * faces, walls, terms or case slots for it. */
+ * faces, walls, terms or case slots for it.  u0 holds nv*n_cells values (SoA), or nv values for a
+ * uniform start (the reference's static_amr2d_initialize from freestream primitives,
+ * src/static_amr2d.cpp:360-367, in conserved form), which the device fills itself. */
 int amr_batch_admit(amr_batch* batch, const amr_mesh_view_t* mesh, const amr_params_t* params,
                     const double* u0, uint64_t u0_count, const amr_case_control_t* control,
                     int32_t* slot, char* error, uint64_t error_size);
@@ -328,6 +330,17 @@ int amr_batch_admit_many(amr_batch* batch, uint64_t count, const amr_mesh_view_t
 /* Runs `trials` trials of every live case (one persistent launch, replayed from a CUDA
  * graph that is recaptured when the case set changes), then refreshes host-side status. */
 int amr_batch_advance(amr_batch* batch, int32_t trials, char* error, uint64_t error_size);
+/* amr_batch_advance in two halves: the first enqueues the trials on the batch's stream and returns
+ * at once, the second waits for them and refreshes the host-side statuses.  One host thread can so
+ * keep several batches' trials in flight together (each batch has its own stream).  Make no other
+ * call on a batch between its two halves.  No counterpart in the reference. */
+int amr_batch_advance_async(amr_batch* batch, int32_t trials, char* error, uint64_t error_size);
+int amr_batch_wait(amr_batch* batch, char* error, uint64_t error_size);
+/* Device bytes a batch allocated (arena, state, scratch and records). */
+uint64_t amr_batch_device_bytes(const amr_batch* batch);
+/* Free and total memory of CUDA device `device` (cudaMemGetInfo), for admission by free device
+ * memory.  Returns 0, or 1 when the device cannot be queried.  No counterpart in the reference. */
+int amr_device_memory(int32_t device, uint64_t* free_bytes, uint64_t* total_bytes);
 /* Evaluates the steady criteria for every live case whose next check time has been reached. */
 int amr_batch_check(amr_batch* batch, char* error, uint64_t error_size);
 int amr_batch_status(const amr_batch* batch, int32_t slot, amr_case_status_t* out);

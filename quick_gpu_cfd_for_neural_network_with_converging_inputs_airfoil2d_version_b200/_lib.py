@@ -27,6 +27,10 @@ SIGNATURES = {
     'amr_batch_admit': (C.c_int, [_P, _P, _P, _P, C.c_uint64, _P, _P, _S, C.c_uint64]),
     'amr_batch_admit_many': (C.c_int, [_P, C.c_uint64, _P, _P, _P, _P, _P, C.c_int32, _P, _P, _S, C.c_uint64]),
     'amr_batch_advance': (C.c_int, [_P, C.c_int32, _S, C.c_uint64]),
+    'amr_batch_advance_async': (C.c_int, [_P, C.c_int32, _S, C.c_uint64]),
+    'amr_batch_wait': (C.c_int, [_P, _S, C.c_uint64]),
+    'amr_batch_device_bytes': (C.c_uint64, [_P]),
+    'amr_device_memory': (C.c_int, [C.c_int32, _P, _P]),
     'amr_batch_check': (C.c_int, [_P, _S, C.c_uint64]),
     'amr_batch_status': (C.c_int, [_P, C.c_int32, _P]),
     'amr_batch_download': (C.c_int, [_P, C.c_int32, _P, C.c_uint64, _S, C.c_uint64]),

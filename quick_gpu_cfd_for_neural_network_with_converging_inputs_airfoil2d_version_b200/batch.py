@@ -16,6 +16,14 @@ class BatchError(RuntimeError):
     pass
 
 
+def device_memory(device=0):
+    """(free, total) bytes of device memory (cudaMemGetInfo)."""
+    free, total = C.c_uint64(), C.c_uint64()
+    if lib().amr_device_memory(int(device), C.byref(free), C.byref(total)):
+        raise BatchError(f'cannot query device {device}')
+    return free.value, total.value
+
+
 def case_control(tend, maxsteps, steady=True, mach=1.65, aoa=1.5, **kw):
     c = _abi.CaseControl()
     s = dict(cases.STEADY)
@@ -50,6 +58,9 @@ class Batch:
         self.ncells = {}
 
     def admit(self, mesh, params, u0, control):
+        """Admits one case; u0 is the SoA start state (nv * n_cells values) or, for a uniform start,
+        the nv conserved values (cases.uniform_state), which the device fills in.  Returns the slot,
+        or None when the arena has no room."""
         u0 = np.ascontiguousarray(u0, dtype=np.float64)
         view = mesh.view()
         slot = C.c_int32(-1)
@@ -101,6 +112,18 @@ class Batch:
     def advance(self, trials=32):
         err = errbuf()
         if lib().amr_batch_advance(self._h, int(trials), err, len(err)):
+            raise BatchError(err.value.decode())
+
+    def advance_async(self, trials=32):
+        """Enqueues `trials` trials and returns at once; wait() completes them.  Make no other call
+        on the batch in between."""
+        err = errbuf()
+        if lib().amr_batch_advance_async(self._h, int(trials), err, len(err)):
+            raise BatchError(err.value.decode())
+
+    def wait(self):
+        err = errbuf()
+        if lib().amr_batch_wait(self._h, err, len(err)):
             raise BatchError(err.value.decode())
 
     def check(self):
@@ -155,6 +178,11 @@ class Batch:
         b = errbuf(128)
         lib().amr_batch_launch_config(self._h, b, len(b))
         return b.value.decode()
+
+    @property
+    def device_bytes(self):
+        """Device memory the batch allocated."""
+        return lib().amr_batch_device_bytes(self._h)
 
     @property
     def live(self):

@@ -149,6 +149,16 @@ class CaseSpec:
         return freestream(self.mach, self.aoa, gamma)
 
 
+def uniform_state(mesh, w, gamma=1.4):
+    """The nv conserved values of a uniform start from primitives w = (rho, u, v, p): the values
+    initial_state repeats over the cells.  A batch given these nv values fills the state on the
+    device (no per-cell upload)."""
+    values = [w[0], w[0] * w[1], w[0] * w[2], w[3] / (gamma - 1) + 0.5 * w[0] * (w[1] * w[1] + w[2] * w[2])]
+    if mesh.nv == 5:
+        values.append(w[0] * float(mesh.transport['sa_nu_inf'][0]))
+    return np.array(values, dtype=np.float64)
+
+
 def initial_state(mesh, w, gamma=1.4):
     """Uniform conserved state from primitives w = (rho, u, v, p), SoA u[var*n + cell]
     (the reference's static_amr2d_initialize, src/static_amr2d.cpp:360-367)."""

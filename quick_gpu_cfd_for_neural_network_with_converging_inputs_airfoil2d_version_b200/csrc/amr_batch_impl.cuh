@@ -185,6 +185,21 @@ struct UploadTable {
   int n;
 };
 
+// A uniform start state on the device: every cell of a case's range [c0, c0 + n) gets the
+// conserved values hi[v] (and, in the FP32 form, the trailing words lo[v]); the case's padding
+// cell c0 + n gets 1 and 0, as a staged state does.
+template <class R> struct UniformState {
+  R hi[5], lo[5];
+};
+template <class R>
+static __global__ void fill_uniform_kernel(R* U, R* L, long long cap, int c0, int n, int nv, UniformState<R> w) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= n; k += gridDim.x * blockDim.x)
+    for (int v = 0; v < nv; ++v) {
+      U[v * cap + c0 + k] = k < n ? w.hi[v] : R(1);
+      if (L) L[v * cap + c0 + k] = k < n ? w.lo[v] : R(0);
+    }
+}
+
 // blockIdx.y picks the table; the copy width is the widest of 8, 4 or 1 bytes that divides
 // both addresses and the size.
 static __global__ void scatter_uploads_kernel(const unsigned char* __restrict__ stage, UploadTable t) {
@@ -320,6 +335,11 @@ template <class R> class Batch final : public BatchBase {
               diag_cfg_.alloc(7 * c.max_cases, A, error, "diag") && case_tiles_.alloc(2 * c.max_cases, A, error, "diag") &&
               ddt_.alloc(2 * nc, A, error, "diag");
     if (!ok) return false;
+    if (sizeof(R) == 4 && !(L0_.alloc(nv_ * nc, A, error, "state") && L1_.alloc(nv_ * nc, A, error, "state")))
+      return false;
+    if (sizeof(R) == 4 && model_ == MODEL_SA &&
+        !(fsa_.alloc(cap_faces_, A, error, "faces") && wsa_.alloc(cap_walls_, A, error, "walls")))
+      return false;
     if (!s_geo_.alloc(slot_fluxes_ ? 6 * cap_slots_ : 0, A, error, "slots")) return false;
     // face and wall records of the split launch mode
     ok = s_item_.alloc(cap_slots_, A, error, "slots") && f_case_.alloc(cap_faces_, A, error, "faces") &&
@@ -999,11 +1019,24 @@ template <class R> class Batch final : public BatchBase {
     cf.srd_rate = viscous && m->transport.stabilization == AMR_B200_VISCOUS_SRD && m->small_cells > 0 && cf.has_srd;
     cf.cell0 = cb;
     cf.cell1 = cb + (int)n;
-    // state (variable-major, each variable's n cells then the padding cell)
-    PVec<R> u = pvu<R>(S, nv_ * (n + 1));
-    for (int v = 0; v < nv_; ++v) {
-      for (long long k = 0; k < n; ++k) u[v * (n + 1) + k] = (R)sp.u0[v * n + k];
-      u[v * (n + 1) + n] = R(1);
+    // state (variable-major, each variable's n cells then the padding cell).  A uniform start
+    // (u0 holds nv values) is not staged: a kernel fills it on the device after the uploads.
+    const bool uniform = uniform_start(sp.u0_count, n);
+    const long long sn = uniform ? 0 : n + 1;
+    PVec<R> u = pvu<R>(S, nv_ * sn);
+    // FP32 form: the trailing word holds what the leading word rounds off the FP64 start state
+    PVec<R> ulo = pvu<R>(S, sizeof(R) == 4 ? nv_ * sn : 0);
+    if (!uniform) {
+      for (int v = 0; v < nv_; ++v) {
+        for (long long k = 0; k < n; ++k) u[v * (n + 1) + k] = (R)sp.u0[v * n + k];
+        u[v * (n + 1) + n] = R(1);
+      }
+      if (sizeof(R) == 4)
+        for (int v = 0; v < nv_; ++v) {
+          for (long long k = 0; k < n; ++k)
+            ulo[v * (n + 1) + k] = (R)(sp.u0[v * n + k] - (double)u[v * (n + 1) + k]);
+          ulo[v * (n + 1) + n] = R(0);
+        }
     }
     // control
     CaseCtl& ctl = j.ctl;
@@ -1040,15 +1073,30 @@ template <class R> class Batch final : public BatchBase {
       ok = up(st, t_own_.p + tb, t_own, G) && up(st, t_src_.p + tb, t_src, G) && up(st, t_x_.p + tb, t_x, G) &&
            up(st, t_y_.p + tb, t_y, G);
     if (ok && model_ == MODEL_SA) ok = up(st, c_wd_.p + cb, c_wd, G);
-    for (int v = 0; ok && v < nv_; ++v) {
+    for (int v = 0; ok && !uniform && v < nv_; ++v) {
       ok = stage_up(st, U0_.p + v * cap_cells_ + cb, u.data() + v * (n + 1), sizeof(R) * (n + 1));
       j.state_bytes += sizeof(R) * (n + 1);
+      if (ok && L0_.p) {
+        ok = stage_up(st, L0_.p + v * cap_cells_ + cb, ulo.data() + v * (n + 1), sizeof(R) * (n + 1));
+        j.state_bytes += sizeof(R) * (n + 1);
+      }
     }
     CaseCfg<R>* cf_staged = static_cast<CaseCfg<R>*>(S.take(sizeof(cf)));
     *cf_staged = cf;
     ok = ok && stage_up(st, cfg_.p + slot, cf_staged, sizeof(cf));
     if (!ok) return job_fail(j, 1, "upload staging");
     if (!flush_uploads(st, &j.error)) return (void)(j.status = 1);
+    if (uniform) {
+      UniformState<R> w{};
+      for (int v = 0; v < nv_; ++v) {
+        w.hi[v] = (R)sp.u0[v];
+        w.lo[v] = (R)(sp.u0[v] - (double)w.hi[v]);
+      }
+      const int blocks = (int)std::min<long long>((n + 256) / 256, 1024);
+      fill_uniform_kernel<R><<<blocks, 256, 0, stream_>>>(U0_.p, L0_.p, cap_cells_, cb, (int)n, nv_, w);
+      if (!cuda_ok(cudaGetLastError(), &j.error, "uniform start")) return (void)(j.status = 1);
+      j.state_bytes += sizeof(w);
+    }
     if (!st.done && !cuda_ok(cudaEventCreateWithFlags(&st.done, cudaEventDisableTiming), &j.error, "staging event"))
       return (void)(j.status = 1);
     if (!cuda_ok(cudaEventRecord(st.done, stream_), &j.error, "staging event")) return (void)(j.status = 1);
@@ -1132,6 +1180,15 @@ template <class R> class Batch final : public BatchBase {
   }
 
   int advance(int trials, std::string* error) override {
+    const int rc = advance_begin(trials, error);
+    return rc ? rc : advance_end(error);
+  }
+
+  // First half of advance: everything up to the stream synchronisation (capture or replay of the
+  // trials' graph, with the control read-back at its end), so that several batches can have
+  // their trials in flight at once.  advance_end waits and refreshes the host-side statuses.
+  int advance_begin(int trials, std::string* error) override {
+    if (in_flight_) return fail1(error, "an advance is already in flight");
     if (trials < 1 || trials > 1024) return fail1(error, "trials must be 1..1024");
     if (live_ == 0) return 0;
     if (!sync_tiles(error)) return 1;
@@ -1150,7 +1207,20 @@ template <class R> class Batch final : public BatchBase {
     } else {
       ok = enqueue(trials, MODE_TRIALS, error);
     }
-    ok = ok && cuda_ok(cudaStreamSynchronize(stream_), error, "advance");
+    if (!ok) {
+      cudaStreamSynchronize(stream_);
+      return 1;
+    }
+    in_flight_ = true;
+    in_flight_trials_ = trials;
+    return 0;
+  }
+
+  int advance_end(std::string* error) override {
+    if (!in_flight_) return 0;
+    in_flight_ = false;
+    const int trials = in_flight_trials_;
+    const bool ok = cuda_ok(cudaStreamSynchronize(stream_), error, "advance");
     launches_ += kernels_per_advance(trials);
     stats_.status_polls += 1;
     stats_.control_d2h_bytes += sizeof(CaseCtl) * config_.max_cases;
@@ -1199,7 +1269,13 @@ template <class R> class Batch final : public BatchBase {
 
   int download(int slot, double* u, uint64_t count, std::string* error) override {
     if (slot < 0 || slot >= config_.max_cases || !cases_[slot].live) return fail1(error, "no such case");
-    const int ok = copy_out(h_ctl_[slot].cur ? U1_.p : U0_.p, slot, u, count, error);
+    const int cur = h_ctl_[slot].cur;
+    int ok = copy_out(cur ? U1_.p : U0_.p, slot, u, count, error);
+    if (ok == 0 && L0_.p) {  // FP32 form: the value is the leading plus the trailing word
+      std::vector<double> lo(count);
+      ok = copy_out(cur ? L1_.p : L0_.p, slot, lo.data(), count, error);
+      for (uint64_t i = 0; ok == 0 && i < count; ++i) u[i] += lo[i];
+    }
     if (ok == 0) {
       stats_.state_d2h_bytes += sizeof(R) * count;
       stats_.full_downloads += 1;
@@ -1328,6 +1404,9 @@ template <class R> class Batch final : public BatchBase {
     return 0;
   }
 
+  // A start state of nv values (rather than nv per cell) is the same state in every cell.
+  bool uniform_start(uint64_t u0_count, long long n) const { return n > 1 && u0_count == (uint64_t)nv_; }
+
   bool validate(const amr_mesh_view_t& m, const amr_params_t& p, uint64_t u0_count, std::string* why) const {
     const auto finite = [](double x) { return std::isfinite(x); };
     if (m.n_cells == 0 || m.n_faces == 0 || !m.cells || !m.faces || !m.face_offsets || !m.cell_faces)
@@ -1339,7 +1418,8 @@ template <class R> class Batch final : public BatchBase {
     if (model != model_) return fail(why, "flow model differs from the batch's");
     const int flux = p.flux == AMR_B200_FLUX_AUSMPUP ? FLUX_AUSM : FLUX_HLLC;
     if (flux != flux_ && model_ >= 0) return fail(why, "numerical flux differs from the batch's");
-    if (u0_count != (uint64_t)(nv_ * m.n_cells)) return fail(why, "initial state size mismatch");
+    if (u0_count != (uint64_t)(nv_ * m.n_cells) && !uniform_start(u0_count, (long long)m.n_cells))
+      return fail(why, "initial state size mismatch");
     if (p.limiter != AMR_B200_LIMITER_FIRST_ORDER || p.time_integrator != AMR_B200_TIME_SSP_RK3 || !finite(p.gamma) ||
         !(p.gamma > 1) || !(p.cfl > 0) || p.cfl > .5 || !finite(p.dt_fixed) || p.dt_fixed < 0 || !finite(p.ausm_mco) ||
         p.ausm_mco <= 0 || (p.flux != AMR_B200_FLUX_HLLC && p.flux != AMR_B200_FLUX_AUSMPUP))
@@ -1665,6 +1745,8 @@ template <class R> class Batch final : public BatchBase {
     d.U0 = U0_.p;
     d.U1 = U1_.p;
     d.U2 = U2_.p;
+    d.L0 = L0_.p;
+    d.L1 = L1_.p;
     d.R0 = R0_.p;
     d.grad = grad_.p;
     d.mu = mu_.p;
@@ -1682,6 +1764,8 @@ template <class R> class Batch final : public BatchBase {
     d.w_owner = w_owner_.p;
     d.s_item = s_item_.p;
     d.fval = fval_.p;
+    d.fsa = fsa_.p;
+    d.wsa = wsa_.p;
     d.wval = wval_.p;
     d.crec = crec_.p;
     d.ddt = ddt_.p;
@@ -1841,13 +1925,15 @@ template <class R> class Batch final : public BatchBase {
     t_own_.free(); t_src_.free(); t_x_.free(); t_y_.free();
     g_mem_.free(); g_cell_.free(); g_cnt_.free(); g_vol_.free(); q_cell_.free(); q_grp_.free(); q_list_.free(); q_cnt_.free();
     qhat_.free();
-    U0_.free(); U1_.free(); U2_.free(); R0_.free(); grad_.free(); mu_.free(); eddy_.free(); sgrad_.free(); sdiff_.free();
+    U0_.free(); U1_.free(); U2_.free(); R0_.free(); L0_.free(); L1_.free(); fsa_.free(); wsa_.free(); grad_.free(); mu_.free(); eddy_.free(); sgrad_.free(); sdiff_.free();
     ssrc_.free(); srate_.free(); diag_part_.free(); diag_out_.free(); diag_cfg_.free(); case_tiles_.free();
   }
 
   amr_batch_config_t config_{};
   int model_ = 0, flux_ = 0, nv_ = 4, sms_ = 148, clock_khz_ = 1965000;
   int block_ = 256, grid_ = 0, max_grid_ = 0, grid_request_ = 0;
+  bool in_flight_ = false;  // an advance_begin awaits its advance_end
+  int in_flight_trials_ = 0;
   int mode_ = AMR_B200_LAUNCH_PERSISTENT;  // persistent cooperative kernel, one kernel per phase, or split
   long long hw_cells_ = 0, hw_faces_ = 0, hw_walls_ = 0;
   int h_live_end_[4] = {0, 0, 0, 0};
@@ -1899,6 +1985,8 @@ template <class R> class Batch final : public BatchBase {
   DevBuf<int> g_mem_, g_cell_, q_cell_, q_grp_, q_list_;
   DevBuf<double> g_cnt_, g_vol_, q_cnt_, qhat_;
   DevBuf<R> U0_, U1_, U2_, R0_, grad_, mu_, eddy_, sgrad_, sdiff_, ssrc_, srate_;
+  DevBuf<R> L0_, L1_;  // FP32 form: trailing words of U0_ / U1_ (not allocated in FP64)
+  DevBuf<R> fsa_, wsa_;  // compact FP32 SA records: the SA flux column per face and wall record
   DevBuf<double> diag_part_, diag_out_, diag_cfg_, ddt_, ex_buf_;
   DevBuf<int> case_tiles_;
   std::vector<std::unique_ptr<Stager>> stagers_;  // two per admission worker; the first also serves downloads

@@ -358,6 +358,41 @@ int amr_batch_advance(amr_batch* b, int32_t trials, char* error, uint64_t error_
   return 0;
 }
 
+int amr_batch_advance_async(amr_batch* b, int32_t trials, char* error, uint64_t error_size) {
+  if (!b) return 1;
+  std::string err;
+  if (b->batch->advance_begin(trials, &err)) {
+    put(error, error_size, err);
+    return 1;
+  }
+  return 0;
+}
+
+int amr_batch_wait(amr_batch* b, char* error, uint64_t error_size) {
+  if (!b) return 1;
+  std::string err;
+  if (b->batch->advance_end(&err)) {
+    put(error, error_size, err);
+    return 1;
+  }
+  return 0;
+}
+
+uint64_t amr_batch_device_bytes(const amr_batch* b) { return b ? b->batch->stats().allocated_bytes : 0; }
+
+int amr_device_memory(int32_t device, uint64_t* free_bytes, uint64_t* total_bytes) {
+  if (!free_bytes || !total_bytes) return 1;
+  int previous = 0;
+  if (cudaGetDevice(&previous) != cudaSuccess || cudaSetDevice(device) != cudaSuccess) return 1;
+  size_t f = 0, t = 0;
+  const cudaError_t st = cudaMemGetInfo(&f, &t);
+  cudaSetDevice(previous);
+  if (st != cudaSuccess) return 1;
+  *free_bytes = f;
+  *total_bytes = t;
+  return 0;
+}
+
 // Steady rule of the reference driver: residual norms over the region and the load changes
 // must stay within tolerance for `hold` consecutive checks once time >= min_time.
 int amr_batch_check(amr_batch* b, char* error, uint64_t error_size) {

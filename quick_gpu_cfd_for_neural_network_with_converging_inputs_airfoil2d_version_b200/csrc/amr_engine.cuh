@@ -84,6 +84,14 @@ constexpr int SLOT_WALL = 1 << 9;  // s_meta flag: the slot is a wall fragment o
 constexpr int TILE_W = 32;
 constexpr int SM_COLS = 12;  // values per slot (shared-memory columns, face and wall records)
 constexpr int CREC = 16;     // values in a packed cell record
+// The split mode's global cell records.  FP32 viscous models store 12 values (48 bytes): state 0-4,
+// gradient 5-8, SA phi gradient 9-10; the face kernel recomputes viscosity, eddy viscosity and the
+// SA diffusion coefficient from the state (cell_transport), with the gradient kernel's expressions.
+// FP64 keeps the full CREC layout (and the tiled mode's shared-memory records always do).
+template <class R, int MODEL> struct CellRec {
+  static constexpr bool compact = sizeof(R) == 4 && MODEL >= 1;
+  static constexpr int stride = compact ? 12 : CREC;
+};
 constexpr unsigned FULL_MASK = 0xffffffffu;
 
 struct GridBarrier {
@@ -141,6 +149,10 @@ template <class R> struct Dev {
   R* U2;
   R* R0;
   R* Rr;
+  // FP32 form: trailing words of the accepted state buffers U0 / U1 (null in FP64).  The value
+  // of a variable is U + L; fluxes read U alone, the final stage of a step updates both.
+  R* L0;
+  R* L1;
   R* grad;
   R* mu;
   R* eddy;
@@ -161,6 +173,8 @@ template <class R> struct Dev {
   const int* s_item;
   R* fval;          // per face: 12 values, 8 in the compact FP32 viscous format (RecFormat)
   R* wval;          // per wall: the same
+  R* fsa;           // compact FP32 SA format: the SA flux per face record (column 10)
+  R* wsa;           // and per wall record
   R* crec;          // CREC per cell: packed state and gradient-phase fields (viscous models)
   // tiled mode
   const BTile* btiles;
@@ -356,7 +370,8 @@ template <class R, int MODEL> __device__ __forceinline__ void load_cell_record(c
 // SA diffusion 13.
 template <class R, int MODEL, class In>
 __device__ __forceinline__ bool grad_finish(const Dev<R>& d, const CaseCfg<R>& cf, int k, const In& Uin, const R* gr,
-                                            const R* sg, bool soa = true, R* rec = nullptr, bool src_out = true) {
+                                            const R* sg, bool soa = true, R* rec = nullptr, bool src_out = true,
+                                            bool compact_rec = false) {
   const long long n = d.ncap;
   const Prim<R> w = prim(Uin, n, k, cf.gamma);
   const R mu = dyn_visc(cf.trn, w.p / (w.rho * cf.trn.gas_constant));
@@ -396,7 +411,16 @@ __device__ __forceinline__ bool grad_finish(const Dev<R>& d, const CaseCfg<R>& c
     c[12] = MODEL == MODEL_SA ? sg[1] : R(0);
     c[13] = sdiff;
     c[14] = c[15] = R(0);
-    store_cell_record<R, MODEL>(rec, c);
+    if (compact_rec) {  // CellRec compact layout: the SA phi gradient follows the gradient
+      c[9] = c[11];
+      c[10] = c[12];
+      c[11] = R(0);
+      store_group(rec, c);
+      store_group(rec + 4, c + 4);
+      store_group(rec + 8, c + 8);
+    } else {
+      store_cell_record<R, MODEL>(rec, c);
+    }
   }
   return !bad;
 }
@@ -499,11 +523,54 @@ __device__ __forceinline__ void face_in_soa(const Dev<R>& d, const R* gp, int k,
 }
 
 // Loads a FaceIn from the two cells' packed records (split mode, viscous models).
+// Viscosity, eddy viscosity and SA diffusion coefficient of a cell from its conserved state c[0..4],
+// by grad_finish's expressions (prim, dyn_visc, sa_eddy and sa_neg's diffusion), for the compact
+// records that do not store them.
 template <class R, int MODEL>
-__device__ __forceinline__ void face_in_records(const Dev<R>& d, const R* gp, int k, int m, FaceIn<R>& f) {
+__device__ __forceinline__ void cell_transport(const CaseCfg<R>& cf, const R* c, R& mu, R& eddy, R& sdiff) {
+  const R rho = c[0], u = c[1] / rho, v = c[2] / rho;
+  const R p = (cf.gamma - R(1)) * (c[3] - R(0.5) * (c[1] * u + c[2] * v));
+  mu = dyn_visc(cf.trn, p / (rho * cf.trn.gas_constant));
+  eddy = R(0);
+  sdiff = R(0);
+  if (MODEL == MODEL_SA) {
+    const R ph = c[4] / rho, nu = mu / rho;
+    eddy = rho * sa_eddy(ph, nu);
+    if (ph < R(0)) {
+      const R chi = ph / nu, cube = chi * chi * chi;
+      const R fn = (R(16) + cube) / (R(16) - cube);
+      sdiff = (nu + ph * fn) / R(AMRB_SIG);
+    } else {
+      sdiff = (nu + ph) / R(AMRB_SIG);
+    }
+  }
+}
+
+template <class R, int MODEL>
+__device__ __forceinline__ void load_cell_rec(const Dev<R>& d, const CaseCfg<R>& cf, int k, R* a) {
+  constexpr int S = CellRec<R, MODEL>::stride;
+  if (CellRec<R, MODEL>::compact) {
+    const R* src = d.crec + S * (long long)k;
+    R c[12];
+    load_group(src, c);
+    load_group(src + 4, c + 4);
+    load_group(src + 8, c + 8);
+    for (int v = 0; v < 9; ++v) a[v] = c[v];
+    a[11] = c[9];
+    a[12] = c[10];
+    if (MODEL != MODEL_SA) a[4] = a[11] = a[12] = R(0);
+    cell_transport<R, MODEL>(cf, a, a[9], a[10], a[13]);
+  } else {
+    load_cell_record<R, MODEL>(d.crec + S * (long long)k, a);
+  }
+}
+
+template <class R, int MODEL>
+__device__ __forceinline__ void face_in_records(const Dev<R>& d, const CaseCfg<R>& cf, const R* gp, int k, int m,
+                                                FaceIn<R>& f) {
   R a[CREC], b[CREC];
-  load_cell_record<R, MODEL>(d.crec + CREC * (long long)k, a);
-  load_cell_record<R, MODEL>(d.crec + CREC * (long long)m, b);
+  load_cell_rec<R, MODEL>(d, cf, k, a);
+  load_cell_rec<R, MODEL>(d, cf, m, b);
   for (int v = 0; v < 5; ++v) { f.uk[v] = a[v]; f.um[v] = b[v]; }
   for (int v = 0; v < 4; ++v) { f.gk[v] = a[5 + v]; f.gm[v] = b[5 + v]; }
   f.mk = a[9]; f.mm = b[9]; f.ek = a[10]; f.em = b[10];
@@ -686,8 +753,8 @@ template <class R, int MODEL>
 __device__ __forceinline__ void slot_wall_records(const Dev<R>& d, const CaseCfg<R>& cf, R nx, R ny, R wdist, R wl, int k,
                                                   int dn, bool base, R* dst, int stride, bool& bad) {
   R a[CREC], b[CREC];
-  load_cell_record<R, MODEL>(d.crec + CREC * (long long)k, a);
-  load_cell_record<R, MODEL>(d.crec + CREC * (long long)dn, b);
+  load_cell_rec<R, MODEL>(d, cf, k, a);
+  load_cell_rec<R, MODEL>(d, cf, dn, b);
   WallIn<R> w;
   for (int v = 0; v < 4; ++v) w.uk[v] = a[v];
   for (int v = 0; v < 5; ++v) w.ud[v] = b[v];
@@ -729,6 +796,18 @@ __device__ __forceinline__ void wall_fluxes(const CaseCfg<R>& cf, const WallIn<R
   }
 }
 
+// Correctly rounded sums that the compiler neither contracts nor reorders, and Knuth's TwoSum:
+// s + e == a + b exactly, s the rounded sum.
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+template <class R> __device__ __forceinline__ void two_sum(R a, R b, R& s, R& e) {
+  s = add_rn(a, b);
+  const R bv = sub_rn(s, a);
+  e = add_rn(sub_rn(a, sub_rn(s, bv)), sub_rn(b, bv));
+}
+
 // The 12 values of one slot, returned by value so that they stay in registers.
 template <class R> struct Cols {
   R v[SM_COLS];
@@ -737,17 +816,16 @@ template <class R> struct Cols {
 // Per-cell end of the F phase: in-order sums of the cell's slot values (faces [a, e) in CSR order,
 // then walls [e, b)), residual, cell dt (base stage) and the stage update.  get(q, col) yields
 // the 12 values of slot q with the flux columns signed for cell k.  Returns the cell dt.
+template <class R, int MODEL, class In>
+__device__ __forceinline__ double finish_tail(const Dev<R>& d, const CaseCfg<R>& cf, int cs, int k, int stage,
+                                              const In& Uin, R* Ub, R* Un, const R* sum, const R* vs, R spectral, R vspec,
+                                              R snet, R sspec, bool& bad);
+
 template <class R, int MODEL, class Get, class In>
 __device__ __forceinline__ double finish_cell(const Dev<R>& d, const CaseCfg<R>& cf, int cs, int k, int stage, int a,
                                               int e, int b, const Get& get, const In& Uin, R* Ub, R* Un, bool& bad) {
-  const long long n = d.ncap;
-  const R g = cf.gamma;
   const bool base = stage == STAGE_BASE;
   const bool spec = base || stage == STAGE_DIAG;  // spectral sums wanted (dt, or the export's dt limits)
-  double cell_dt = __longlong_as_double(0x7FF0000000000000ll);
-  const double V = d.c_vol[k];
-  const Prim<R> wk = prim(Uin, n, k, g);
-  if (!prim_ok(Uin, n, k, wk)) bad = true;
   R sum[4] = {0, 0, 0, 0}, vs[4] = {0, 0, 0, 0}, spectral = 0, vspec = 0, snet = 0, sspec = 0;
   for (int q = a; q < b; ++q) {
     const bool wall = q >= e;
@@ -769,6 +847,22 @@ __device__ __forceinline__ double finish_cell(const Dev<R>& d, const CaseCfg<R>&
       if (spec) sspec += col[11];
     }
   }
+  return finish_tail<R, MODEL>(d, cf, cs, k, stage, Uin, Ub, Un, sum, vs, spectral, vspec, snet, sspec, bad);
+}
+
+// The end of a cell's F phase after its in-order slot sums: residual, cell dt (base stage) and
+// the stage update, or the residual and dt limits of the diagnostics pass.  Returns the cell dt.
+template <class R, int MODEL, class In>
+__device__ __forceinline__ double finish_tail(const Dev<R>& d, const CaseCfg<R>& cf, int cs, int k, int stage,
+                                              const In& Uin, R* Ub, R* Un, const R* sum, const R* vs, R spectral, R vspec,
+                                              R snet, R sspec, bool& bad) {
+  const long long n = d.ncap;
+  const R g = cf.gamma;
+  const bool base = stage == STAGE_BASE;
+  double cell_dt = __longlong_as_double(0x7FF0000000000000ll);
+  const double V = d.c_vol[k];
+  const Prim<R> wk = prim(Uin, n, k, g);
+  if (!prim_ok(Uin, n, k, wk)) bad = true;
   R res[5];
   for (int v = 0; v < 4; ++v) res[v] = (R)(-sum[v] / V);
   if (MODEL >= MODEL_LAMINAR) {
@@ -808,11 +902,37 @@ __device__ __forceinline__ double finish_cell(const Dev<R>& d, const CaseCfg<R>&
     const bool simple = cf.has_srd && (d.c_flags[k] & 1);
     const bool check = stage == STAGE_2 && (!cf.has_srd || simple);
     R out[5];
-    for (int v = 0; v < nv; ++v) {
-      if (stage == STAGE_1)
-        out[v] = R(0.75) * Ub[v * n + k] + R(0.25) * (Uin[v * n + k] + dt * res[v]);
-      else
-        out[v] = Ub[v * n + k] / R(3) + R(2.0 / 3) * (Uin[v * n + k] + dt * res[v]);
+    bool two_word = false;
+    if constexpr (sizeof(R) == 4) {
+      two_word = stage == STAGE_2 && d.L0 != nullptr;
+    }
+    if (two_word) {
+      // FP32 form, final stage: the accepted state is a two-word FP32 value (U leading, L
+      // trailing).  The update U+ = U/3 + 2/3 (U2 + dt R2) is formed as U + 2/3 ((U2 - U) + dt R2)
+      // and added to U + L with an error-free FP32 sum (Knuth's TwoSum), so increments below
+      // half an ulp of U accumulate in L instead of being rounded away; with only a leading
+      // word a case stalls short of its steady state once dt R falls below that size.
+      // Cases with SRD redistribute the final state afterwards and keep L = 0.
+      const R* Lb = Ub == d.U0 ? d.L0 : d.L1;
+      R* Ln = Un == d.U0 ? d.L0 : d.L1;
+      for (int v = 0; v < nv; ++v) {
+        const R ub = Ub[v * n + k];
+        if (cf.has_srd) {
+          out[v] = ub / R(3) + R(2.0 / 3) * (Uin[v * n + k] + dt * res[v]);
+          Ln[v * n + k] = R(0);
+          continue;
+        }
+        const R inc = R(2.0 / 3) * ((Uin[v * n + k] - ub) + dt * res[v]);
+        two_sum(ub, add_rn(inc, Lb[v * n + k]), out[v], Ln[v * n + k]);
+      }
+    }
+    if (!two_word) {
+      for (int v = 0; v < nv; ++v) {
+        if (stage == STAGE_1)
+          out[v] = R(0.75) * Ub[v * n + k] + R(0.25) * (Uin[v * n + k] + dt * res[v]);
+        else
+          out[v] = Ub[v * n + k] / R(3) + R(2.0 / 3) * (Uin[v * n + k] + dt * res[v]);
+      }
     }
     if (simple)
       for (int v = 0; v < 4; ++v) out[v] = srd_self(out[v], V, d.c_gvol[k]);
@@ -1374,7 +1494,11 @@ template <class R, int MODEL> struct RecFormat {
   static constexpr int stride = compact ? 8 : SM_COLS;
 };
 
-template <class R, int MODEL> __device__ __forceinline__ void store_item(R* dst, R* rec, bool base, bool wall) {
+// The compact record's SA flux (column 10) lives in a per-record array of its own (sa_dst /
+// sa_src), so that the stages after the first, which need no spectral columns, move 20 bytes per
+// record instead of 32.
+template <class R, int MODEL>
+__device__ __forceinline__ void store_item(R* dst, R* rec, bool base, bool wall, R* sa_dst = nullptr) {
   if (!RecFormat<R, MODEL>::compact) {
     store_record<R, MODEL>(dst, rec, base);
     return;
@@ -1388,12 +1512,13 @@ template <class R, int MODEL> __device__ __forceinline__ void store_item(R* dst,
     net[3] = rec[7];
   }
   store_group(dst, net);
-  if (base || MODEL == MODEL_SA) store_group(dst + 4, rec + 8);
+  if (MODEL == MODEL_SA) *sa_dst = rec[10];
+  if (base) store_group(dst + 4, rec + 8);
 }
 
 // The 12 columns of a stored item, flux columns multiplied by sg (the slot's orientation).
 template <class R, int MODEL>
-__device__ __forceinline__ void load_item(const R* src, R* col, bool base, bool wall, R sg) {
+__device__ __forceinline__ void load_item(const R* src, R* col, bool base, bool wall, R sg, const R* sa_src = nullptr) {
   for (int c = 0; c < SM_COLS; ++c) col[c] = R(0);
   if (!RecFormat<R, MODEL>::compact) {
     load_record<R, MODEL>(src, col, base);
@@ -1408,7 +1533,8 @@ __device__ __forceinline__ void load_item(const R* src, R* col, bool base, bool 
       col[7] = col[3];
       col[0] = col[3] = R(0);
     }
-    if (base || MODEL == MODEL_SA) load_group(src + 4, col + 8);
+    if (base) load_group(src + 4, col + 8);
+    if (MODEL == MODEL_SA) col[10] = __ldg(sa_src);
   }
   if (MODEL == MODEL_SA) col[10] = sg * col[10];
 }
@@ -1434,7 +1560,8 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::cell) grad_cells_ker
           for (int v = 0; v < 4; ++v) sg[v] += t[4 + v];
       }
       // the packed record feeds the item kernel; the SoA copies only the residual-mode loads
-      return grad_finish<R, MODEL>(d, cf, k, Uin, gr, sg, stage == STAGE_DIAG, d.crec + CREC * (long long)k);
+      return grad_finish<R, MODEL>(d, cf, k, Uin, gr, sg, stage == STAGE_DIAG,
+                                   d.crec + CellRec<R, MODEL>::stride * (long long)k, true, CellRec<R, MODEL>::compact);
     };
     const bool ok = d.fused_first && stage == STAGE_1
                         ? cell(FusedIn<R>{state_buf(d, c.cur), d.R0, (R)c.dt_trial})
@@ -1462,13 +1589,13 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::item) item_kernel(De
       const int own = __ldg(d.f_own + f), nb = __ldg(d.f_nb + f);
       if (MODEL >= MODEL_LAMINAR) {
         FaceIn<R> in;
-        face_in_records<R, MODEL>(d, d.f_geo + 6 * (long long)f, own, nb >= 0 ? nb : own, in);
+        face_in_records<R, MODEL>(d, d.cfg[cs], d.f_geo + 6 * (long long)f, own, nb >= 0 ? nb : own, in);
         face_fluxes<R, MODEL, FLUX>(d.cfg[cs], in, __ldg(d.f_len + f), nb, __ldg(d.f_meta + f), base, rec, 1, false, bad);
       } else {
         slot_face<R, MODEL, FLUX>(d, d.cfg[cs], d.f_geo + 6 * (long long)f, __ldg(d.f_len + f), own, nb,
                                   __ldg(d.f_meta + f), stage_input(d, stage, c.cur), base, rec, 1, false, bad);
       }
-      store_item<R, MODEL>(d.fval + RecFormat<R, MODEL>::stride * (long long)f, rec, base, false);
+      store_item<R, MODEL>(d.fval + RecFormat<R, MODEL>::stride * (long long)f, rec, base, false, d.fsa + f);
     } else {
       const int w = idx - nf;
       const int owner = d.w_owner[w];
@@ -1483,7 +1610,7 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::item) item_kernel(De
       else
         slot_wall<R, MODEL>(d, d.cfg[cs], __ldg(d.w_nx + w), __ldg(d.w_ny + w), __ldg(d.w_dist + w), __ldg(d.w_len + w),
                             owner, __ldg(d.w_donor + w), stage_input(d, stage, c.cur), base, rec, 1, bad);
-      store_item<R, MODEL>(d.wval + RecFormat<R, MODEL>::stride * (long long)w, rec, base, true);
+      store_item<R, MODEL>(d.wval + RecFormat<R, MODEL>::stride * (long long)w, rec, base, true, d.wsa + w);
     }
     if (bad && stage != STAGE_DIAG) atomicOr(&d.ctl[cs].bad, 1);
   }
@@ -1497,8 +1624,9 @@ template <class R, int MODEL> struct ItemSlots {
     const int id = __ldg(d->s_item + q);  // wall index, or 2 * face record + (cell is the face's left)
     constexpr int S = RecFormat<R, MODEL>::stride;
     const R* src = wall ? d->wval + S * (long long)id : d->fval + S * (long long)(id >> 1);
+    const R* sa = wall ? d->wsa + id : d->fsa + (id >> 1);
     Cols<R> o;
-    load_item<R, MODEL>(src, o.v, base, wall, (wall || (id & 1)) ? R(1) : R(-1));
+    load_item<R, MODEL>(src, o.v, base, wall, (wall || (id & 1)) ? R(1) : R(-1), sa);
     return o;
   }
 };

@@ -316,13 +316,20 @@ int Batch<R>::diagnostics(const std::vector<int>& slots, const std::vector<doubl
 template <class R> int Batch<R>::autotune(int trials, std::string* error) {
   if (live_ == 0) return 0;
   const long long nbytes = (long long)sizeof(R) * nv_ * cap_cells_;
+  // saved state buffers: leading words, then (FP32 form) the trailing words
+  const int words = L0_.p ? 2 : 1;
   DevBuf<R> s0, s1;
   uint64_t dummy = 0;
-  if (!s0.alloc(nv_ * cap_cells_, &dummy, error, "autotune") || !s1.alloc(nv_ * cap_cells_, &dummy, error, "autotune"))
+  if (!s0.alloc(words * nv_ * cap_cells_, &dummy, error, "autotune") ||
+      !s1.alloc(words * nv_ * cap_cells_, &dummy, error, "autotune"))
     return 1;
   std::vector<CaseCtl> ctl_save(h_ctl_, h_ctl_ + config_.max_cases);
   cudaMemcpyAsync(s0.p, U0_.p, nbytes, cudaMemcpyDeviceToDevice, stream_);
   cudaMemcpyAsync(s1.p, U1_.p, nbytes, cudaMemcpyDeviceToDevice, stream_);
+  if (L0_.p) {
+    cudaMemcpyAsync(s0.p + nv_ * cap_cells_, L0_.p, nbytes, cudaMemcpyDeviceToDevice, stream_);
+    cudaMemcpyAsync(s1.p + nv_ * cap_cells_, L1_.p, nbytes, cudaMemcpyDeviceToDevice, stream_);
+  }
   // the tuning runs are not the caller's work: the advance statistics are restored afterwards
   const amr_gpu_stats_t stats_save = stats_;
   double best = 1e30;
@@ -571,6 +578,10 @@ void Batch<R>::restore(const std::vector<CaseCtl>& ctl_save, const DevBuf<R>& s0
   cudaMemcpyAsync(ctl_.p, h_ctl_, sizeof(CaseCtl) * config_.max_cases, cudaMemcpyHostToDevice, stream_);
   cudaMemcpyAsync(U0_.p, s0.p, nbytes, cudaMemcpyDeviceToDevice, stream_);
   cudaMemcpyAsync(U1_.p, s1.p, nbytes, cudaMemcpyDeviceToDevice, stream_);
+  if (L0_.p) {
+    cudaMemcpyAsync(L0_.p, s0.p + nv_ * cap_cells_, nbytes, cudaMemcpyDeviceToDevice, stream_);
+    cudaMemcpyAsync(L1_.p, s1.p + nv_ * cap_cells_, nbytes, cudaMemcpyDeviceToDevice, stream_);
+  }
   cudaStreamSynchronize(stream_);
 }
 

@@ -43,6 +43,9 @@ class BatchBase {
   virtual int release(int slot) = 0;
   // Runs `trials` trials of every live case and refreshes the host copies of the controls.
   virtual int advance(int trials, std::string* error) = 0;
+  // advance in two halves: enqueue the trials (no wait), then wait and refresh the statuses.
+  virtual int advance_begin(int trials, std::string* error) = 0;
+  virtual int advance_end(std::string* error) = 0;
   // Sets a case's target time and step cap (the session's advance arguments).
   virtual int set_target(int slot, double target, long long maxsteps, std::string* error) = 0;
   // Residual of every live case's accepted state into the engine's residual buffer.

@@ -33,14 +33,16 @@ def fixed_time(tend, max_steps=10 ** 9):
     return lambda spec: case_control(tend, max_steps, steady=False, mach=spec.mach, aoa=spec.aoa)
 
 
-def solve(items, precision, control, trials=32, launch_mode=0, download=True, device=0, max_polls=10 ** 7):
+def solve(items, precision, control, trials=32, launch_mode=0, download=True, device=0, max_polls=10 ** 7,
+          history=False):
     """Admits every case, advances `trials` trials per poll and applies the steady rule after each
     poll until every case has retired.  Returns (results, device_seconds): per case the status
     record (time, steps, rejected, status, converged, cl, cd, cm, ...) and, with download, its
-    accepted state u (FP64 copy)."""
+    accepted state u (FP64 copy); with history, the record of every steady check as 'history'
+    (time, steps, residual norms, loads, hold)."""
     b = Batch(precision=precision, launch_mode=launch_mode, device=device, **batch_kwargs(items))
     try:
-        entries = [(m, s.params(), cases.initial_state(m, s.initial_primitive()), control(s)) for s, m in items]
+        entries = [(m, s.params(), cases.uniform_state(m, s.initial_primitive()), control(s)) for s, m in items]
         slots = b.admit_many(entries)
         if any(s is None for s in slots):
             raise RuntimeError('batch arena too small for the workload')
@@ -48,6 +50,7 @@ def solve(items, precision, control, trials=32, launch_mode=0, download=True, de
             b.autotune(4)
         seconds = 0.0
         live = set(slots)
+        hist = {s: [] for s in slots}
         for _ in range(max_polls):
             if not live:
                 break
@@ -55,13 +58,18 @@ def solve(items, precision, control, trials=32, launch_mode=0, download=True, de
             seconds += b.last_advance_seconds
             b.check()
             for s in list(live):
-                if b.status(s)['finished']:
+                st = b.status(s)
+                if history and st['checks'] > len(hist[s]):
+                    hist[s].append({k: st[k] for k in ('time', 'steps', 'residual', 'cl', 'cd', 'cm', 'hold')})
+                if st['finished']:
                     live.discard(s)
         out = []
         for s in slots:
             r = b.status(s)
             if download:
                 r['u'] = b.download(s)
+            if history:
+                r['history'] = hist[s]
             out.append(r)
         return out, seconds
     finally:

@@ -121,3 +121,19 @@ def test_bulk_no_room_by_cells_and_readmit_into_freed_ranges():
     alone = run([items[small]], 32, 'split', 1, 1, bulk=False)[1][0]
     assert np.array_equal(b.download(0), alone)
     b.destroy()
+
+
+@pytest.mark.parametrize('precision,mode', [(32, 'split'), (64, 'phases')])
+def test_uniform_start_filled_on_device_equals_staged_start(precision, mode):
+    """A start given as the nv conserved values (filled on the device, leading and trailing words)
+    runs bit for bit like the same state staged cell by cell, alone and in bulk admission."""
+    mix = sa_mix()
+    staged = items_of(mix, 12)
+    uniform = [(mesh, spec.params(), cases.uniform_state(mesh, spec.initial_primitive()),
+                case_control(1e30, 12, steady=False, mach=spec.mach, aoa=spec.aoa)) for spec, mesh in mix]
+    ref_slots, ref_states, ref_steps = run(staged, precision, mode, 1, 4, bulk=False)
+    for bulk in (False, True):
+        slots, states, steps = run(uniform, precision, mode, 4, 4, bulk=bulk)
+        assert slots == ref_slots and steps == ref_steps
+        for a, b in zip(states, ref_states):
+            assert np.array_equal(a, b), bulk
