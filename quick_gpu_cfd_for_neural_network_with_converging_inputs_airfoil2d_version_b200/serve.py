@@ -2,14 +2,16 @@
 
 Requests (one airfoil + flow condition each) arrive as a Poisson process.  Each request's mesh
 is built on a pool of host threads (the native builder, amr_mesh_build) as soon as it
-arrives; built requests are admitted first come first served while the device arena has room
-(amr_batch_admit answers "no room" with 3); the batch advances a fixed number of trials per
-poll; the reference driver's steady rule (src/quick_airfoil.cpp:75-92), evaluated on the
+arrives; built requests are admitted first come first served into device arenas (batches): the
+first arena with room takes it (amr_batch_admit answers "no room" with 3), and when none has
+room a new arena is created if the device's free memory (cudaMemGetInfo) still holds one beside
+a reserve.  Every poll enqueues a fixed number of trials on every arena with live cases, then
+waits; the reference driver's steady rule (src/quick_airfoil.cpp:75-92), evaluated on the
 device, retires converged cases, and the step cap retires the rest as capped.  A request's
 latency runs from its arrival to the poll that retires it.
 
     reqs = poisson_requests(2000, rate=50.0, seed=20261203)
-    server = Server(Batch(precision=32, max_cases=512), max_steps=30000)
+    server = Server(lambda: Batch(precision=32, max_cases=64, max_cells=64 * 9800), max_steps=30000)
     results = server.run(reqs)
     print(summarize(results, server.wall_seconds))
 
@@ -25,6 +27,7 @@ import numpy as np
 from . import _abi, airfoils, cases
 
 STATUS_MAXSTEPS = _abi.STATUS_MAXSTEPS
+UNPLACEABLE = ('unplaceable',)  # _admit: the request does not fit even an empty arena
 
 
 @dataclasses.dataclass
@@ -47,6 +50,7 @@ class Result:
     cd: float = float('nan')
     cm: float = float('nan')
     error: str = ''
+    u: object = None        # final state, with Server(keep_states=True)
 
     @property
     def latency(self):
@@ -80,12 +84,27 @@ def build_request_mesh(req):
 
 
 class Server:
-    """Runs one batch.  `batch` is a batch.Batch (or an object with the same admit / advance /
-    check / status / release methods); `build` maps a Request to its MeshArrays."""
+    """Runs the serving loop over one or more arenas (batches).
 
-    def __init__(self, batch, max_steps=30000, trials=32, builder_threads=0, build=build_request_mesh, steady=None,
-                 clock=time.perf_counter, sleep=time.sleep):
-        self.batch = batch
+    `arena` is either one batch (a fixed arena: requests are admitted while it has room) or a
+    callable that creates one (arenas on demand, admission by free device memory): a built request
+    goes into the first arena with room for it; when none has room, a new arena is created if the
+    device's free memory, less `hbm_reserve` bytes, still covers one arena of the size the first
+    one took (`memory` returns (free, total) bytes; by default cudaMemGetInfo of `device`), and
+    otherwise the request waits for a retirement.  Arenas that empty, beyond the first, are
+    destroyed and their memory returned.  `max_live_cells` optionally caps the live cells (the
+    point past which more concurrent cases add latency but no throughput).  Every poll enqueues
+    `trials` trials on every arena with live cases before waiting for any, so the arenas' kernels
+    overlap on the device.  `build` maps a Request to its MeshArrays; with keep_states each
+    result carries its final state."""
+
+    def __init__(self, arena, max_steps=30000, trials=32, builder_threads=0, build=build_request_mesh, steady=None,
+                 clock=time.perf_counter, sleep=time.sleep, memory=None, device=0, hbm_reserve=2 << 30,
+                 max_live_cells=None, keep_states=False, max_arenas=256):
+        if callable(arena) and not hasattr(arena, 'admit'):
+            self.make_arena, self.arenas = arena, []
+        else:
+            self.make_arena, self.arenas = None, [arena]
         self.max_steps = int(max_steps)
         self.trials = int(trials)
         self.build = build
@@ -93,13 +112,78 @@ class Server:
         self.clock = clock
         self.sleep = sleep
         self.threads = builder_threads if builder_threads > 0 else None
+        self.device = device
+        self.memory = memory
+        self.hbm_reserve = int(hbm_reserve)
+        self.max_live_cells = max_live_cells
+        self.keep_states = keep_states
+        self.max_arenas = max_arenas
+        self.arena_bytes = None
         self.wall_seconds = 0.0
         self.polls = 0
         self.cell_steps = 0
+        self.live_cells = 0
+        self.peak_live_cells = 0
+        self.peak_arenas = len(self.arenas)
+        self.arenas_created = 0
 
     def _control(self, spec):
         from .batch import case_control
         return case_control(1e30, self.max_steps, steady=True, mach=spec.mach, aoa=spec.aoa, **self.steady)
+
+    def _free_memory(self):
+        if self.memory is not None:
+            return self.memory()[0]
+        from .batch import device_memory
+        return device_memory(self.device)[0]
+
+    def _grow(self):
+        """A new arena when the device's free memory allows one more; None otherwise."""
+        if self.make_arena is None or len(self.arenas) >= self.max_arenas:
+            return None
+        if self.arena_bytes is not None and self._free_memory() - self.hbm_reserve < self.arena_bytes:
+            return None
+        a = self.make_arena()
+        if self.arena_bytes is None:
+            self.arena_bytes = int(getattr(a, 'device_bytes', 0))
+        self.arenas.append(a)
+        self.arenas_created += 1
+        self.peak_arenas = max(self.peak_arenas, len(self.arenas))
+        return a
+
+    def _admit(self, r, mesh):
+        """(arena, slot) of the admitted request, or None when no arena has room for it now."""
+        if self.max_live_cells is not None and self.live and self.live_cells + mesh.n_cells > self.max_live_cells:
+            return None
+        u0 = cases.uniform_state(mesh, r.spec.initial_primitive())  # the device fills the cells
+        ctl = self._control(r.spec)
+        for a in self.arenas:
+            slot = a.admit(mesh, r.spec.params(), u0, ctl)
+            if slot is not None:
+                return a, slot
+        a = self._grow()
+        if a is not None:
+            slot = a.admit(mesh, r.spec.params(), u0, ctl)
+            if slot is not None:
+                return a, slot
+            # not even an empty arena holds it: give the arena back and fail the request
+            self.arenas.remove(a)
+            if hasattr(a, 'destroy'):
+                a.destroy()
+            return UNPLACEABLE
+        return None
+
+    def _advance(self, arenas):
+        if all(hasattr(a, 'advance_async') for a in arenas):
+            for a in arenas:
+                a.advance_async(self.trials)
+            for a in arenas:
+                a.wait()
+        else:
+            for a in arenas:
+                a.advance(self.trials)
+        for a in arenas:
+            a.check()
 
     def run(self, requests):
         requests = sorted(requests, key=lambda r: r.arrival)
@@ -107,7 +191,8 @@ class Server:
         pending = list(requests)          # not yet arrived
         building = {}                     # future -> request
         ready = []                        # (request, mesh) built, waiting for room
-        live = {}                         # slot -> (request, cells)
+        self.live = {}                    # (arena id, slot) -> (arena, slot, request, cells)
+        live = self.live
         t0 = self.clock()
         pool = concurrent.futures.ThreadPoolExecutor(max_workers=self.threads)
         try:
@@ -126,31 +211,43 @@ class Server:
                 ready.sort(key=lambda item: item[0].arrival)
                 while ready:
                     r, mesh = ready[0]
-                    u0 = cases.initial_state(mesh, r.spec.initial_primitive())
-                    slot = self.batch.admit(mesh, r.spec.params(), u0, self._control(r.spec))
-                    if slot is None:
+                    placed = self._admit(r, mesh)
+                    if placed is UNPLACEABLE or (placed is None and not live):
+                        # nothing live will free room: the request does not fit an empty arena, or
+                        # the device has no memory for one
+                        ready.pop(0)
+                        res = results[r.id]
+                        res.outcome, res.error, res.finished = 'failed', 'no room', self.clock() - t0
+                        continue
+                    if placed is None:
                         break                 # no room: admit again after a retirement
+                    a, slot = placed
                     ready.pop(0)
-                    live[slot] = (r, mesh.n_cells)
+                    live[(id(a), slot)] = (a, slot, r, mesh.n_cells)
+                    self.live_cells += mesh.n_cells
+                    self.peak_live_cells = max(self.peak_live_cells, self.live_cells)
                     results[r.id].admitted = self.clock() - t0
                     results[r.id].cells = mesh.n_cells
                 if not live:
                     # idle: wait for the next arrival or build
                     waits = [pending[0].arrival - (self.clock() - t0)] if pending else []
-                    if building:
+                    if building or ready:
                         waits.append(0.002)
                     if waits:
                         self.sleep(max(0.0, min(waits)))
                     continue
-                before = {s: self.batch.status(s)['steps'] for s in live}
-                self.batch.advance(self.trials)
-                self.batch.check()
+                before = {key: a.status(slot)['steps'] for key, (a, slot, _, _) in live.items()}
+                active = []
+                for a, _, _, _ in live.values():
+                    if all(a is not b for b in active):
+                        active.append(a)
+                self._advance(active)
                 self.polls += 1
                 done_at = self.clock() - t0
-                for s in list(live):
-                    st = self.batch.status(s)
-                    r, cells = live[s]
-                    self.cell_steps += (st['steps'] - before[s]) * cells
+                for key in list(live):
+                    a, slot, r, cells = live[key]
+                    st = a.status(slot)
+                    self.cell_steps += (st['steps'] - before[key]) * cells
                     if not (st['finished'] or st['status']):
                         continue
                     res = results[r.id]
@@ -162,8 +259,17 @@ class Server:
                         res.outcome = 'capped'
                     else:
                         res.outcome, res.error = 'failed', f"status {st['status']}"
-                    self.batch.release(s)
-                    del live[s]
+                    if self.keep_states:
+                        res.u = a.download(slot)
+                    a.release(slot)
+                    self.live_cells -= cells
+                    del live[key]
+                # arenas that emptied, beyond the first, give their memory back
+                for a in self.arenas[1:]:
+                    if self.make_arena is not None and all(v[0] is not a for v in live.values()):
+                        self.arenas.remove(a)
+                        if hasattr(a, 'destroy'):
+                            a.destroy()
         finally:
             pool.shutdown(wait=True)
         self.wall_seconds = self.clock() - t0

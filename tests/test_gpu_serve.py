@@ -1,6 +1,7 @@
 """GPU test of the serving loop on the real engine: natively built meshes, admission while the
-arena has room, device steady-rule retirement and the step cap; a served case must end bit for
-bit where the same case run alone in a batch ends."""
+arena has room or into new arenas while the device has free memory, device steady-rule retirement
+and the step cap; a served case must end bit for bit where the same case run alone in a batch
+ends, also when it shared the device with other requests."""
 import numpy as np
 import pytest
 
@@ -52,3 +53,40 @@ def test_served_case_matches_a_lone_batch_run():
     st = lone.status(slot)
     assert st['status'] == _abi.STATUS_MAXSTEPS and st['steps'] == 64
     assert (st['cl'], st['cd'], st['cm']) == (res.cl, res.cd, res.cm)
+
+
+def lone_run(req, mesh, max_steps, trials=32):
+    """The request alone in its own batch, polled and checked as the server does."""
+    lone = Batch(precision=32, model=_abi.MODEL_LAMINAR, sa=True, max_cases=1, max_cells=mesh.n_cells + 64,
+                 launch_mode=_abi.LAUNCH_SPLIT, block_threads=128)
+    u0 = cases.initial_state(mesh, req.spec.initial_primitive())
+    slot = lone.admit(mesh, req.spec.params(), u0, case_control(1e30, max_steps, steady=True, mach=req.spec.mach,
+                                                                 aoa=req.spec.aoa))
+    while True:
+        lone.advance(trials)
+        lone.check()
+        st = lone.status(slot)
+        if st['finished'] or st['status']:
+            break
+    u = lone.download(slot)
+    lone.destroy()
+    return st, u
+
+
+def test_overlapping_requests_each_equal_alone():
+    """Four requests 20 ms apart, two per arena (so a second arena opens by free device memory and
+    both arenas' trials are in flight together); later requests are admitted while earlier ones run.
+    Each served case's final state and loads equal its lone run bit for bit."""
+    reqs = serve.poisson_requests(4, rate=50.0, seed=7)
+    make = lambda: Batch(precision=32, model=_abi.MODEL_LAMINAR, sa=True, max_cases=2, max_cells=2 * 9800,
+                         launch_mode=_abi.LAUNCH_SPLIT, block_threads=128)
+    server = serve.Server(make, max_steps=3000, trials=32, builder_threads=4, keep_states=True)
+    results = server.run(reqs)
+    assert all(r.outcome == 'capped' and r.steps == 3000 for r in results), [(r.outcome, r.steps) for r in results]
+    assert server.peak_arenas == 2 and len(server.arenas) == 1
+    first_done = min(r.finished for r in results)
+    assert sum(1 for r in results if r.admitted < first_done) >= 3  # at least three on the device together
+    for req, res in zip(reqs, results):
+        st, u = lone_run(req, serve.build_request_mesh(req), 3000)
+        assert st['steps'] == res.steps and (st['cl'], st['cd'], st['cm']) == (res.cl, res.cd, res.cm)
+        assert np.array_equal(u, res.u), req.id

@@ -124,6 +124,70 @@ def test_admission_waits_for_room_fifo():
         assert finished_before >= i - 1
 
 
+class FakeDevice:
+    """Device memory for arenas of `arena_bytes` each: free = total - arenas * arena_bytes."""
+
+    def __init__(self, total, arena_bytes):
+        self.total, self.arena_bytes, self.arenas = total, arena_bytes, 0
+        self.peak = 0
+
+    def memory(self):
+        return self.total - self.arenas * self.arena_bytes, self.total
+
+
+def test_arenas_grow_by_free_memory_and_are_returned():
+    """Admission by free device memory: a request that fits no arena opens a new one while the
+    device's free memory, less the reserve, covers one more; emptied arenas beyond the first are
+    destroyed (their memory returned)."""
+    clock = FakeClock()
+    reqs = requests_euler(12, rate=1e6)  # everything arrives at once
+    needs = {r.id: 96 for r in reqs}
+    dev = FakeDevice(total=1000, arena_bytes=100)
+    made, destroyed = [], []
+
+    def make_arena():
+        b = FakeBatch(clock, 2100, needs)  # two cases per arena
+        b.device_bytes = dev.arena_bytes
+        dev.arenas += 1
+        dev.peak = max(dev.peak, dev.arenas)
+
+        def destroy(b=b):
+            destroyed.append(b)
+            dev.arenas -= 1
+        b.destroy = destroy
+        made.append(b)
+        return b
+
+    # reserve 650: free - reserve >= 100 holds for 0, 1 and 2 existing arenas, so at most 3
+    server = serve.Server(make_arena, max_steps=200, trials=32, builder_threads=2, build=fake_build, clock=clock,
+                          sleep=clock.sleep, memory=dev.memory, hbm_reserve=650)
+    results = server.run(reqs)
+    assert all(r.outcome == 'converged' for r in results)
+    assert server.peak_arenas == 3 and dev.peak == 3 and len(made) >= 3
+    assert server.peak_live_cells <= 3 * 2100
+    # at most six live at once: the seventh admission waited for a retirement
+    admitted = sorted(results, key=lambda r: r.admitted)
+    assert sum(1 for r in results if r.finished <= admitted[6].admitted) >= 1
+    assert len(server.arenas) == 1 and len(destroyed) == len(made) - 1
+
+
+def test_live_cell_cap_and_unplaceable_request():
+    clock = FakeClock()
+    reqs = requests_euler(6, rate=1e6)
+    needs = {r.id: 64 for r in reqs}
+    server = serve.Server(lambda: FakeBatch(clock, 10 ** 9, needs), max_steps=200, trials=32, builder_threads=2,
+                          build=fake_build, clock=clock, sleep=clock.sleep, memory=lambda: (10 ** 12, 10 ** 12),
+                          max_live_cells=2100)
+    results = server.run(reqs)
+    assert all(r.outcome == 'converged' for r in results) and server.peak_live_cells <= 2100
+    # a request larger than an empty arena fails instead of waiting forever
+    big = serve.Server(lambda: FakeBatch(clock, 500, needs), max_steps=200, trials=32, builder_threads=2,
+                       build=fake_build, clock=clock, sleep=clock.sleep, memory=lambda: (10 ** 12, 10 ** 12))
+    out = big.run(reqs[:2])
+    assert [r.outcome for r in out] == ['failed', 'failed'] and out[0].error == 'no room'
+    assert big.arenas_created == 2 and big.arenas == []  # each trial arena was given back
+
+
 def _rank_main(rank, world, port, out_path):
     os.environ.update(MASTER_ADDR='127.0.0.1', MASTER_PORT=str(port))
     dist.init_process_group('gloo', rank=rank, world_size=world)
