@@ -67,7 +67,9 @@ def peaks():
 
 def algorithmic_bytes(mesh, s=4, sg=4):
     """Compulsory HBM bytes of one accepted step of one case (intermediates count 0):
-    8*nv*s*n state traffic + 3*[n*c_cell + nf*c_face + nw*c_wall + T*c_term + S_srd]."""
+    8*nv*s*n state traffic + 3*[n*c_cell + nf*c_face + nw*c_wall + T*c_term + S_srd], plus, for the
+    FP32 form's two-word accepted state, the read and write of the trailing word in the final stage
+    (2*nv*4*n)."""
     n, nf, nw, nv = mesh.n_cells, mesh.n_faces, mesh.n_walls, mesh.nv
     viscous = mesh.laminar
     T = int(mesh.visc_offsets[-1]) if viscous else 0
@@ -79,7 +81,8 @@ def algorithmic_bytes(mesh, s=4, sg=4):
     if mesh.small_cells:
         sizes = np.diff(mesh.group_offsets.astype(np.int64))
         srd = 16 * int(sizes[sizes > 1].sum())
-    return 8 * nv * s * n + 3 * (n * c_cell + nf * c_face + nw * c_wall + T * c_term + srd)
+    trailing = 2 * nv * 4 * n if s == 4 else 0
+    return 8 * nv * s * n + trailing + 3 * (n * c_cell + nf * c_face + nw * c_wall + T * c_term + srd)
 
 
 def _cuda_pci_bus_id(device):
@@ -218,7 +221,7 @@ def new_batch(case_list, precision, device=0, block=0, grid=0, mode=0):
 
 
 def admit_all(b, case_list, steps_cap=10 ** 9):
-    items = [(m, s.params(), cases.initial_state(m, s.initial_primitive()),
+    items = [(m, s.params(), cases.uniform_state(m, s.initial_primitive()),
               case_control(1e30, steps_cap, steady=False, mach=s.mach, aoa=s.aoa)) for s, m in case_list]
     slots = b.admit_many(items)
     assert all(s is not None for s in slots), 'arena too small'
@@ -288,9 +291,9 @@ def run_e2e(case_list, precision, steps, device=0, trials=32, block=0, grid=0, m
     t_create = time.perf_counter()
     items, h2d = [], 0
     for spec, mesh in case_list:
-        u0 = cases.initial_state(mesh, spec.initial_primitive())
+        u0 = cases.uniform_state(mesh, spec.initial_primitive())  # filled on the device
         items.append((mesh, spec.params(), u0, case_control(1e30, 10 ** 9, steady=False)))
-        h2d += mesh_bytes(mesh, precision) + u0.nbytes * precision // 64
+        h2d += mesh_bytes(mesh, precision) + u0.nbytes
     t_items = time.perf_counter()
     slots = b.admit_many(items)
     t_admit = time.perf_counter()
@@ -502,16 +505,37 @@ def reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def serving_arena(args, device):
+    """Factory of one serving arena: FP32 SA batch of args.arena_cases cases (9800 cells each)."""
+    return lambda: Batch(precision=32, model=_abi.MODEL_LAMINAR, sa=True, max_cases=args.arena_cases,
+                         max_cells=args.arena_cases * 9800, device=device, launch_mode=_abi.LAUNCH_SPLIT,
+                         block_threads=128)
+
+
+def plain_fp64_solves(items, max_steps):
+    """The plain FP64 path on (spec, mesh) items, one case at a time to the steady criteria or the
+    step cap (the FP64 batch of one case is bit for bit the single-case FP64 session); host wall
+    time per case, polls and checks included."""
+    out = []
+    for spec, mesh in items:
+        t0 = time.perf_counter()
+        (r,), dev = runs.solve([(spec, mesh)], 64, runs.steady_control(max_steps=max_steps), download=False)
+        out.append(dict(r, wall=time.perf_counter() - t0, device_seconds=dev))
+    return out
+
+
 def run_serving(args, rank, world, local):
     """--workload serve: the served form.  Poisson request arrivals (seeded), host mesh builds on a
-    thread pool, admission by free device memory, device steady-rule retirement or the step cap.
-    Each rank serves its shard on its own GPU; rank 0 prints one JSON line."""
+    thread pool, admission into arenas by free device memory (and an optional live-cell cap),
+    device steady-rule retirement or the step cap; then the loads of a sample of the requests
+    against the plain FP64 path at the same cap.  Each rank serves its shard on its own GPU; rank 0
+    prints one JSON line."""
     from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200 import serve
     reqs = serve.poisson_requests(args.requests, args.rate, args.seed)
     mine = serve.shard(reqs, rank, world)
-    batch = Batch(precision=32, model=_abi.MODEL_LAMINAR, sa=True, max_cases=args.serve_cases,
-                  max_cells=args.serve_cases * 9800, device=local, launch_mode=_abi.LAUNCH_SPLIT, block_threads=128)
-    server = serve.Server(batch, max_steps=args.max_steps, trials=32, builder_threads=max(1, (os.cpu_count() or 2) - 1))
+    server = serve.Server(serving_arena(args, local), max_steps=args.max_steps, trials=32, device=local,
+                          builder_threads=max(1, (os.cpu_count() or 2) - 1), hbm_reserve=args.hbm_reserve,
+                          max_live_cells=args.max_live_cells or None)
     dist_barrier(world)
     with ClockSampler(local) as clk:
         results = server.run(mine)
@@ -520,20 +544,113 @@ def run_serving(args, rank, world, local):
     merged = serve.gather_results(results, world)
     if rank == 0:
         summary = serve.summarize(merged, wall, cell_steps)
+        # loads against the plain FP64 path on a sample (first LF1 and LF2 requests), same cap
+        sample = [r for r in reqs if r.spec.profile == 'LF1'][:args.plain_sample // 2] + \
+                 [r for r in reqs if r.spec.profile == 'LF2'][:args.plain_sample // 2]
+        plain = plain_fp64_solves([(r.spec, serve.build_request_mesh(r)) for r in sample], args.max_steps)
+        by_id = {r.id: r for r in merged}
+        errs = [dict(id=q.id, profile=q.spec.profile, steps32=by_id[q.id].steps, steps64=p['steps'],
+                     dcl=abs(by_id[q.id].cl - p['cl']), dcd=abs(by_id[q.id].cd - p['cd']), dcm=abs(by_id[q.id].cm - p['cm']))
+                for q, p in zip(sample, plain)]
         line = dict(metric='served solves/s and p50/p99 latency (converged and capped apart)', impl='ours',
                     value=summary['completed_per_s'], unit='solves/s', n_gpus=world, higher_is_better=True,
                     scaling='weak', dtype='f32', data='synthetic',
                     config=dict(workload='served-sa-fp32', requests=args.requests, rate_per_s=args.rate, seed=args.seed,
-                                max_steps=args.max_steps, profiles='LF1:LF2 1:1', arena_cases=args.serve_cases,
+                                max_steps=args.max_steps, profiles='LF1:LF2 1:1', arena_cases=args.arena_cases,
+                                hbm_reserve=args.hbm_reserve, max_live_cells=args.max_live_cells or None,
                                 meshes='native host builder, seeded NACA 4-digit draws'),
-                    serving=summary, polls=server.polls, clocks=clk.summary())
+                    serving=summary, polls=server.polls, arenas=dict(peak=server.peak_arenas, created=server.arenas_created,
+                                                                      bytes_each=server.arena_bytes),
+                    peak_live_cells=server.peak_live_cells,
+                    loads_vs_plain_fp64=dict(sample=errs, max_dcl=max(e['dcl'] for e in errs),
+                                             max_dcd=max(e['dcd'] for e in errs), max_dcm=max(e['dcm'] for e in errs)),
+                    clocks=clk.summary())
         print(json.dumps(line), flush=True)
     dist_barrier(world)
 
 
+def converged_leg(args):
+    """--workload converged: converged solves per second of the served FP32 form against the plain
+    FP64 path on the same request mix.  args.requests requests of the served distribution arrive
+    at once and run to the steady criteria (cap args.max_steps); the plain FP64 path solves a
+    sample of the same requests one at a time; both converged-solve rates, their ratio, and the
+    loads of the sampled requests against each other."""
+    from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200 import serve
+    reqs = serve.poisson_requests(args.requests, 1e9, args.seed)
+    server = serve.Server(serving_arena(args, 0), max_steps=args.max_steps, trials=32,
+                          builder_threads=max(1, (os.cpu_count() or 2) - 1), hbm_reserve=args.hbm_reserve)
+    with ClockSampler(0) as clk:
+        results = server.run(reqs)
+    summary = serve.summarize(results, server.wall_seconds, server.cell_steps)
+    sample = [r for r in reqs if r.spec.profile == 'LF1'][:args.plain_sample // 2] + \
+             [r for r in reqs if r.spec.profile == 'LF2'][:args.plain_sample // 2]
+    plain = plain_fp64_solves([(r.spec, serve.build_request_mesh(r)) for r in sample], args.max_steps)
+    plain_wall = sum(p['wall'] for p in plain)
+    plain_conv = sum(1 for p in plain if p['converged'])
+    by_id = {r.id: r for r in results}
+    errs = [dict(id=q.id, profile=q.spec.profile, converged32=by_id[q.id].outcome == 'converged',
+                 converged64=bool(p['converged']), steps32=by_id[q.id].steps, steps64=p['steps'],
+                 dcl=abs(by_id[q.id].cl - p['cl']), dcd=abs(by_id[q.id].cd - p['cd']), dcm=abs(by_id[q.id].cm - p['cm']))
+            for q, p in zip(sample, plain)]
+    fp32_rate = summary['converged_per_s']
+    fp64_rate = plain_conv / plain_wall if plain_wall > 0 else 0.0
+    line = dict(workload='converged-solves-fp32-served-vs-plain-fp64', requests=args.requests, max_steps=args.max_steps,
+                seed=args.seed, arena_cases=args.arena_cases,
+                fp32_served=dict(converged_per_s=fp32_rate, wall_seconds=server.wall_seconds,
+                                 outcomes=summary['outcomes'], cell_steps_per_s=summary.get('cell_steps_per_s'),
+                                 peak_arenas=server.peak_arenas, latency=summary['latency']),
+                plain_fp64=dict(converged_per_s=fp64_rate, sample=len(sample), converged=plain_conv, wall_seconds=plain_wall,
+                                note='one case at a time; rate from a sample of the same requests'),
+                ratio=fp32_rate / fp64_rate if fp64_rate > 0 else None,
+                loads_sample=errs, max_dcl=max(e['dcl'] for e in errs), max_dcd=max(e['dcd'] for e in errs),
+                clocks=clk.summary())
+    print(json.dumps(line), flush=True)
+
+
+def g0001_items():
+    """The reference's example G0001 on LF1 and LF2 with the reference pipeline's default settings
+    (tests/golden: the settings text and the contour prepared by the reference's own pipeline);
+    meshes from the native builder (bit-identical tables to the reference builder's)."""
+    from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200 import builder, settings
+    ka = json.loads((GOLDEN / 'known_answers.json').read_text())
+    z = np.load(GOLDEN / 'examples.npz')
+    i = list(z['names']).index('G0001')
+    a, b = z['offsets'][i], z['offsets'][i + 1]
+    items = []
+    for profile in ('LF1', 'LF2'):
+        s, boxes = settings.parse_settings(ka['settings']['default_' + profile])
+        spec = settings.SettingsSpec(s, boxes, profile)
+        items.append((spec, builder.build_mesh(spec, z['x'][a:b], z['y'][a:b], z['patches'][a:b])))
+    return items, ka['full_steady']
+
+
+def g0001_steady(args):
+    """G0001 LF1 and LF2 to the steady criteria in FP64 and FP32 (two-word state), with the
+    residual norms and loads of every check, against the reference's published FP64 solve."""
+    items, published = g0001_items()
+    ctl = runs.steady_control(stop_time=100.0)
+    r64, s64 = runs.solve(items, 64, ctl, history=True)
+    r32, s32 = runs.solve(items, 32, ctl, history=True)
+    out = {}
+    for (spec, mesh), a, b in zip(items, r32, r64):
+        pub = published[spec.profile]
+        same_t = a['time'] == b['time']
+        out[spec.profile] = dict(
+            cells=mesh.n_cells, published=pub,
+            fp64=dict(converged=b['converged'], steps=b['steps'], time=b['time'], cl=b['cl'], cd=b['cd'], cm=b['cm'],
+                      dcl_published=b['cl'] - pub['Cl'], dcd_published=b['cd'] - pub['Cd'],
+                      dcm_published=b['cm'] - pub['Cm'], history=b['history']),
+            fp32=dict(converged=a['converged'], steps=a['steps'], time=a['time'], cl=a['cl'], cd=a['cd'], cm=a['cm'],
+                      history=a['history']),
+            load_error=runs.load_errors(a, b),
+            field_error_at_common_time=runs.field_errors(a['u'], b['u'], mesh.nv) if same_t else None)
+    return dict(device_seconds=dict(fp64=s64, fp32=s32), cases=out)
+
+
 def accuracy_leg(args):
     """NACA 2412 LF2 SA to the steady criteria or 20000 steps, FP64 and FP32: loads at every check
-    and of the final states, and the per-field error of the FP32 final state."""
+    and of the final states, and the per-field error of the FP32 final state; and G0001 LF1/LF2 to
+    the steady criteria in FP64 and FP32 with their convergence histories."""
     w = workloads.naca2412_lf2_sa()
     spec, mesh = w.items[0]
     ctl = runs.steady_control(max_steps=args.accuracy_steps)
@@ -552,7 +669,8 @@ def accuracy_leg(args):
     line = dict(workload='accuracy-naca2412-lf2-sa', cells=mesh.n_cells, max_steps=args.accuracy_steps,
                 fp64=out[64], fp32=out[32], load_error_last_check=e_check, load_error_final_state=e_final,
                 field_error_final_state=fields,
-                note='FP32 and FP64 end at the same step count; their final times differ by the dt history')
+                note='FP32 and FP64 end at the same step count; their final times differ by the dt history',
+                g0001_steady=g0001_steady(args))
     print(json.dumps(line), flush=True)
 
 
@@ -613,7 +731,7 @@ def main():
     ap.add_argument('--steps', type=int, default=320)
     ap.add_argument('--warmup', type=int, default=64)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--workload', default='batched', choices=['batched', 'accuracy', 'time-accurate', 'serve'])
+    ap.add_argument('--workload', default='batched', choices=['batched', 'accuracy', 'time-accurate', 'serve', 'converged'])
     ap.add_argument('--cases', type=int, default=256)
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--no-solve', action='store_true', help='skip the measured full-solve leg')
@@ -625,7 +743,10 @@ def main():
     ap.add_argument('--requests', type=int, default=200)
     ap.add_argument('--rate', type=float, default=50.0)
     ap.add_argument('--max-steps', type=int, default=3000)
-    ap.add_argument('--serve-cases', type=int, default=512)
+    ap.add_argument('--arena-cases', type=int, default=64, help='cases per serving arena')
+    ap.add_argument('--hbm-reserve', type=int, default=4 << 30, help='device bytes kept free when opening an arena')
+    ap.add_argument('--max-live-cells', type=int, default=0, help='live-cell cap of the served form (0: none)')
+    ap.add_argument('--plain-sample', type=int, default=4, help='requests the plain FP64 path solves for comparison')
     ap.add_argument('--seed', type=int, default=workloads.SEED)
     ap.add_argument('--accuracy-steps', type=int, default=20000)
     ap.add_argument('--ta-cases', type=int, default=128)
@@ -641,6 +762,10 @@ def main():
     if args.workload == 'accuracy':
         if rank == 0:
             accuracy_leg(args)
+        return
+    if args.workload == 'converged':
+        if rank == 0:
+            converged_leg(args)
         return
     if args.workload == 'time-accurate':
         if rank == 0:

@@ -17,7 +17,7 @@ def _rank(rank, world, port, out):
     bench.dist_barrier(w)
     t = bench.dist_max(1.5 + rank, w)
     total = bench.dist_sum(10 * (rank + 1), w)
-    draws = [spec.mach for spec, _ in bench.batched_cases(4, seed=20261203 + rank)]  # the replica's own cases
+    draws = [spec.mach for spec in bench.workloads.batched_sa_specs(4, seed=bench.rank_seed(rank))]  # the replica's own cases
     with open(f'{out}.{rank}', 'w') as f:
         f.write(' '.join(repr(m) for m in draws))
     if rank == 0:
