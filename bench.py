@@ -786,12 +786,12 @@ def main():
     value = cell_steps / dev_seconds
     cfg = r['config']
     block, grid, mode = parse_launch(cfg)
-    solve = None if args.no_solve else run_solve(case_list, SOLVE_STEPS, local, block, grid, mode)
-    clk.__exit__(None, None, None)
-    # the device-timed batch is freed after the end-to-end run, so that its teardown in the driver
-    # does not overlap (and slow) the end-to-end run's own batch creation
+    # the end-to-end run comes before any batch is freed: a batch's teardown in the driver can take
+    # up to a second and, overlapping the next batch's creation, slows that creation
     e2e = run_e2e(case_list, 32, args.steps, device=local, block=block, grid=grid, mode=mode)
     r.pop('batch').destroy()
+    solve = None if args.no_solve else run_solve(case_list, SOLVE_STEPS, local, block, grid, mode)
+    clk.__exit__(None, None, None)
     e2e_value = dist_sum(e2e['value'], world)
     # roofline of the step: algorithmic bytes per launch / launch duration (CUDA events)
     bytes_per_step = sum(algorithmic_bytes(m) for _, m in case_list)

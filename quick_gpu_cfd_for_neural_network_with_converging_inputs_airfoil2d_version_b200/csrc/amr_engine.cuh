@@ -904,26 +904,31 @@ __device__ __forceinline__ double finish_tail(const Dev<R>& d, const CaseCfg<R>&
     R out[5];
     bool two_word = false;
     if constexpr (sizeof(R) == 4) {
-      two_word = stage == STAGE_2 && d.L0 != nullptr;
+      two_word = d.L0 != nullptr;
     }
     if (two_word) {
-      // FP32 form, final stage: the accepted state is a two-word FP32 value (U leading, L
-      // trailing).  The update U+ = U/3 + 2/3 (U2 + dt R2) is formed as U + 2/3 ((U2 - U) + dt R2)
-      // and added to U + L with an error-free FP32 sum (Knuth's TwoSum), so increments below
-      // half an ulp of U accumulate in L instead of being rounded away; with only a leading
-      // word a case stalls short of its steady state once dt R falls below that size.
-      // Cases with SRD redistribute the final state afterwards and keep L = 0.
+      // FP32 form: the accepted state is a two-word FP32 value (U leading, L trailing).  The
+      // final stage U+ = U/3 + 2/3 (U2 + dt R2) is formed as U + 2/3 (D2 + dt R2), with
+      // D2 = U2 - U = (dt R0 + dt R1) / 4, and added to U + L with an error-free FP32 sum
+      // (Knuth's TwoSum), so increments below half an ulp of U accumulate in L instead of being
+      // rounded away; with only a leading word a case stalls short of its steady state once dt R
+      // falls below that size.  Stage 1 stores U2 for the fluxes and, in the trailing words of the
+      // next state buffer (which the final stage rewrites), the unrounded increment D2.  Cases with
+      // SRD redistribute the stage states afterwards and keep L = 0.
       const R* Lb = Ub == d.U0 ? d.L0 : d.L1;
       R* Ln = Un == d.U0 ? d.L0 : d.L1;
       for (int v = 0; v < nv; ++v) {
         const R ub = Ub[v * n + k];
-        if (cf.has_srd) {
+        if (stage == STAGE_1) {
+          out[v] = R(0.75) * ub + R(0.25) * (Uin[v * n + k] + dt * res[v]);
+          if (!cf.has_srd) Ln[v * n + k] = R(0.25) * (dt * d.R0[v * n + k] + dt * res[v]);
+        } else if (cf.has_srd) {
           out[v] = ub / R(3) + R(2.0 / 3) * (Uin[v * n + k] + dt * res[v]);
           Ln[v * n + k] = R(0);
-          continue;
+        } else {
+          const R inc = R(2.0 / 3) * (Ln[v * n + k] + dt * res[v]);
+          two_sum(ub, add_rn(inc, Lb[v * n + k]), out[v], Ln[v * n + k]);
         }
-        const R inc = R(2.0 / 3) * ((Uin[v * n + k] - ub) + dt * res[v]);
-        two_sum(ub, add_rn(inc, Lb[v * n + k]), out[v], Ln[v * n + k]);
       }
     }
     if (!two_word) {
@@ -1464,6 +1469,24 @@ template <> struct SplitOcc<float> {
   static constexpr int item = AMRB_SPLIT_MINB_F32, cell = AMRB_SPLIT_CELL_MINB_F32, gather = AMRB_SPLIT_GATHER_MINB_F32;
 };
 template <> struct SplitOcc<double> { static constexpr int item = 3, cell = 4, gather = 4; };
+// Blocks per SM per stage: FP32 stage 1 forms U1 = U + dt R0 in place in its gradient and gather
+// kernels (and its gather also keeps the stage increment), so those two get more registers.
+#ifndef AMRB_SPLIT1_CELL_MINB_F32
+#define AMRB_SPLIT1_CELL_MINB_F32 AMRB_SPLIT_CELL_MINB_F32
+#endif
+#ifndef AMRB_SPLIT1_GATHER_MINB_F32
+#define AMRB_SPLIT1_GATHER_MINB_F32 AMRB_SPLIT_GATHER_MINB_F32
+#endif
+#ifndef AMRB_SPLIT2_GATHER_MINB_F32
+#define AMRB_SPLIT2_GATHER_MINB_F32 AMRB_SPLIT_GATHER_MINB_F32
+#endif
+template <class R, int STAGE> struct SplitStageOcc : SplitOcc<R> {};
+template <> struct SplitStageOcc<float, 1> {
+  static constexpr int item = AMRB_SPLIT_MINB_F32, cell = AMRB_SPLIT1_CELL_MINB_F32, gather = AMRB_SPLIT1_GATHER_MINB_F32;
+};
+template <> struct SplitStageOcc<float, 2> {
+  static constexpr int item = AMRB_SPLIT_MINB_F32, cell = AMRB_SPLIT_CELL_MINB_F32, gather = AMRB_SPLIT2_GATHER_MINB_F32;
+};
 
 __device__ __forceinline__ int stage_rule(int stage) {
   return stage == STAGE_DIAG ? SKIP_LIVE : (stage == STAGE_BASE ? SKIP_ACTIVE : SKIP_STAGE);
@@ -1539,8 +1562,13 @@ __device__ __forceinline__ void load_item(const R* src, R* col, bool base, bool 
   if (MODEL == MODEL_SA) col[10] = sg * col[10];
 }
 
-template <class R, int MODEL>
-__global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::cell) grad_cells_kernel(Dev<R> d, int stage) {
+// The split kernels are compiled once per stage (STAGE_BASE, STAGE_1, STAGE_2, STAGE_DIAG): each
+// instance carries only its stage's path, so its registers go to that path alone (the base
+// stage's FP64 dt sums, the first stage's in-place first update and the final stage's two-word
+// update are never live in one kernel).
+template <class R, int MODEL, int STAGE>
+__global__ void __launch_bounds__(PHASE_BLOCK, SplitStageOcc<R, STAGE>::cell) grad_cells_kernel(Dev<R> d) {
+  constexpr int stage = STAGE;
   chain_begin();
   const int rule = stage_rule(stage);
   const int ncells = d.live_end[0];
@@ -1570,8 +1598,9 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::cell) grad_cells_ker
   }
 }
 
-template <class R, int MODEL, int FLUX>
-__global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::item) item_kernel(Dev<R> d, int stage) {
+template <class R, int MODEL, int FLUX, int STAGE>
+__global__ void __launch_bounds__(PHASE_BLOCK, SplitStageOcc<R, STAGE>::item) item_kernel(Dev<R> d) {
+  constexpr int stage = STAGE;
   chain_begin();
   const int rule = stage_rule(stage);
   const bool base = stage == STAGE_BASE || stage == STAGE_DIAG;  // spectral columns wanted
@@ -1631,8 +1660,9 @@ template <class R, int MODEL> struct ItemSlots {
   }
 };
 
-template <class R, int MODEL>
-__global__ void __launch_bounds__(PHASE_BLOCK, SplitOcc<R>::gather) gather_kernel(Dev<R> d, int stage) {
+template <class R, int MODEL, int STAGE>
+__global__ void __launch_bounds__(PHASE_BLOCK, SplitStageOcc<R, STAGE>::gather) gather_kernel(Dev<R> d) {
+  constexpr int stage = STAGE;
   chain_begin();
   const int rule = stage_rule(stage);
   const int ncells = d.live_end[0];

@@ -1,6 +1,8 @@
 // amr_engine_inst.cuh -- kernel dispatch, diagnostics reductions and the launch autotuner.
 // Included once per precision by amr_engine_f64.cu and amr_engine_f32.cu.
 #pragma once
+#include <type_traits>
+
 #include "amr_batch_impl.cuh"
 
 namespace amrb {
@@ -98,9 +100,9 @@ template <class R, int MODEL, int FLUX>
 static cudaError_t launch_split_t(const Dev<R>& d, bool srd, int trials, int mode, cudaStream_t st, int sms) {
   const int B = PHASE_BLOCK;
   const long long ncap = d.ncap, icap = (long long)d.cap_faces + d.cap_walls;
-  const int cblocks = (int)std::min<long long>((ncap + B - 1) / B, (long long)sms * SplitOcc<R>::cell);
-  const int gblocks = (int)std::min<long long>((ncap + B - 1) / B, (long long)sms * SplitOcc<R>::gather);
-  const int iblocks = (int)std::min<long long>((icap + B - 1) / B, (long long)sms * SplitOcc<R>::item);
+  // grids of one wave of co-resident blocks at each kernel's register budget
+  const auto cells_grid = [&](int per_sm) { return (int)std::min<long long>((ncap + B - 1) / B, (long long)sms * per_sm); };
+  const auto items_grid = [&](int per_sm) { return (int)std::min<long long>((icap + B - 1) / B, (long long)sms * per_sm); };
   const int fblocks = (int)std::min<long long>((ncap + 255) / 256, (long long)sms * 8);
   const int cases = d.n_cases;
   const int kblocks = (cases + 127) / 128;
@@ -110,10 +112,20 @@ static cudaError_t launch_split_t(const Dev<R>& d, bool srd, int trials, int mod
   const bool fused = MODEL >= MODEL_LAMINAR && !srd;
   Dev<R> dd = d;
   dd.fused_first = fused ? 1 : 0;
+  auto stage_kernels = [&](auto stage_tag) {
+    constexpr int S = decltype(stage_tag)::value;
+    using O = SplitStageOcc<R, S>;
+    if (MODEL >= MODEL_LAMINAR) chain(grad_cells_kernel<R, MODEL, S>, dim3(cells_grid(O::cell)), dim3(B), 0, st, dd);
+    chain(item_kernel<R, MODEL, FLUX, S>, dim3(items_grid(O::item)), dim3(B), 0, st, dd);
+    chain(gather_kernel<R, MODEL, S>, dim3(cells_grid(O::gather)), dim3(B), 0, st, dd);
+  };
   auto stage_seq = [&](int stage) {
-    if (MODEL >= MODEL_LAMINAR) chain(grad_cells_kernel<R, MODEL>, dim3(cblocks), dim3(B), 0, st, dd, stage);
-    chain(item_kernel<R, MODEL, FLUX>, dim3(iblocks), dim3(B), 0, st, dd, stage);
-    chain(gather_kernel<R, MODEL>, dim3(gblocks), dim3(B), 0, st, dd, stage);
+    switch (stage) {
+      case STAGE_BASE: stage_kernels(std::integral_constant<int, STAGE_BASE>{}); break;
+      case STAGE_1: stage_kernels(std::integral_constant<int, STAGE_1>{}); break;
+      case STAGE_2: stage_kernels(std::integral_constant<int, STAGE_2>{}); break;
+      default: stage_kernels(std::integral_constant<int, STAGE_DIAG>{}); break;
+    }
   };
   if (mode == MODE_RESIDUAL) {
     stage_seq(STAGE_DIAG);

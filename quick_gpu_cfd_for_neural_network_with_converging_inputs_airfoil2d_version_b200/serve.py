@@ -209,7 +209,9 @@ class Server:
                         res = results[r.id]
                         res.outcome, res.error, res.finished = 'failed', str(e), self.clock() - t0
                 ready.sort(key=lambda item: item[0].arrival)
-                while ready:
+                # first come, first served: never ahead of an earlier request whose mesh is building
+                oldest_building = min((b.arrival for b in building.values()), default=float('inf'))
+                while ready and ready[0][0].arrival < oldest_building:
                     r, mesh = ready[0]
                     placed = self._admit(r, mesh)
                     if placed is UNPLACEABLE or (placed is None and not live):
