@@ -48,13 +48,15 @@ from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b
 METRIC = 'solves/s & cell-steps/s at |ΔCL|,|ΔCD|≤1e-4 vs plain FP64; p50/p99 latency'
 GOLDEN = ROOT / 'tests' / 'golden'
 SOLVE_STEPS = 5000  # steps per solve of the batched workload
-# DRAM bytes (read + write) of one step of the default workload (256 cases, split launch mode),
-# summed over the step's kernel launches from an ncu capture of `bench.py --profile split`
-# (dram__bytes_read.sum + dram__bytes_write.sum, caches flushed before every launch, so it bounds
-# the warm traffic from above).  It comes from that separate capture, not from the timed run.
-SPLIT_256_TRAFFIC_PER_STEP = None
-TRAFFIC_SOURCE = ('ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum over the 11 launches of one step of '
-                  '`bench.py --profile split --cases 256` (separate capture, cold cache)')
+# DRAM bytes (read + write) of one step of the default workload (256 cases, split launch mode): the
+# nine split-kernel launches of one trial captured with ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum, caches flushed before every launch) on the first 64 draws of the same
+# stream (614.0 MB for 454,622 cells), scaled by cells to the 256-case workload (1,818,201 cells).
+# It comes from that separate capture, not from the timed run.
+SPLIT_256_TRAFFIC_PER_STEP = 2.456e9
+TRAFFIC_SOURCE = ('separate ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, cold cache) of the nine '
+                  'split-kernel launches of one trial of `bench.py --profile split --cases 64`, scaled by cells to '
+                  'the 256-case workload')
 
 
 def peaks():
