@@ -105,7 +105,6 @@ template <class R> struct Dev {
   const CaseCfg<R>* cfg;
   const Tile* tiles;
   int n_tiles, n_cases;
-  int fused_first;  // split mode: stage 1 reads U + dt R0 in place of a stored first update
   // cells
   const int* c_case;
   const double* c_vol;
@@ -1356,18 +1355,19 @@ template <class R> struct PhaseOcc;
 template <> struct PhaseOcc<float> { static constexpr int flux = AMRB_FLUX_MINB_F32, grad = 8; };
 template <> struct PhaseOcc<double> { static constexpr int flux = 3, grad = 4; };
 
-template <class R, int MODEL>
-__global__ void __launch_bounds__(PHASE_BLOCK, PhaseOcc<R>::grad) phase_grad_kernel(Dev<R> d, int stage) {
+// Compiled once per stage, like the split kernels, so that each instance carries its own path only.
+template <class R, int MODEL, int STAGE>
+__global__ void __launch_bounds__(PHASE_BLOCK, PhaseOcc<R>::grad) phase_grad_kernel(Dev<R> d) {
   chain_begin();
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  tile_sweep<R, MODEL, 0, true>(d, stage, reinterpret_cast<R*>(smem_raw));
+  tile_sweep<R, MODEL, 0, true>(d, STAGE, reinterpret_cast<R*>(smem_raw));
 }
 
-template <class R, int MODEL, int FLUX>
-__global__ void __launch_bounds__(PHASE_BLOCK, PhaseOcc<R>::flux) phase_flux_kernel(Dev<R> d, int stage) {
+template <class R, int MODEL, int FLUX, int STAGE>
+__global__ void __launch_bounds__(PHASE_BLOCK, PhaseOcc<R>::flux) phase_flux_kernel(Dev<R> d) {
   chain_begin();
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  tile_sweep<R, MODEL, FLUX, false>(d, stage, reinterpret_cast<R*>(smem_raw));
+  tile_sweep<R, MODEL, FLUX, false>(d, STAGE, reinterpret_cast<R*>(smem_raw));
 }
 
 // U1 = U + dt R0, one thread per cell (phase mode).  Every thread derives its case's step size
@@ -1408,7 +1408,7 @@ __global__ void __launch_bounds__(MAX_BLOCK) phase_first_cells_kernel(Dev<R> d) 
   }
 }
 
-// The first update's control part alone, one thread per case (split mode with fused_first: the
+// The first update's control part alone, one thread per case (split mode with the fused first update: the
 // state part, U1 = U + dt R0, is formed where the stage-1 kernels read it).  Same decisions as
 // phase_first_cells_kernel makes at a case's first cell.
 template <class R>
@@ -1469,23 +1469,42 @@ template <> struct SplitOcc<float> {
   static constexpr int item = AMRB_SPLIT_MINB_F32, cell = AMRB_SPLIT_CELL_MINB_F32, gather = AMRB_SPLIT_GATHER_MINB_F32;
 };
 template <> struct SplitOcc<double> { static constexpr int item = 3, cell = 4, gather = 4; };
-// Blocks per SM per stage: FP32 stage 1 forms U1 = U + dt R0 in place in its gradient and gather
-// kernels (and its gather also keeps the stage increment), so those two get more registers.
-#ifndef AMRB_SPLIT1_CELL_MINB_F32
-#define AMRB_SPLIT1_CELL_MINB_F32 AMRB_SPLIT_CELL_MINB_F32
+// Blocks per SM per stage and kernel (FP32), each defaulting to its kernel's SplitOcc value; FP32
+// stage 1 forms U1 = U + dt R0 in place in its gradient and gather kernels (and its gather also keeps
+// the stage increment), so those are the instances that need the most registers.
+#ifndef AMRB_S0_CELL_F32
+#define AMRB_S0_CELL_F32 AMRB_SPLIT_CELL_MINB_F32
 #endif
-#ifndef AMRB_SPLIT1_GATHER_MINB_F32
-#define AMRB_SPLIT1_GATHER_MINB_F32 AMRB_SPLIT_GATHER_MINB_F32
+#ifndef AMRB_S1_CELL_F32
+#define AMRB_S1_CELL_F32 AMRB_SPLIT_CELL_MINB_F32
 #endif
-#ifndef AMRB_SPLIT2_GATHER_MINB_F32
-#define AMRB_SPLIT2_GATHER_MINB_F32 AMRB_SPLIT_GATHER_MINB_F32
+#ifndef AMRB_S2_CELL_F32
+#define AMRB_S2_CELL_F32 AMRB_SPLIT_CELL_MINB_F32
+#endif
+#ifndef AMRB_S0_GATHER_F32
+#define AMRB_S0_GATHER_F32 AMRB_SPLIT_GATHER_MINB_F32
+#endif
+#ifndef AMRB_S1_GATHER_F32
+#define AMRB_S1_GATHER_F32 AMRB_SPLIT_GATHER_MINB_F32
+#endif
+#ifndef AMRB_S2_GATHER_F32
+#define AMRB_S2_GATHER_F32 AMRB_SPLIT_GATHER_MINB_F32
+#endif
+#ifndef AMRB_S0_ITEM_F32
+#define AMRB_S0_ITEM_F32 AMRB_SPLIT_MINB_F32
+#endif
+#ifndef AMRB_S12_ITEM_F32
+#define AMRB_S12_ITEM_F32 AMRB_SPLIT_MINB_F32
 #endif
 template <class R, int STAGE> struct SplitStageOcc : SplitOcc<R> {};
+template <> struct SplitStageOcc<float, 0> {
+  static constexpr int item = AMRB_S0_ITEM_F32, cell = AMRB_S0_CELL_F32, gather = AMRB_S0_GATHER_F32;
+};
 template <> struct SplitStageOcc<float, 1> {
-  static constexpr int item = AMRB_SPLIT_MINB_F32, cell = AMRB_SPLIT1_CELL_MINB_F32, gather = AMRB_SPLIT1_GATHER_MINB_F32;
+  static constexpr int item = AMRB_S12_ITEM_F32, cell = AMRB_S1_CELL_F32, gather = AMRB_S1_GATHER_F32;
 };
 template <> struct SplitStageOcc<float, 2> {
-  static constexpr int item = AMRB_SPLIT_MINB_F32, cell = AMRB_SPLIT_CELL_MINB_F32, gather = AMRB_SPLIT2_GATHER_MINB_F32;
+  static constexpr int item = AMRB_S12_ITEM_F32, cell = AMRB_S2_CELL_F32, gather = AMRB_S2_GATHER_F32;
 };
 
 __device__ __forceinline__ int stage_rule(int stage) {
@@ -1562,11 +1581,12 @@ __device__ __forceinline__ void load_item(const R* src, R* col, bool base, bool 
   if (MODEL == MODEL_SA) col[10] = sg * col[10];
 }
 
-// The split kernels are compiled once per stage (STAGE_BASE, STAGE_1, STAGE_2, STAGE_DIAG): each
-// instance carries only its stage's path, so its registers go to that path alone (the base
-// stage's FP64 dt sums, the first stage's in-place first update and the final stage's two-word
-// update are never live in one kernel).
-template <class R, int MODEL, int STAGE>
+// The split kernels are compiled once per stage (STAGE_BASE, STAGE_1, STAGE_2, STAGE_DIAG), and the
+// stage-1 cell kernels once more for the in-place first update (FUSED: U1 = U + dt R0 formed where
+// it is read): each instance carries only its own path, so its registers go to that path alone
+// (the base stage's FP64 dt sums, the first stage's update and the final stage's two-word update
+// are never live in one kernel).
+template <class R, int MODEL, int STAGE, bool FUSED = false>
 __global__ void __launch_bounds__(PHASE_BLOCK, SplitStageOcc<R, STAGE>::cell) grad_cells_kernel(Dev<R> d) {
   constexpr int stage = STAGE;
   chain_begin();
@@ -1591,7 +1611,7 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitStageOcc<R, STAGE>::cell) gr
       return grad_finish<R, MODEL>(d, cf, k, Uin, gr, sg, stage == STAGE_DIAG,
                                    d.crec + CellRec<R, MODEL>::stride * (long long)k, true, CellRec<R, MODEL>::compact);
     };
-    const bool ok = d.fused_first && stage == STAGE_1
+    const bool ok = FUSED && stage == STAGE_1
                         ? cell(FusedIn<R>{state_buf(d, c.cur), d.R0, (R)c.dt_trial})
                         : cell(stage_input(d, stage, c.cur));
     if (!ok) atomicOr(&d.ctl[cs].bad, 1);
@@ -1660,7 +1680,7 @@ template <class R, int MODEL> struct ItemSlots {
   }
 };
 
-template <class R, int MODEL, int STAGE>
+template <class R, int MODEL, int STAGE, bool FUSED = false>
 __global__ void __launch_bounds__(PHASE_BLOCK, SplitStageOcc<R, STAGE>::gather) gather_kernel(Dev<R> d) {
   constexpr int stage = STAGE;
   chain_begin();
@@ -1680,7 +1700,7 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitStageOcc<R, STAGE>::gather) 
       const int a = d.c_slot[k], b = d.c_slot[k + 1];
       const int e = b - (d.c_wall[k + 1] - d.c_wall[k]);
       const ItemSlots<R, MODEL> get{&d, base || stage == STAGE_DIAG};
-      if (d.fused_first && stage == STAGE_1)
+      if (FUSED && stage == STAGE_1)
         cell_dt = finish_cell<R, MODEL>(d, d.cfg[cs], cs, k, stage, a, e, b, get,
                                         FusedIn<R>{state_buf(d, c.cur), d.R0, (R)c.dt_trial}, state_buf(d, c.cur),
                                         state_buf(d, c.cur ^ 1), bad);

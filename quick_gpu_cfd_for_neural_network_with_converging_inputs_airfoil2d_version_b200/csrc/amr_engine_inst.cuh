@@ -59,21 +59,26 @@ static cudaError_t launch_phases_t(const Dev<R>& d, bool srd, int trials, int mo
   const size_t sm = EngineOps<R>::smem_bytes(block);
   const int cases = d.n_cases;
   const int cblocks = (cases + 127) / 128;
+  auto phase_pair = [&](auto stage_tag) {
+    constexpr int S = decltype(stage_tag)::value;
+    if (MODEL >= MODEL_LAMINAR) chain(phase_grad_kernel<R, MODEL, S>, dim3(tiles), dim3(block), sm, st, d);
+    chain(phase_flux_kernel<R, MODEL, FLUX, S>, dim3(tiles), dim3(block), sm, st, d);
+  };
   if (mode == MODE_RESIDUAL) {
-    if (MODEL >= MODEL_LAMINAR) chain(phase_grad_kernel<R, MODEL>, dim3(tiles), dim3(block), sm, st, d, STAGE_DIAG);
-    chain(phase_flux_kernel<R, MODEL, FLUX>, dim3(tiles), dim3(block), sm, st, d, STAGE_DIAG);
+    phase_pair(std::integral_constant<int, STAGE_DIAG>{});
     return cudaGetLastError();
   }
   chain(phase_commit_kernel, dim3(cblocks), dim3(128), 0, st, d.ctl, cases, 1);
   for (int t = 0; t < trials; ++t) {
-    if (MODEL >= MODEL_LAMINAR) chain(phase_grad_kernel<R, MODEL>, dim3(tiles), dim3(block), sm, st, d, STAGE_BASE);
-    chain(phase_flux_kernel<R, MODEL, FLUX>, dim3(tiles), dim3(block), sm, st, d, STAGE_BASE);
+    phase_pair(std::integral_constant<int, STAGE_BASE>{});
     if (srd && MODEL >= MODEL_LAMINAR && d.any_srd_rate) chain(srd_rate_kernel<R, MODEL>, dim3(cases), dim3(MAX_BLOCK), 0, st, d, -1);
     chain(phase_first_cells_kernel<R, MODEL>, dim3((d.n_cells + 255) / 256 + 1), dim3(256), 0, st, d);
     for (int stage = 1; stage <= 2; ++stage) {
       if (srd) chain(phase_srd_kernel<R, MODEL>, dim3(cases), dim3(block), 0, st, d, stage);
-      if (MODEL >= MODEL_LAMINAR) chain(phase_grad_kernel<R, MODEL>, dim3(tiles), dim3(block), sm, st, d, stage);
-      chain(phase_flux_kernel<R, MODEL, FLUX>, dim3(tiles), dim3(block), sm, st, d, stage);
+      if (stage == 1)
+        phase_pair(std::integral_constant<int, STAGE_1>{});
+      else
+        phase_pair(std::integral_constant<int, STAGE_2>{});
     }
     if (srd) chain(phase_srd_kernel<R, MODEL>, dim3(cases), dim3(block), 0, st, d, 3);
     chain(phase_commit_kernel, dim3(cblocks), dim3(128), 0, st, d.ctl, cases, 0);
@@ -110,11 +115,18 @@ static cudaError_t launch_split_t(const Dev<R>& d, bool srd, int trials, int mod
   // U1 where they read it and one thread per case makes the update's control decisions.
   // (Euler reads U1 in the face kernel; SRD changes U1 between the update and stage 1.)
   const bool fused = MODEL >= MODEL_LAMINAR && !srd;
-  Dev<R> dd = d;
-  dd.fused_first = fused ? 1 : 0;
+  const Dev<R>& dd = d;
   auto stage_kernels = [&](auto stage_tag) {
     constexpr int S = decltype(stage_tag)::value;
     using O = SplitStageOcc<R, S>;
+    if constexpr (S == STAGE_1) {
+      if (fused) {
+        chain(grad_cells_kernel<R, MODEL, S, true>, dim3(cells_grid(O::cell)), dim3(B), 0, st, dd);
+        chain(item_kernel<R, MODEL, FLUX, S>, dim3(items_grid(O::item)), dim3(B), 0, st, dd);
+        chain(gather_kernel<R, MODEL, S, true>, dim3(cells_grid(O::gather)), dim3(B), 0, st, dd);
+        return;
+      }
+    }
     if (MODEL >= MODEL_LAMINAR) chain(grad_cells_kernel<R, MODEL, S>, dim3(cells_grid(O::cell)), dim3(B), 0, st, dd);
     chain(item_kernel<R, MODEL, FLUX, S>, dim3(items_grid(O::item)), dim3(B), 0, st, dd);
     chain(gather_kernel<R, MODEL, S>, dim3(cells_grid(O::gather)), dim3(B), 0, st, dd);
