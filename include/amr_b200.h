@@ -344,6 +344,11 @@ int amr_device_memory(int32_t device, uint64_t* free_bytes, uint64_t* total_byte
 /* Evaluates the steady criteria for every live case whose next check time has been reached. */
 int amr_batch_check(amr_batch* batch, char* error, uint64_t error_size);
 int amr_batch_status(const amr_batch* batch, int32_t slot, amr_case_status_t* out);
+/* The accepted states of `count` cases, u_out[i][u_counts[i]] for slots[i] (u_counts[i] ==
+ * nv * n_cells of that case), in one staged copy with one synchronisation.  No counterpart in the
+ * reference, which downloads one session's state at a time. */
+int amr_batch_download_many(amr_batch* batch, uint64_t count, const int32_t* slots, double* const* u_out,
+                            const uint64_t* u_counts, char* error, uint64_t error_size);
 int amr_batch_download(amr_batch* batch, int32_t slot, double* u_out, uint64_t u_count,
                        char* error, uint64_t error_size);
 /* Compact results of one case, computed on the device from its accepted state, so a retired

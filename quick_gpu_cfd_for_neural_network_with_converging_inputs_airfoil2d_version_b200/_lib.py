@@ -34,6 +34,7 @@ SIGNATURES = {
     'amr_batch_check': (C.c_int, [_P, _S, C.c_uint64]),
     'amr_batch_status': (C.c_int, [_P, C.c_int32, _P]),
     'amr_batch_download': (C.c_int, [_P, C.c_int32, _P, C.c_uint64, _S, C.c_uint64]),
+    'amr_batch_download_many': (C.c_int, [_P, C.c_uint64, _P, _P, _P, _S, C.c_uint64]),
     'amr_batch_release': (C.c_int, [_P, C.c_int32]),
     'amr_batch_live_cases': (C.c_int, [_P]),
     'amr_batch_free_cells': (C.c_uint64, [_P]),

@@ -145,6 +145,19 @@ class Batch:
             raise BatchError(err.value.decode())
         return u
 
+    def download_many(self, slots):
+        """The accepted states of several cases (one staged copy, one synchronisation)."""
+        slots = list(slots)
+        outs = [np.empty(self.nv * self.ncells[s]) for s in slots]
+        n = len(slots)
+        if n == 0:
+            return []
+        err = errbuf()
+        if lib().amr_batch_download_many(self._h, n, (C.c_int32 * n)(*slots), (C.c_void_p * n)(*[u.ctypes.data for u in outs]),
+                                         (C.c_uint64 * n)(*[len(u) for u in outs]), err, len(err)):
+            raise BatchError(err.value.decode())
+        return outs
+
     def export(self, slot, mesh):
         """Device-computed compact results of a case (see StaticAmrGpu.export)."""
         from .snapshot import export_rows

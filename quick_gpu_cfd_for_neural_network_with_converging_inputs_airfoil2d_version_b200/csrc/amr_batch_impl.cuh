@@ -139,6 +139,13 @@ class PinnedStage {
     b.used += bytes;
     return p;
   }
+  // Whether take(bytes) would be served by the existing blocks (no new page-locked allocation).
+  bool can_take(size_t bytes) const {
+    bytes = (bytes + 255) & ~size_t(255);
+    for (size_t i = cur_; i < blocks_.size(); ++i)
+      if (blocks_[i].used + bytes <= blocks_[i].size) return true;
+    return false;
+  }
   // offset in the device staging buffer of a host address inside a block, or -1
   long long dev_offset(const void* host) const {
     const char* h = static_cast<const char*>(host);
@@ -354,7 +361,7 @@ template <class R> class Batch final : public BatchBase {
          w_ldon_.alloc(block_tiles_ ? cap_walls_ : 0, A, error, "walls");
     if (!ok) return false;
     if (model_ >= MODEL_LAMINAR) {
-      ok = crec_.alloc(CREC * nc, A, error, "scratch") && t_own_.alloc(cap_terms_, A, error, "terms") &&
+      ok = crec_.alloc(CREC * nc, A, error, "scratch") && t_own_.alloc(slot_fluxes_ ? cap_terms_ : 0, A, error, "terms") &&
            t_src_.alloc(cap_terms_, A, error, "terms") && t_x_.alloc(cap_terms_, A, error, "terms") &&
            t_y_.alloc(cap_terms_, A, error, "terms") && grad_.alloc(4 * nc, A, error, "scratch") &&
            mu_.alloc(nc, A, error, "scratch") && eddy_.alloc(nc, A, error, "scratch");
@@ -841,7 +848,7 @@ template <class R> class Batch final : public BatchBase {
     PVec<R> w_nx = pvu<R>(S, nw), w_ny = pvu<R>(S, nw), w_len = pvu<R>(S, nw), w_dist = pv<R>(S, nw, R(1));
     PVec<double> w_xm = pvu<double>(S, nw), w_ym = pvu<double>(S, nw);
     PVec<int> w_donor = pv<int>(S, nw, cb), w_owner = pvu<int>(S, nw);
-    PVec<int> t_own = pvu<int>(S, nt), t_src = pvu<int>(S, nt);
+    PVec<int> t_own = pvu<int>(S, sf ? nt : 0), t_src = pvu<int>(S, nt);  // t_own: slot-tile modes only
     PVec<R> t_x = pvu<R>(S, nt), t_y = pvu<R>(S, nt);
     PVec<int> f_case = pv<int>(S, nf, slot), f_own = pvu<int>(S, nf), f_nb = pvu<int>(S, nf), f_meta = pvu<int>(S, nf);
     PVec<R> f_len = pvu<R>(S, nf), f_geo = viscous ? pvu<R>(S, 6 * nf) : pv<R>(S, 6 * nf, R(0));
@@ -910,7 +917,7 @@ template <class R> class Batch final : public BatchBase {
       if (viscous)
         for (uint64_t q = m->visc_offsets[k]; q < m->visc_offsets[k + 1]; ++q) {
           const amr_gradient_term_t& t = m->visc_terms[q];
-          t_own[q] = cb + (int)k;
+          if (sf) t_own[q] = cb + (int)k;
           t_src[q] = t.source >= 0 ? cb + t.source : (t.source == -1 ? -1 : -2 - t.side);
           t_x[q] = (R)t.x;
           t_y[q] = (R)t.y;
@@ -1070,7 +1077,7 @@ template <class R> class Batch final : public BatchBase {
          up(st, bt_floc_.p + hc.tfaces.b, bt_floc, G) && up(st, s_loc_.p + sb, s_loc, G) &&
          up(st, w_ldon_.p + wb, w_ldon, G);  // the last five are empty without block tiles
     if (ok && viscous)
-      ok = up(st, t_own_.p + tb, t_own, G) && up(st, t_src_.p + tb, t_src, G) && up(st, t_x_.p + tb, t_x, G) &&
+      ok = (!sf || up(st, t_own_.p + tb, t_own, G)) && up(st, t_src_.p + tb, t_src, G) && up(st, t_x_.p + tb, t_x, G) &&
            up(st, t_y_.p + tb, t_y, G);
     if (ok && model_ == MODEL_SA) ok = up(st, c_wd_.p + cb, c_wd, G);
     for (int v = 0; ok && !uniform && v < nv_; ++v) {
@@ -1281,6 +1288,70 @@ template <class R> class Batch final : public BatchBase {
       stats_.full_downloads += 1;
     }
     return ok;
+  }
+
+  // Several cases' accepted states in one go: every case's rows (and, in FP32, its trailing words)
+  // are queued into page-locked staging, then one synchronisation, then the conversion to FP64.
+  int download_many(const std::vector<int>& slots, double* const* outs, const uint64_t* counts,
+                    std::string* error) override {
+    const size_t m = slots.size();
+    for (size_t i = 0; i < m; ++i) {
+      const int slot = slots[i];
+      if (slot < 0 || slot >= config_.max_cases || !cases_[slot].live) return fail1(error, "no such case");
+      if (!outs[i] || counts[i] != (uint64_t)(nv_ * cases_[slot].n)) return fail1(error, "state size mismatch");
+    }
+    const int words = L0_.p ? 2 : 1;
+    // The cases go through page-locked memory the batch already holds, as many per round as fit:
+    // the admission staging arena (idle outside admissions, which end synchronised), else the
+    // first stager's blocks (page-locking new memory runs at about 1 GB/s, so none is added).
+    PinnedStage& S = stagers_[0]->stage;
+    const size_t arena_bytes = arena_h_ ? (size_t)arena_stages_ * arena_slice_ : 0;
+    size_t arena_used = 0;
+    const auto grain = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const auto fits = [&](size_t b) { return arena_bytes ? arena_used + grain(b) <= arena_bytes : S.can_take(b); };
+    const auto take = [&](size_t b) -> void* {
+      if (!arena_bytes) return S.take(b);
+      void* p = arena_h_ + arena_used;
+      arena_used += grain(b);
+      return p;
+    };
+    std::vector<R*> tmp(m * words);
+    for (size_t i0 = 0; i0 < m;) {
+      S.reset();
+      arena_used = 0;
+      size_t i1 = i0;
+      for (; i1 < m; ++i1) {
+        const HostCase<R>& hc = cases_[slots[i1]];
+        const size_t bytes = sizeof(R) * nv_ * hc.n;
+        if (i1 > i0 && !fits(words * grain(bytes))) break;
+        if (i1 == i0 && arena_bytes && words * grain(bytes) > arena_bytes) return fail1(error, "download staging too small");
+        const int cur = h_ctl_[slots[i1]].cur;
+        for (int w = 0; w < words; ++w) {
+          const R* buf = w == 0 ? (cur ? U1_.p : U0_.p) : (cur ? L1_.p : L0_.p);
+          R* dst = static_cast<R*>(take(bytes));
+          tmp[i1 * words + w] = dst;
+          if (!cuda_ok(cudaMemcpy2DAsync(dst, sizeof(R) * hc.n, buf + hc.cells.b, sizeof(R) * cap_cells_,
+                                         sizeof(R) * hc.n, nv_, cudaMemcpyDeviceToHost, stream_),
+                       error, "download"))
+            return 1;
+        }
+      }
+      if (!cuda_ok(cudaStreamSynchronize(stream_), error, "download sync")) return 1;
+      // the conversion to FP64 (leading plus trailing word) on up to 8 host threads, case by case
+      const int threads = (int)std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency()));
+      parallel_for(i1 - i0, threads, [&](size_t j, int) {
+        const size_t i = i0 + j;
+        const R* hi = tmp[i * words];
+        const R* lo = words == 2 ? tmp[i * words + 1] : nullptr;
+        for (uint64_t q = 0; q < counts[i]; ++q) outs[i][q] = lo ? (double)hi[q] + (double)lo[q] : (double)hi[q];
+      });
+      for (size_t i = i0; i < i1; ++i) {
+        stats_.state_d2h_bytes += sizeof(R) * words * counts[i];
+        stats_.full_downloads += 1;
+      }
+      i0 = i1;
+    }
+    return 0;
   }
 
   int diagnostics(const std::vector<int>& slots, const std::vector<double>& rm, std::vector<double>* out,

@@ -515,6 +515,17 @@ int amr_batch_download(amr_batch* b, int32_t slot, double* u, uint64_t count, ch
   return 0;
 }
 
+int amr_batch_download_many(amr_batch* b, uint64_t count, const int32_t* slots, double* const* u_out,
+                            const uint64_t* u_counts, char* error, uint64_t error_size) {
+  if (!b || (count && (!slots || !u_out || !u_counts))) return 1;
+  std::string err;
+  if (b->batch->download_many(std::vector<int>(slots, slots + count), u_out, u_counts, &err)) {
+    put(error, error_size, err);
+    return 1;
+  }
+  return 0;
+}
+
 int amr_batch_release(amr_batch* b, int32_t slot) {
   if (!b) return 1;
   if (b->batch->release(slot)) return 1;

@@ -127,7 +127,8 @@ static cudaError_t launch_split_t(const Dev<R>& d, bool srd, int trials, int mod
         return;
       }
     }
-    if (MODEL >= MODEL_LAMINAR) chain(grad_cells_kernel<R, MODEL, S>, dim3(cells_grid(O::cell)), dim3(B), 0, st, dd);
+    if (MODEL >= MODEL_LAMINAR)
+      chain(grad_cells_kernel<R, MODEL, S>, dim3(cells_grid(O::cell)), dim3(B), 0, st, dd);
     chain(item_kernel<R, MODEL, FLUX, S>, dim3(items_grid(O::item)), dim3(B), 0, st, dd);
     chain(gather_kernel<R, MODEL, S>, dim3(cells_grid(O::gather)), dim3(B), 0, st, dd);
   };

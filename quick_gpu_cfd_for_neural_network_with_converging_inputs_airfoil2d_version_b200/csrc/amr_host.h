@@ -52,6 +52,8 @@ class BatchBase {
   virtual int residual(std::string* error) = 0;
   virtual int download_residual(int slot, double* out, uint64_t count, std::string* error) = 0;
   virtual int download(int slot, double* u, uint64_t count, std::string* error) = 0;
+  virtual int download_many(const std::vector<int>& slots, double* const* outs, const uint64_t* counts,
+                            std::string* error) = 0;
   // Compact results of one case from its accepted state, computed on the device: wall-stress
   // rows (14 per wall, viscous models), SA cell rows (3 per cell) and the convective and viscous
   // dt limits.  Runs one residual pass of the live cases first.

@@ -137,3 +137,19 @@ def test_uniform_start_filled_on_device_equals_staged_start(precision, mode):
         assert slots == ref_slots and steps == ref_steps
         for a, b in zip(states, ref_states):
             assert np.array_equal(a, b), bulk
+
+
+def test_download_many_equals_per_case_downloads():
+    """The bulk download returns every case's state exactly as one download per case does (both
+    FP32 words summed)."""
+    mix = sa_mix()
+    items = items_of(mix + mix[:1], 10)
+    b = Batch(precision=32, model=_abi.MODEL_LAMINAR, sa=True, max_cases=4,
+              max_cells=sum(m.n_cells for m, _, _, _ in items) + 1000, **MODES['split'])
+    slots = b.admit_many(items)
+    for _ in range(2):
+        b.advance(8)
+    bulk = b.download_many(slots[::-1])
+    for s, u in zip(slots[::-1], bulk):
+        assert np.array_equal(u, b.download(s))
+    b.destroy()
