@@ -793,6 +793,10 @@ def main():
     e2e = run_e2e(case_list, 32, args.steps, device=local, block=block, grid=grid, mode=mode)
     r.pop('batch').destroy()
     solve = None if args.no_solve else run_solve(case_list, SOLVE_STEPS, local, block, grid, mode)
+    if solve is not None:  # whole-job figures: every rank solves its own cases at the same time
+        solve['solves_per_s'] = dist_sum(solve['solves_per_s'], world)
+        solve['cell_steps_per_s'] = dist_sum(solve['cell_steps_per_s'], world)
+        solve['cases'] *= world
     clk.__exit__(None, None, None)
     e2e_value = dist_sum(e2e['value'], world)
     # roofline of the step: algorithmic bytes per launch / launch duration (CUDA events)
