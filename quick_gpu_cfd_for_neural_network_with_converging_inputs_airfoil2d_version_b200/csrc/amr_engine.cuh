@@ -863,12 +863,26 @@ __device__ __forceinline__ double finish_tail(const Dev<R>& d, const CaseCfg<R>&
   const Prim<R> wk = prim(Uin, n, k, g);
   if (!prim_ok(Uin, n, k, wk)) bad = true;
   R res[5];
-  for (int v = 0; v < 4; ++v) res[v] = (R)(-sum[v] / V);
-  if (MODEL >= MODEL_LAMINAR) {
-    for (int v = 0; v < 4; ++v) res[v] += (R)(vs[v] / V);
-    if (MODEL == MODEL_SA) {
-      res[4] = (R)(-snet / V) + d.ssrc[k];
-      if (!isfinite(res[4])) bad = true;
+  if constexpr (sizeof(R) == 4) {
+    // FP32 form: the residual in FP32 arithmetic, one reciprocal of the volume per cell (the FP64
+    // divisions by V cost more than the rest of the cell's sums); dt stays FP64 below
+    const R inv = R(1) / (R)V;
+    for (int v = 0; v < 4; ++v) res[v] = -sum[v] * inv;
+    if (MODEL >= MODEL_LAMINAR) {
+      for (int v = 0; v < 4; ++v) res[v] += vs[v] * inv;
+      if (MODEL == MODEL_SA) {
+        res[4] = -snet * inv + d.ssrc[k];
+        if (!isfinite(res[4])) bad = true;
+      }
+    }
+  } else {
+    for (int v = 0; v < 4; ++v) res[v] = (R)(-sum[v] / V);
+    if (MODEL >= MODEL_LAMINAR) {
+      for (int v = 0; v < 4; ++v) res[v] += (R)(vs[v] / V);
+      if (MODEL == MODEL_SA) {
+        res[4] = (R)(-snet / V) + d.ssrc[k];
+        if (!isfinite(res[4])) bad = true;
+      }
     }
   }
   const int nv = MODEL == MODEL_SA ? 5 : 4;
