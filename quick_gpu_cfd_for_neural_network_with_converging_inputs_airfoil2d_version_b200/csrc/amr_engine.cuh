@@ -887,14 +887,25 @@ __device__ __forceinline__ double finish_tail(const Dev<R>& d, const CaseCfg<R>&
   }
   const int nv = MODEL == MODEL_SA ? 5 : 4;
   if (base) {
-    if (spectral > R(0)) cell_dt = cf.cfl * d.c_area[k] / (double)spectral;
-    if (MODEL >= MODEL_LAMINAR) {
-      const double vdt = vspec > R(0) ? cf.viscous_cfl * V / (double)vspec : __longlong_as_double(0x7FF0000000000000ll);
-      double sdt = __longlong_as_double(0x7FF0000000000000ll);
+    double vdt = __longlong_as_double(0x7FF0000000000000ll), sdt = vdt;
+    if constexpr (sizeof(R) == 4) {
+      // FP32 form: the cell's limits are quotients of FP32 sums, formed in FP32 and widened; the
+      // per-case minimum, dt and time stay FP64
+      if (spectral > R(0)) cell_dt = (double)((R)(cf.cfl * d.c_area[k]) / spectral);
+      if (MODEL >= MODEL_LAMINAR && vspec > R(0)) vdt = (double)((R)(cf.viscous_cfl * V) / vspec);
+      if (MODEL == MODEL_SA) {
+        const R rate = R(2) * sspec / (wk.rho * (R)V) + d.srate[k];
+        if (rate > R(0)) sdt = (double)((R)cf.sa_cfl / rate);
+      }
+    } else {
+      if (spectral > R(0)) cell_dt = cf.cfl * d.c_area[k] / (double)spectral;
+      if (MODEL >= MODEL_LAMINAR && vspec > R(0)) vdt = cf.viscous_cfl * V / (double)vspec;
       if (MODEL == MODEL_SA) {
         const double rate = 2 * (double)sspec / ((double)wk.rho * V) + (double)d.srate[k];
-        sdt = rate > 0 ? cf.sa_cfl / rate : sdt;
+        if (rate > 0) sdt = cf.sa_cfl / rate;
       }
+    }
+    if (MODEL >= MODEL_LAMINAR) {
       if (cf.srd_rate) {
         d.ddt[n + k] = vdt;  // mapped through the SRD neighbourhoods before it joins the minimum
         cell_dt = rmin(cell_dt, sdt);
