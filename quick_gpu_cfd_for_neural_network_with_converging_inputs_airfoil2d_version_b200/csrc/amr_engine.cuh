@@ -25,6 +25,7 @@
 // never leaves the device.
 #pragma once
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "amr_physics.cuh"
@@ -812,10 +813,16 @@ template <class R> struct Cols {
   R v[SM_COLS];
 };
 
+// A slot getter whose face columns 0-3 are already net fluxes (convective minus viscous) and whose
+// walls yield only viscous columns 0 and 3 beside momentum columns 1-2 declares net_cols = true;
+// the cell then keeps one running sum per variable instead of separate viscous sums.
+template <class G, class = void> struct NetCols : std::false_type {};
+template <class G> struct NetCols<G, std::void_t<decltype(G::net_cols)>> : std::bool_constant<G::net_cols> {};
+
 // Per-cell end of the F phase: in-order sums of the cell's slot values (faces [a, e) in CSR order,
 // then walls [e, b)), residual, cell dt (base stage) and the stage update.  get(q, col) yields
 // the 12 values of slot q with the flux columns signed for cell k.  Returns the cell dt.
-template <class R, int MODEL, class In>
+template <class R, int MODEL, class In, bool NET = false>
 __device__ __forceinline__ double finish_tail(const Dev<R>& d, const CaseCfg<R>& cf, int cs, int k, int stage,
                                               const In& Uin, R* Ub, R* Un, const R* sum, const R* vs, R spectral, R vspec,
                                               R snet, R sspec, bool& bad);
@@ -830,7 +837,16 @@ __device__ __forceinline__ double finish_cell(const Dev<R>& d, const CaseCfg<R>&
     const bool wall = q >= e;
     const Cols<R> cc = get(q, wall);
     const R* col = cc.v;
-    if (!wall) {
+    if (NetCols<Get>::value) {
+      if (!wall) {
+        for (int v = 0; v < 4; ++v) sum[v] += col[v];
+      } else {
+        sum[0] -= col[4];
+        sum[1] += col[1];
+        sum[2] += col[2];
+        sum[3] -= col[7];
+      }
+    } else if (!wall) {
       for (int v = 0; v < 4; ++v) sum[v] += col[v];
     } else {
       sum[1] += col[1];
@@ -838,7 +854,8 @@ __device__ __forceinline__ double finish_cell(const Dev<R>& d, const CaseCfg<R>&
     }
     if (spec) spectral += col[8];
     if (MODEL >= MODEL_LAMINAR) {
-      for (int v = 0; v < 4; ++v) vs[v] += col[4 + v];
+      if (!NetCols<Get>::value)
+        for (int v = 0; v < 4; ++v) vs[v] += col[4 + v];
       if (spec) vspec += col[9];
     }
     if (MODEL == MODEL_SA) {
@@ -846,12 +863,13 @@ __device__ __forceinline__ double finish_cell(const Dev<R>& d, const CaseCfg<R>&
       if (spec) sspec += col[11];
     }
   }
-  return finish_tail<R, MODEL>(d, cf, cs, k, stage, Uin, Ub, Un, sum, vs, spectral, vspec, snet, sspec, bad);
+  return finish_tail<R, MODEL, In, NetCols<Get>::value>(d, cf, cs, k, stage, Uin, Ub, Un, sum, vs, spectral, vspec, snet,
+                                                        sspec, bad);
 }
 
 // The end of a cell's F phase after its in-order slot sums: residual, cell dt (base stage) and
 // the stage update, or the residual and dt limits of the diagnostics pass.  Returns the cell dt.
-template <class R, int MODEL, class In>
+template <class R, int MODEL, class In, bool NET>
 __device__ __forceinline__ double finish_tail(const Dev<R>& d, const CaseCfg<R>& cf, int cs, int k, int stage,
                                               const In& Uin, R* Ub, R* Un, const R* sum, const R* vs, R spectral, R vspec,
                                               R snet, R sspec, bool& bad) {
@@ -869,7 +887,8 @@ __device__ __forceinline__ double finish_tail(const Dev<R>& d, const CaseCfg<R>&
     const R inv = R(1) / (R)V;
     for (int v = 0; v < 4; ++v) res[v] = -sum[v] * inv;
     if (MODEL >= MODEL_LAMINAR) {
-      for (int v = 0; v < 4; ++v) res[v] += vs[v] * inv;
+      if (!NET)
+        for (int v = 0; v < 4; ++v) res[v] += vs[v] * inv;
       if (MODEL == MODEL_SA) {
         res[4] = -snet * inv + d.ssrc[k];
         if (!isfinite(res[4])) bad = true;
@@ -1692,6 +1711,7 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitStageOcc<R, STAGE>::item) it
 
 // The 12 values of a slot's face or wall record, flux columns signed for the slot's cell.
 template <class R, int MODEL> struct ItemSlots {
+  static constexpr bool net_cols = RecFormat<R, MODEL>::compact;
   const Dev<R>* d;
   bool base;
   __device__ __forceinline__ Cols<R> operator()(int q, bool wall) const {
