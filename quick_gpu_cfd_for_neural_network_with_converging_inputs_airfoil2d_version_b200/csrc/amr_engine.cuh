@@ -817,6 +817,9 @@ template <class R> struct Cols {
 // walls yield only viscous columns 0 and 3 beside momentum columns 1-2 declares net_cols = true;
 // the cell then keeps one running sum per variable instead of separate viscous sums.
 template <class G, class = void> struct NetCols : std::false_type {};
+#ifndef AMRB_GATHER_UNROLL
+#define AMRB_GATHER_UNROLL 2
+#endif
 template <class G> struct NetCols<G, std::void_t<decltype(G::net_cols)>> : std::bool_constant<G::net_cols> {};
 
 // Per-cell end of the F phase: in-order sums of the cell's slot values (faces [a, e) in CSR order,
@@ -833,7 +836,7 @@ __device__ __forceinline__ double finish_cell(const Dev<R>& d, const CaseCfg<R>&
   const bool base = stage == STAGE_BASE;
   const bool spec = base || stage == STAGE_DIAG;  // spectral sums wanted (dt, or the export's dt limits)
   R sum[4] = {0, 0, 0, 0}, vs[4] = {0, 0, 0, 0}, spectral = 0, vspec = 0, snet = 0, sspec = 0;
-  for (int q = a; q < b; ++q) {
+  const auto slot = [&](int q) {
     const bool wall = q >= e;
     const Cols<R> cc = get(q, wall);
     const R* col = cc.v;
@@ -862,6 +865,14 @@ __device__ __forceinline__ double finish_cell(const Dev<R>& d, const CaseCfg<R>&
       if (!wall) snet += col[10]; else snet -= col[10];
       if (spec) sspec += col[11];
     }
+  };
+  if constexpr (NetCols<Get>::value) {
+    // stored records: two slots' id and record loads in flight together
+    constexpr int kUnroll = AMRB_GATHER_UNROLL;
+#pragma unroll kUnroll
+    for (int q = a; q < b; ++q) slot(q);
+  } else {
+    for (int q = a; q < b; ++q) slot(q);
   }
   return finish_tail<R, MODEL, In, NetCols<Get>::value>(d, cf, cs, k, stage, Uin, Ub, Un, sum, vs, spectral, vspec, snet,
                                                         sspec, bad);
@@ -1736,14 +1747,20 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitStageOcc<R, STAGE>::gather) 
   // the loop bound is warp-uniform so the segmented shuffles below see full warps
   for (int k0 = blockIdx.x * blockDim.x; k0 < ncells; k0 += gridDim.x * blockDim.x) {
     const int k = k0 + threadIdx.x;
-    int cs = k < ncells ? d.c_case[k] : -1;
+    int cs = -1, a = 0, b = 0, nw = 0;
+    if (k < ncells) {
+      // the cell's own table loads go out together, ahead of its case's skip test
+      cs = d.c_case[k];
+      a = d.c_slot[k];
+      b = d.c_slot[k + 1];
+      nw = d.c_wall[k + 1] - d.c_wall[k];
+    }
     bool bad = false;
     double cell_dt = __longlong_as_double(0x7FF0000000000000ll);
     if (cs >= 0 && skip_case(d.ctl[cs], rule)) cs = -1;
     if (cs >= 0) {
       const CaseCtl& c = d.ctl[cs];
-      const int a = d.c_slot[k], b = d.c_slot[k + 1];
-      const int e = b - (d.c_wall[k + 1] - d.c_wall[k]);
+      const int e = b - nw;
       const ItemSlots<R, MODEL> get{&d, base || stage == STAGE_DIAG};
       if (FUSED && stage == STAGE_1)
         cell_dt = finish_cell<R, MODEL>(d, d.cfg[cs], cs, k, stage, a, e, b, get,
