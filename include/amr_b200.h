@@ -317,7 +317,7 @@ int amr_batch_admit(amr_batch* batch, const amr_mesh_view_t* mesh, const amr_par
                     int32_t* slot, char* error, uint64_t error_size);
 /* Admits `count` cases at once (entry i: meshes[i], params[i], u0[i][u0_counts[i]],
  * controls[i]), converting them into the engine layout on `threads` host threads (0 = up to
- * 8) with one stream synchronisation for the lot.  slots[i] receives the id or -1,
+ * 16) with one stream synchronisation for the lot.  slots[i] receives the id or -1,
  * status[i] 0 (admitted), 1 (invalid; the first such message goes to error) or 3 (no room).
  * Ids and arena placement follow the request order whatever the thread count, so the result
  * equals `count` amr_batch_admit calls.  Returns 1 if any case was invalid, else 3 if any

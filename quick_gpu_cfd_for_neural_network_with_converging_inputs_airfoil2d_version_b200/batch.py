@@ -76,7 +76,7 @@ class Batch:
 
     def admit_many(self, items, threads=0):
         """Admits (mesh, params, u0, control) tuples in one call, converting them on `threads`
-        host threads (0: up to 8).  Returns one slot per item (None where the arena had no
+        host threads (0: up to 16).  Returns one slot per item (None where the arena had no
         room); slots and placement equal those of admitting the items one by one, in order.
         Raises BatchError naming the first invalid item (the valid ones stay admitted; their
         slots are on the exception's `slots`)."""

@@ -14,6 +14,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <system_error>
@@ -92,6 +93,90 @@ template <class T> struct DevBuf {
   }
 };
 
+// Page-locked host memory shared by every batch of the process and lent for the length of one
+// call: admissions stage their tables in it and downloads land in it.  Page-locking runs at about
+// 1 GB/s, longer than preparing and filling a bulk admission of a few hundred cases takes, so a
+// block once locked is kept when given back (idle blocks up to 1 GB) and lent again.  Lending
+// and giving back are thread-safe.  The pool is never destroyed: the runtime may be gone at exit.
+class PinnedPool {
+ public:
+  struct Lease {
+    char* p = nullptr;
+    size_t size = 0;
+    bool fresh = false;  // page-locked for this lease
+  };
+  static PinnedPool& get() {
+    static PinnedPool* pool = new PinnedPool();
+    return *pool;
+  }
+  // The idle block that fits `want` most tightly, else the largest idle one of at least
+  // `least`, else a newly page-locked block of `want` bytes; an empty lease if that fails.
+  Lease lend(size_t least, size_t want) {
+    {
+      std::lock_guard<std::mutex> hold(m_);
+      int best = -1;
+      for (int i = 0; i < (int)idle_.size(); ++i)
+        if (idle_[i].size >= want && (best < 0 || idle_[i].size < idle_[best].size)) best = i;
+      if (best < 0)
+        for (int i = 0; i < (int)idle_.size(); ++i)
+          if (idle_[i].size >= least && (best < 0 || idle_[i].size > idle_[best].size)) best = i;
+      if (best >= 0) {
+        Lease l = idle_[best];
+        l.fresh = false;
+        idle_.erase(idle_.begin() + best);
+        idle_bytes_ -= l.size;
+        return l;
+      }
+    }
+    Lease l;
+    if (cudaHostAlloc(reinterpret_cast<void**>(&l.p), want, cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      return Lease();
+    }
+    l.size = want;
+    l.fresh = true;
+    return l;
+  }
+  // Takes a lease back (no copy from or to it may be in flight); frees the oldest idle blocks
+  // beyond the cap.
+  void give_back(const Lease& l) {
+    if (!l.p) return;
+    std::vector<Lease> drop;
+    {
+      std::lock_guard<std::mutex> hold(m_);
+      idle_.push_back(l);
+      idle_bytes_ += l.size;
+      while (idle_bytes_ > kKeep && !idle_.empty()) {
+        drop.push_back(idle_.front());
+        idle_bytes_ -= idle_.front().size;
+        idle_.erase(idle_.begin());
+      }
+    }
+    for (const Lease& d : drop) cudaFreeHost(d.p);
+  }
+
+ private:
+  static constexpr size_t kKeep = size_t(1) << 30;
+  std::mutex m_;
+  std::vector<Lease> idle_;
+  size_t idle_bytes_ = 0;
+};
+
+// A lease given back when the holder's scope ends, after the holder's stream has drained (so no
+// copy into it is still in flight on an error path).
+struct LeaseGuard {
+  cudaStream_t stream;
+  PinnedPool::Lease lease;
+  LeaseGuard(cudaStream_t s, const PinnedPool::Lease& l) : stream(s), lease(l) {}
+  LeaseGuard(const LeaseGuard&) = delete;
+  LeaseGuard& operator=(const LeaseGuard&) = delete;
+  ~LeaseGuard() {
+    if (!lease.p) return;
+    cudaStreamSynchronize(stream);
+    PinnedPool::get().give_back(lease);
+  }
+};
+
 // Host staging of one admission (or one download).  Tables are built straight into
 // page-locked blocks by a bump allocator that is reset per call, so an upload needs no
 // host-side copy: one DMA per used block into a device staging buffer laid out like the
@@ -138,13 +223,6 @@ class PinnedStage {
     void* p = b.p + b.used;
     b.used += bytes;
     return p;
-  }
-  // Whether take(bytes) would be served by the existing blocks (no new page-locked allocation).
-  bool can_take(size_t bytes) const {
-    bytes = (bytes + 255) & ~size_t(255);
-    for (size_t i = cur_; i < blocks_.size(); ++i)
-      if (blocks_[i].used + bytes <= blocks_[i].size) return true;
-    return false;
   }
   // offset in the device staging buffer of a host address inside a block, or -1
   long long dev_offset(const void* host) const {
@@ -422,8 +500,8 @@ template <class R> class Batch final : public BatchBase {
     slots->assign(count, -1);
     status->assign(count, 0);
     errors->assign(count, std::string());
-    // the fill is bound by host memory bandwidth, which 8 threads saturate on common hosts
-    if (threads <= 0) threads = (int)std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency()));
+    // preparing and filling 256 cases: 30 + 41 ms on 8 threads, 19 + 30 ms on 16, no gain beyond
+    if (threads <= 0) threads = (int)std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency()));
     threads = (int)std::max<size_t>(1, std::min<size_t>((size_t)threads, count));
     while ((int)stagers_.size() < threads) stagers_.emplace_back(new Stager());
     // The staging arena, sized by a bound over every request, is allocated on a helper thread
@@ -469,6 +547,7 @@ template <class R> class Batch final : public BatchBase {
       }
     }
     if (arena_thread.joinable()) arena_thread.join();
+    return_arena_host();  // every admission above ended synchronised
     return invalid ? 1 : (full ? 3 : 0);
   }
 
@@ -580,44 +659,62 @@ template <class R> class Batch final : public BatchBase {
                         block_tiles_ ? 2 * n : 0, block_tiles_ ? 2 * nf + 64 : 0, block_tiles_);
   }
 
-  // One page-locked host allocation and one device allocation, cut into `stages` equal slices
-  // that the first `stages` stagers adopt (allocation calls contend in the driver, so one large
-  // call replaces one per stage).  Grows only; every earlier upload has completed when called.
+  // The staging arena: one device allocation cut into `stages` equal slices that the first
+  // `stages` stagers use (grows only), and for the length of one call a page-locked host block of
+  // the same layout lent by the PinnedPool (allocation calls contend in the driver, so one large
+  // block replaces one per stage).  Every earlier upload has completed when called.
   bool ensure_arena(int stages, size_t slice, std::string* error) {
     slice = (slice + 4095) & ~size_t(4095);
-    if (stages <= arena_stages_ && slice <= arena_slice_) return true;
-    stages = std::max(stages, arena_stages_);
-    slice = std::max(slice, arena_slice_);
-    free_arena();
-    const size_t bytes = (size_t)stages * slice;
-    if (!cuda_ok(cudaHostAlloc(reinterpret_cast<void**>(&arena_h_), bytes, cudaHostAllocDefault), error,
-                 "staging arena") ||
-        !cuda_ok(cudaMalloc(reinterpret_cast<void**>(&arena_d_), bytes), error, "staging arena")) {
+    if (stages > arena_stages_ || slice > arena_slice_) {
+      stages = std::max(stages, arena_stages_);
+      slice = std::max(slice, arena_slice_);
       free_arena();
-      return false;
+      const size_t bytes = (size_t)stages * slice;
+      if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&arena_d_), bytes), error, "staging arena")) {
+        free_arena();
+        return false;
+      }
+      stats_.allocated_bytes += bytes;
+      arena_stages_ = stages;
+      arena_slice_ = slice;
+      for (int i = 0; i < stages; ++i) {
+        stagers_[i]->dev_ext = arena_d_ + (size_t)i * slice;
+        stagers_[i]->dev_ext_n = slice;
+      }
     }
-    stats_.pinned_bytes += bytes;
-    stats_.allocated_bytes += bytes;
-    arena_stages_ = stages;
-    arena_slice_ = slice;
-    for (int i = 0; i < stages; ++i) {
-      stagers_[i]->stage.adopt(arena_h_ + (size_t)i * slice, slice);
+    if (arena_lease_.p) return true;
+    const size_t bytes = (size_t)arena_stages_ * arena_slice_;
+    arena_lease_ = PinnedPool::get().lend(bytes, bytes);
+    if (!arena_lease_.p) return fail(error, "staging arena: page-locked allocation failed");
+    if (arena_lease_.fresh) stats_.pinned_bytes += arena_lease_.size;
+    arena_h_ = arena_lease_.p;
+    for (int i = 0; i < arena_stages_; ++i) {
+      stagers_[i]->stage.adopt(arena_h_ + (size_t)i * arena_slice_, arena_slice_);
       stagers_[i]->pinned_seen = stagers_[i]->stage.pinned_bytes();
-      stagers_[i]->dev_ext = arena_d_ + (size_t)i * slice;
-      stagers_[i]->dev_ext_n = slice;
     }
     return true;
   }
 
-  void free_arena() {
+  // Gives the arena's host block back to the pool at the end of a call, when every copy from it
+  // has completed.
+  void return_arena_host() {
+    if (!arena_lease_.p) return;
     for (int i = 0; i < arena_stages_ && i < (int)stagers_.size(); ++i) {
       stagers_[i]->stage.adopt(nullptr, 0);
+      stagers_[i]->pinned_seen = stagers_[i]->stage.pinned_bytes();
+    }
+    PinnedPool::get().give_back(arena_lease_);
+    arena_lease_ = PinnedPool::Lease();
+    arena_h_ = nullptr;
+  }
+
+  void free_arena() {
+    return_arena_host();
+    for (int i = 0; i < arena_stages_ && i < (int)stagers_.size(); ++i) {
       stagers_[i]->dev_ext = nullptr;
       stagers_[i]->dev_ext_n = 0;
     }
-    if (arena_h_) cudaFreeHost(arena_h_);
     if (arena_d_) cudaFree(arena_d_);
-    arena_h_ = nullptr;
     arena_d_ = nullptr;
     arena_stages_ = 0;
     arena_slice_ = 0;
@@ -1301,30 +1398,35 @@ template <class R> class Batch final : public BatchBase {
       if (!outs[i] || counts[i] != (uint64_t)(nv_ * cases_[slot].n)) return fail1(error, "state size mismatch");
     }
     const int words = L0_.p ? 2 : 1;
-    // The cases go through page-locked memory the batch already holds, as many per round as fit:
-    // the admission staging arena (idle outside admissions, which end synchronised), else the
-    // first stager's blocks (page-locking new memory runs at about 1 GB/s, so none is added).
-    PinnedStage& S = stagers_[0]->stage;
-    const size_t arena_bytes = arena_h_ ? (size_t)arena_stages_ * arena_slice_ : 0;
-    size_t arena_used = 0;
     const auto grain = [](size_t b) { return (b + 255) & ~size_t(255); };
-    const auto fits = [&](size_t b) { return arena_bytes ? arena_used + grain(b) <= arena_bytes : S.can_take(b); };
+    // The cases go through page-locked memory lent by the pool, as many per round as fit; after
+    // an admission the pool holds that admission's staging block, so nothing new is locked.
+    size_t least = 0, want = 0;
+    for (size_t i = 0; i < m; ++i) {
+      const size_t b = words * grain(sizeof(R) * nv_ * cases_[slots[i]].n);
+      least = std::max(least, b);
+      want += b;
+    }
+    want = std::max(least, std::min(want, size_t(64) << 20));
+    const LeaseGuard held(stream_, PinnedPool::get().lend(least, want));
+    if (!held.lease.p) return fail1(error, "download staging: page-locked allocation failed");
+    if (held.lease.fresh) stats_.pinned_bytes += held.lease.size;
+    const size_t arena_bytes = held.lease.size;
+    size_t arena_used = 0;
+    const auto fits = [&](size_t b) { return arena_used + grain(b) <= arena_bytes; };
     const auto take = [&](size_t b) -> void* {
-      if (!arena_bytes) return S.take(b);
-      void* p = arena_h_ + arena_used;
+      void* p = held.lease.p + arena_used;
       arena_used += grain(b);
       return p;
     };
     std::vector<R*> tmp(m * words);
     for (size_t i0 = 0; i0 < m;) {
-      S.reset();
       arena_used = 0;
       size_t i1 = i0;
       for (; i1 < m; ++i1) {
         const HostCase<R>& hc = cases_[slots[i1]];
         const size_t bytes = sizeof(R) * nv_ * hc.n;
         if (i1 > i0 && !fits(words * grain(bytes))) break;
-        if (i1 == i0 && arena_bytes && words * grain(bytes) > arena_bytes) return fail1(error, "download staging too small");
         const int cur = h_ctl_[slots[i1]].cur;
         for (int w = 0; w < words; ++w) {
           const R* buf = w == 0 ? (cur ? U1_.p : U0_.p) : (cur ? L1_.p : L0_.p);
@@ -1463,10 +1565,12 @@ template <class R> class Batch final : public BatchBase {
     const HostCase<R>& hc = cases_[slot];
     const long long n = hc.n;
     if (count != (uint64_t)(nv_ * n)) return fail1(error, "state size mismatch");
-    // one strided copy of the nv variable rows into page-locked staging
-    PinnedStage& S = stagers_[0]->stage;  // idle: every admission ends synchronised
-    S.reset();
-    R* tmp = static_cast<R*>(S.take(sizeof(R) * nv_ * n));
+    // one strided copy of the nv variable rows into page-locked staging lent by the pool
+    const size_t bytes = sizeof(R) * nv_ * n;
+    const LeaseGuard held(stream_, PinnedPool::get().lend(bytes, bytes));
+    if (!held.lease.p) return fail1(error, "download staging: page-locked allocation failed");
+    if (held.lease.fresh) stats_.pinned_bytes += held.lease.size;
+    R* tmp = reinterpret_cast<R*>(held.lease.p);
     if (!cuda_ok(cudaMemcpy2DAsync(tmp, sizeof(R) * n, buf + hc.cells.b, sizeof(R) * cap_cells_, sizeof(R) * n, nv_,
                                    cudaMemcpyDeviceToHost, stream_), error, "download"))
       return 1;
@@ -2061,7 +2165,8 @@ template <class R> class Batch final : public BatchBase {
   DevBuf<double> diag_part_, diag_out_, diag_cfg_, ddt_, ex_buf_;
   DevBuf<int> case_tiles_;
   std::vector<std::unique_ptr<Stager>> stagers_;  // two per admission worker; the first also serves downloads
-  char* arena_h_ = nullptr;                        // staging arena (ensure_arena)
+  char* arena_h_ = nullptr;                        // staging arena's host block, during a call
+  PinnedPool::Lease arena_lease_;                  // (ensure_arena, return_arena_host)
   unsigned char* arena_d_ = nullptr;
   size_t arena_slice_ = 0;
   int arena_stages_ = 0;
