@@ -53,7 +53,7 @@ SOLVE_STEPS = 5000  # steps per solve of the batched workload
 # dram__bytes_write.sum, caches flushed before every launch) on the first 64 draws of the same
 # stream (614.0 MB for 454,622 cells), scaled by cells to the 256-case workload (1,818,201 cells).
 # It comes from that separate capture, not from the timed run.
-SPLIT_256_TRAFFIC_PER_STEP = 2.456e9
+SPLIT_256_TRAFFIC_PER_STEP = 2.412e9
 TRAFFIC_SOURCE = ('separate ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, cold cache) of the nine '
                   'split-kernel launches of one trial of `bench.py --profile split --cases 64`, scaled by cells to '
                   'the 256-case workload')
