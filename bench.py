@@ -8,10 +8,11 @@ One step = one SSP-RK3 step (one trial) of every case in the batch.
 Workload `batched` (the default): 256 seeded NACA 4-digit airfoils (m~U[0,0.06], p~U[0.2,0.6],
 t~U[0.08,0.15]; a draw the mesh builder rejects is redrawn and counted), half on LF1 and half on
 LF2 meshes, SA-neg with Sutherland viscosity, HLLC, M~U[1.2,2.0], AoA~U[-3,5] deg, FP32 state with
-FP64 dt, norms and loads.  `value` is whole-job accepted cell-steps per second over exactly K timed
-steps, CUDA events on the engine's launch stream; `e2e` is the same work through the C ABI from
-host buffers (batch creation, mesh and state upload, the K steps, download of every state) on the
-host clock.  Beside it: a measured 5000-step solve of the same batch (solves/s), the plain FP64
+FP64 dt, norms and loads, in one arena (batch); with --arenas N the cases are dealt into N batches
+whose trials are in flight together (amr_batch_group_advance).  `value` is whole-job accepted
+cell-steps per second over exactly K timed steps, CUDA events from one start event to the last
+arena's end; `e2e` is the same work through the C ABI from host buffers (arena creation, mesh and
+state upload, the K steps, download of every state) on the host clock.  Beside it: a measured 5000-step solve of the same cases (solves/s), the plain FP64
 session on the same meshes, the plain FP64 inviscid Euler+SRD NACA 0012 LF1 case (200 steps) with
 the reference CPU core at 1 thread and at all host threads, and the reference CPU core on a
 bounded sample of the workload.
@@ -41,7 +42,8 @@ ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200 import _abi, cases, runs, workloads  # noqa: E402
-from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200.batch import Batch, case_control  # noqa: E402
+from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200.batch import (  # noqa: E402
+    Batch, case_control, group_advance)
 from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200.mesh import MeshArrays  # noqa: E402
 from quick_gpu_cfd_for_neural_network_with_converging_inputs_airfoil2d_version_b200.session import StaticAmrGpu, default_options  # noqa: E402
 
@@ -230,92 +232,111 @@ def admit_all(b, case_list, steps_cap=10 ** 9):
     return slots
 
 
-def run_batched(case_list, precision, steps, warmup, device=0, trials=32):
-    """Admit every case, autotune, warm up, then time exactly `steps` trials with CUDA events on the
-    engine stream.  Accepted cell-steps are counted per case from the device counters.  The NVML
-    sampler covers the timed loop alone."""
-    b = new_batch(case_list, precision, device)
-    slots = admit_all(b, case_list)
-    b.autotune(4)
+def arena_parts(case_list, arenas):
+    """The workload's cases dealt round-robin into `arenas` batches (LF1 and LF2 stay 1:1 in each)."""
+    return [case_list[i::arenas] for i in range(arenas)]
+
+
+def run_batched(case_list, precision, steps, warmup, device=0, trials=32, arenas=1):
+    """Admit every case into `arenas` batches, autotune each, warm up, then time exactly `steps`
+    trials of all of them with their work in flight together (amr_batch_group_advance: CUDA events
+    from one start event to the last batch's end).  Accepted cell-steps are counted per case from
+    the device counters.  The NVML sampler covers the timed loop alone."""
+    parts = arena_parts(case_list, arenas)
+    bs = [new_batch(part, precision, device) for part in parts]
+    slots = [admit_all(b, part) for b, part in zip(bs, parts)]
+    for b in bs:
+        b.autotune(4)
     done = 0
     while done < warmup:
         k = min(trials, warmup - done)
-        b.advance(k)
+        group_advance(bs, k)
         done += k
-    before = [b.status(s)['steps'] for s in slots]
-    launches0 = b.kernel_launches
+    before = [[b.status(x)['steps'] for x in sl] for b, sl in zip(bs, slots)]
+    launches0 = sum(b.kernel_launches for b in bs)
     dev_seconds, adv, advances = 0.0, 0, 0
     with NvmlSampler(device) as nvml:
         while adv < steps:
             k = min(trials, steps - adv)
-            b.advance(k)
-            dev_seconds += b.last_advance_seconds
+            dev_seconds += group_advance(bs, k)
             adv += k
             advances += 1
-    status = [b.status(s) for s in slots]
-    cell_steps = sum(m.n_cells * (st['steps'] - b0) for (_, m), st, b0 in zip(case_list, status, before))
-    return dict(batch=b, slots=slots, dev_seconds=dev_seconds, launches=b.kernel_launches - launches0,
-                cell_steps=cell_steps, status=status, config=b.launch_config(), advances=advances, nvml=nvml.summary())
+    status = [[b.status(x) for x in sl] for b, sl in zip(bs, slots)]
+    cell_steps = sum(m.n_cells * (st['steps'] - b0) for part, sts, bef in zip(parts, status, before)
+                     for (_, m), st, b0 in zip(part, sts, bef))
+    return dict(batches=bs, dev_seconds=dev_seconds, launches=sum(b.kernel_launches for b in bs) - launches0,
+                cell_steps=cell_steps, status=[x for sts in status for x in sts], config=bs[0].launch_config(),
+                advances=advances, nvml=nvml.summary(), arenas=arenas)
 
 
-def run_solve(case_list, nsteps, device, block, grid, mode, trials=32):
-    """A full solve of the batch: every case from its freestream start to `nsteps` accepted steps,
-    device time from CUDA events; solves/s = cases / that time (measured, not extrapolated)."""
-    b = new_batch(case_list, 32, device, block, grid, mode)
+def run_solve(case_list, nsteps, device, block, grid, mode, trials=32, arenas=1):
+    """A full solve of the workload: every case from its freestream start to `nsteps` accepted
+    steps, its arenas advanced together, device time from CUDA events; solves/s = cases / that
+    time (measured, not extrapolated)."""
+    parts = arena_parts(case_list, arenas)
+    bs = []
     try:
-        slots = admit_all(b, case_list, nsteps)
+        for part in parts:
+            bs.append(new_batch(part, 32, device, block, grid, mode))
+        slots = [admit_all(b, part, nsteps) for b, part in zip(bs, parts)]
         t0 = time.perf_counter()
         dev = 0.0
         polls = 0
         while True:
-            b.advance(trials)
-            dev += b.last_advance_seconds
+            dev += group_advance(bs, trials)
             polls += 1
-            st = [b.status(s) for s in slots]
+            st = [b.status(x) for b, sl in zip(bs, slots) for x in sl]
             if all(x['status'] == _abi.STATUS_MAXSTEPS for x in st) or polls > nsteps:
                 break
         wall = time.perf_counter() - t0
         steps = [x['steps'] for x in st]
-        cell_steps = sum(m.n_cells * x for (_, m), x in zip(case_list, steps))
-        return dict(steps_per_solve=nsteps, cases=len(case_list), device_seconds=dev, host_seconds=wall,
+        cells = [m.n_cells for part in parts for _, m in part]
+        cell_steps = sum(c * x for c, x in zip(cells, steps))
+        return dict(steps_per_solve=nsteps, cases=len(case_list), arenas=arenas, device_seconds=dev, host_seconds=wall,
                     solves_per_s=len(case_list) / dev, cell_steps_per_s=cell_steps / dev,
                     all_cases_completed=all(x == nsteps for x in steps), rejected=sum(x['rejected'] for x in st))
     finally:
-        b.destroy()
+        for b in bs:
+            b.destroy()
 
 
-def run_e2e(case_list, precision, steps, device=0, trials=32, block=0, grid=0, mode=0):
-    """The same work end to end through the C ABI from host buffers: batch creation, mesh and
-    state upload of every case (one bulk admission), `steps` trials with a control read-back per
-    launch, and the download of every final state; host wall clock."""
+def run_e2e(case_list, precision, steps, device=0, trials=32, block=0, grid=0, mode=0, arenas=1):
+    """The same work end to end through the C ABI from host buffers: creation of the arenas, mesh
+    and state upload of every case (one bulk admission per arena), `steps` trials of all arenas
+    together with a control read-back per launch, and the download of every final state (one bulk
+    download per arena); host wall clock."""
+    parts = arena_parts(case_list, arenas)
     t0 = time.perf_counter()
-    b = new_batch(case_list, precision, device, block, grid, mode)
+    bs = [new_batch(part, precision, device, block, grid, mode) for part in parts]
     t_create = time.perf_counter()
-    items, h2d = [], 0
-    for spec, mesh in case_list:
-        u0 = cases.uniform_state(mesh, spec.initial_primitive())  # filled on the device
-        items.append((mesh, spec.params(), u0, case_control(1e30, 10 ** 9, steady=False)))
-        h2d += mesh_bytes(mesh, precision) + u0.nbytes
+    items, h2d = [[] for _ in parts], 0
+    for lst, part in zip(items, parts):
+        for spec, mesh in part:
+            u0 = cases.uniform_state(mesh, spec.initial_primitive())  # filled on the device
+            lst.append((mesh, spec.params(), u0, case_control(1e30, 10 ** 9, steady=False)))
+            h2d += mesh_bytes(mesh, precision) + u0.nbytes
     t_items = time.perf_counter()
-    slots = b.admit_many(items)
+    slots = [b.admit_many(lst) for b, lst in zip(bs, items)]
     t_admit = time.perf_counter()
     adv, advances = 0, 0
     while adv < steps:
         k = min(trials, steps - adv)
-        b.advance(k)
+        group_advance(bs, k)
         adv += k
         advances += 1
     t_advance = time.perf_counter()
     d2h = 0
     cell_steps = 0
-    states = b.download_many(slots)  # one staged copy, one synchronisation
-    for (_, mesh), s, u in zip(case_list, slots, states):
-        d2h += u.nbytes * precision // 64 * 2  # leading and trailing FP32 words
-        cell_steps += mesh.n_cells * b.status(s)['steps']
+    for b, part, sl in zip(bs, parts, slots):
+        states = b.download_many(sl)  # one staged copy, one synchronisation
+        for (_, mesh), x, u in zip(part, sl, states):
+            d2h += u.nbytes * precision // 64 * 2  # leading and trailing FP32 words
+            cell_steps += mesh.n_cells * b.status(x)['steps']
     t_end = time.perf_counter()
     seconds = t_end - t0
-    d2h += advances * 96 * len(slots)  # per-launch control read-back
-    b.destroy()
+    d2h += advances * 96 * len(case_list)  # per-launch control read-back
+    for b in bs:
+        b.destroy()
     return dict(value=cell_steps / seconds, seconds=seconds, h2d=h2d, d2h=d2h,
                 phases=dict(create=t_create - t0, admit=t_admit - t_create, advance=t_advance - t_admit,
                             download=t_end - t_advance, admit_host_inputs=t_items - t_create))
@@ -737,6 +758,8 @@ def main():
     ap.add_argument('--cases', type=int, default=256)
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--no-solve', action='store_true', help='skip the measured full-solve leg')
+    ap.add_argument('--arenas', type=int, default=1,
+                    help='batched workload: arenas (batches) the cases are dealt into, advanced together')
     ap.add_argument('--profile', choices=['persistent', 'phases', 'split', 'tiled'], default=None,
                     help='only the timed batched loop, with this launch mode and --block (for ncu)')
     ap.add_argument('--block', type=int, default=128)
@@ -782,7 +805,7 @@ def main():
     dist_barrier(world)
     clk = ClockSampler(local, interval_ms=100)
     clk.__enter__()
-    r = run_batched(case_list, 32, args.steps, args.warmup, device=local)
+    r = run_batched(case_list, 32, args.steps, args.warmup, device=local, arenas=args.arenas)
     dev_seconds = dist_max(r['dev_seconds'], world)
     cell_steps = dist_sum(r['cell_steps'], world)
     value = cell_steps / dev_seconds
@@ -790,9 +813,11 @@ def main():
     block, grid, mode = parse_launch(cfg)
     # the end-to-end run comes before any batch is freed: a batch's teardown in the driver can take
     # up to a second and, overlapping the next batch's creation, slows that creation
-    e2e = run_e2e(case_list, 32, args.steps, device=local, block=block, grid=grid, mode=mode)
-    r.pop('batch').destroy()
-    solve = None if args.no_solve else run_solve(case_list, SOLVE_STEPS, local, block, grid, mode)
+    e2e = run_e2e(case_list, 32, args.steps, device=local, block=block, grid=grid, mode=mode, arenas=args.arenas)
+    for b in r.pop('batches'):
+        b.destroy()
+    solve = None if args.no_solve else run_solve(case_list, SOLVE_STEPS, local, block, grid, mode,
+                                                 arenas=args.arenas)
     if solve is not None:  # whole-job figures: every rank solves its own cases at the same time
         solve['solves_per_s'] = dist_sum(solve['solves_per_s'], world)
         solve['cell_steps_per_s'] = dist_sum(solve['cell_steps_per_s'], world)
@@ -815,7 +840,8 @@ def main():
                             meshes='seeded NACA 4-digit draws m~U[0,0.06] p~U[0.2,0.6] t~U[0.08,0.15], LF1:LF2 1:1, '
                                    'M~U[1.2,2], AoA~U[-3,5], SA-neg + Sutherland, HLLC, native mesh builder',
                             solve_steps=SOLVE_STEPS,
-                            l2='working set > L2 (no flush needed)', launch=cfg, parallelism='replicas'),
+                            l2='working set > L2 (no flush needed)', launch=cfg, arenas=args.arenas,
+                            parallelism='replicas'),
                 roofline=dict(bound='hbm', achieved=achieved, peak=hbm, unit='GB/s', frac=achieved / hbm,
                               peak_kind=peak_kind, traffic=traffic,
                               traffic_source=TRAFFIC_SOURCE if traffic else None,

@@ -336,6 +336,15 @@ int amr_batch_advance(amr_batch* batch, int32_t trials, char* error, uint64_t er
  * call on a batch between its two halves.  No counterpart in the reference. */
 int amr_batch_advance_async(amr_batch* batch, int32_t trials, char* error, uint64_t error_size);
 int amr_batch_wait(amr_batch* batch, char* error, uint64_t error_size);
+/* Runs `trials` trials of every live case of `count` batches of one device with their work in
+ * flight together: every batch's trials start after one start event, each on its own stream, so
+ * the kernels of one batch fill the tails of another's.  Each batch ends exactly as after its own
+ * amr_batch_advance.  *device_seconds (if not null) receives the device time from the start event
+ * to the last batch's end.  Returns 1 with a message for a null or repeated batch, batches on
+ * different devices or a failed advance (every advance that began is completed first).  No
+ * counterpart in the reference. */
+int amr_batch_group_advance(amr_batch* const* batches, int32_t count, int32_t trials, double* device_seconds,
+                            char* error, uint64_t error_size);
 /* Device bytes a batch allocated (arena, state, scratch and records). */
 uint64_t amr_batch_device_bytes(const amr_batch* batch);
 /* Free and total memory of CUDA device `device` (cudaMemGetInfo), for admission by free device

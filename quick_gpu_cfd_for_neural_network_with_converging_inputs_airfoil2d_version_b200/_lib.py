@@ -29,6 +29,7 @@ SIGNATURES = {
     'amr_batch_advance': (C.c_int, [_P, C.c_int32, _S, C.c_uint64]),
     'amr_batch_advance_async': (C.c_int, [_P, C.c_int32, _S, C.c_uint64]),
     'amr_batch_wait': (C.c_int, [_P, _S, C.c_uint64]),
+    'amr_batch_group_advance': (C.c_int, [_P, C.c_int32, C.c_int32, _P, _S, C.c_uint64]),
     'amr_batch_device_bytes': (C.c_uint64, [_P]),
     'amr_device_memory': (C.c_int, [C.c_int32, _P, _P]),
     'amr_batch_check': (C.c_int, [_P, _S, C.c_uint64]),

@@ -24,6 +24,19 @@ def device_memory(device=0):
     return free.value, total.value
 
 
+def group_advance(batches, trials=32):
+    """Runs `trials` trials of every batch (all on one device) with their work in flight together,
+    each on its own stream after one start event; returns the device seconds from that start to
+    the last batch's end.  Each batch ends exactly as after its own advance(trials)."""
+    n = len(batches)
+    handles = (C.c_void_p * n)(*[b._h for b in batches])
+    seconds = C.c_double()
+    err = errbuf()
+    if lib().amr_batch_group_advance(handles, n, int(trials), C.byref(seconds), err, len(err)):
+        raise BatchError(err.value.decode())
+    return seconds.value
+
+
 def case_control(tend, maxsteps, steady=True, mach=1.65, aoa=1.5, **kw):
     c = _abi.CaseControl()
     s = dict(cases.STEADY)

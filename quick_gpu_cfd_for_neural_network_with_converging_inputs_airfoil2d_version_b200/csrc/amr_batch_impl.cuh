@@ -1320,6 +1320,9 @@ template <class R> class Batch final : public BatchBase {
     return 0;
   }
 
+  cudaStream_t stream() const override { return stream_; }
+  int device() const override { return config_.device; }
+
   int advance_end(std::string* error) override {
     if (!in_flight_) return 0;
     in_flight_ = false;

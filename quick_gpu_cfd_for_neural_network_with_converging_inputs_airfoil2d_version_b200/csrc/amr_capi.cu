@@ -25,6 +25,11 @@ void put(char* buf, uint64_t size, const std::string& text) {
   buf[n] = 0;
 }
 
+int fail(char* buf, uint64_t size, const std::string& text) {
+  put(buf, size, text);
+  return 1;
+}
+
 double now() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
 
 std::unique_ptr<BatchBase> make_batch(const amr_batch_config_t& c, std::string* error) {
@@ -375,6 +380,67 @@ int amr_batch_wait(amr_batch* b, char* error, uint64_t error_size) {
     put(error, error_size, err);
     return 1;
   }
+  return 0;
+}
+
+int amr_batch_group_advance(amr_batch* const* batches, int32_t count, int32_t trials, double* device_seconds,
+                            char* error, uint64_t error_size) {
+  if (!batches || count < 1) return fail(error, error_size, "no batches");
+  for (int i = 0; i < count; ++i) {
+    if (!batches[i]) return fail(error, error_size, "null batch");
+    for (int j = 0; j < i; ++j)
+      if (batches[j] == batches[i]) return fail(error, error_size, "a batch appears twice");
+    if (batches[i]->batch->device() != batches[0]->batch->device())
+      return fail(error, error_size, "the batches are on different devices");
+  }
+  int previous = 0;
+  if (cudaGetDevice(&previous) != cudaSuccess || cudaSetDevice(batches[0]->batch->device()) != cudaSuccess)
+    return fail(error, error_size, "cannot select the batches' device");
+  std::string err;
+  std::vector<cudaEvent_t> ev(count + 1, nullptr);
+  bool ok = true;
+  for (int i = 0; ok && i <= count; ++i) ok = cudaEventCreate(&ev[i]) == cudaSuccess;
+  if (!ok) err = "event creation";
+  // every batch's work starts after one start event; each batch's end is recorded on its stream
+  if (ok && cudaEventRecord(ev[0], batches[0]->batch->stream()) != cudaSuccess) {
+    ok = false;
+    err = "start event";
+  }
+  for (int i = 1; ok && i < count; ++i)
+    if (cudaStreamWaitEvent(batches[i]->batch->stream(), ev[0], 0) != cudaSuccess) {
+      ok = false;
+      err = "stream ordering";
+    }
+  int begun = 0;
+  for (; ok && begun < count; ++begun)
+    if (batches[begun]->batch->advance_begin(trials, &err)) ok = false;
+  for (int i = 0; ok && i < count; ++i)
+    if (cudaEventRecord(ev[i + 1], batches[i]->batch->stream()) != cudaSuccess) {
+      ok = false;
+      err = "end event";
+    }
+  // complete every advance that began, also on an error path
+  for (int i = 0; i < begun; ++i) {
+    std::string e;
+    if (batches[i]->batch->advance_end(&e) && ok) {
+      ok = false;
+      err = e;
+    }
+  }
+  double seconds = 0.0;
+  for (int i = 0; ok && i < count; ++i) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, ev[0], ev[i + 1]) != cudaSuccess) {
+      ok = false;
+      err = "event timing";
+    }
+    seconds = std::max(seconds, 1e-3 * (double)ms);
+  }
+  for (cudaEvent_t e : ev)
+    if (e) cudaEventDestroy(e);
+  cudaSetDevice(previous);
+  if (!ok) return fail(error, error_size, err);
+  if (device_seconds) *device_seconds = seconds;
   return 0;
 }
 

@@ -1,6 +1,8 @@
 // amr_host.h -- host-side engine interface shared by the C ABI (amr_capi.cu) and the two
 // precision instantiations (amr_engine_f64.cu, amr_engine_f32.cu).
 #pragma once
+#include <cuda_runtime.h>
+
 #include <memory>
 #include <string>
 #include <vector>
@@ -46,6 +48,10 @@ class BatchBase {
   // advance in two halves: enqueue the trials (no wait), then wait and refresh the statuses.
   virtual int advance_begin(int trials, std::string* error) = 0;
   virtual int advance_end(std::string* error) = 0;
+  // The stream all of the batch's device work runs on (a group advance orders several batches'
+  // streams against one start event).
+  virtual cudaStream_t stream() const = 0;
+  virtual int device() const = 0;
   // Sets a case's target time and step cap (the session's advance arguments).
   virtual int set_target(int slot, double target, long long maxsteps, std::string* error) = 0;
   // Residual of every live case's accepted state into the engine's residual buffer.
