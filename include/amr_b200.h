@@ -339,8 +339,9 @@ int amr_batch_wait(amr_batch* batch, char* error, uint64_t error_size);
 /* Runs `trials` trials of every live case of `count` batches of one device with their work in
  * flight together: every batch's trials start after one start event, each on its own stream, so
  * the kernels of one batch fill the tails of another's.  Each batch ends exactly as after its own
- * amr_batch_advance.  *device_seconds (if not null) receives the device time from the start event
- * to the last batch's end.  Returns 1 with a message for a null or repeated batch, batches on
+ * amr_batch_advance.  *device_seconds (if not null) receives the device time from the start event,
+ * recorded after every batch's host-side preparation (uploads, graph captures), to the last batch's
+ * end.  Returns 1 with a message for a null or repeated batch, batches on
  * different devices or a failed advance (every advance that began is completed first).  No
  * counterpart in the reference. */
 int amr_batch_group_advance(amr_batch* const* batches, int32_t count, int32_t trials, double* device_seconds,

@@ -1291,7 +1291,10 @@ template <class R> class Batch final : public BatchBase {
   // First half of advance: everything up to the stream synchronisation (capture or replay of the
   // trials' graph, with the control read-back at its end), so that several batches can have
   // their trials in flight at once.  advance_end waits and refreshes the host-side statuses.
-  int advance_begin(int trials, std::string* error) override {
+  // The host-side preparation of an advance of `trials` trials: tile and range uploads and, when
+  // the case set or the trial count changed, the capture of the trials' graph.  advance_begin does
+  // it itself; a group advance does it for every batch before its start event.
+  int prepare_advance(int trials, std::string* error) override {
     if (in_flight_) return fail1(error, "an advance is already in flight");
     if (trials < 1 || trials > 1024) return fail1(error, "trials must be 1..1024");
     if (live_ == 0) return 0;
@@ -1302,6 +1305,12 @@ template <class R> class Batch final : public BatchBase {
         cudaGetLastError();
       }
     }
+    return 0;
+  }
+
+  int advance_begin(int trials, std::string* error) override {
+    if (prepare_advance(trials, error)) return 1;
+    if (live_ == 0) return 0;
     bool ok;
     cudaGetLastError();  // clear any stale error of an earlier runtime call
     if (use_graph_ && graph_exec_) {

@@ -399,8 +399,15 @@ int amr_batch_group_advance(amr_batch* const* batches, int32_t count, int32_t tr
   std::string err;
   std::vector<cudaEvent_t> ev(count + 1, nullptr);
   bool ok = true;
-  for (int i = 0; ok && i <= count; ++i) ok = cudaEventCreate(&ev[i]) == cudaSuccess;
-  if (!ok) err = "event creation";
+  // host-side preparation (uploads, graph captures) of every batch before the start event, so
+  // that the device time covers the trials alone
+  for (int i = 0; ok && i < count; ++i)
+    if (batches[i]->batch->prepare_advance(trials, &err)) ok = false;
+  for (int i = 0; ok && i <= count; ++i)
+    if (cudaEventCreate(&ev[i]) != cudaSuccess) {
+      ok = false;
+      err = "event creation";
+    }
   // every batch's work starts after one start event; each batch's end is recorded on its stream
   if (ok && cudaEventRecord(ev[0], batches[0]->batch->stream()) != cudaSuccess) {
     ok = false;

@@ -46,6 +46,7 @@ class BatchBase {
   // Runs `trials` trials of every live case and refreshes the host copies of the controls.
   virtual int advance(int trials, std::string* error) = 0;
   // advance in two halves: enqueue the trials (no wait), then wait and refresh the statuses.
+  virtual int prepare_advance(int trials, std::string* error) = 0;
   virtual int advance_begin(int trials, std::string* error) = 0;
   virtual int advance_end(std::string* error) = 0;
   // The stream all of the batch's device work runs on (a group advance orders several batches'
