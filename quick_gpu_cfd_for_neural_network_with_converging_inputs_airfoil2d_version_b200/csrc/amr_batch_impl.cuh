@@ -78,18 +78,47 @@ class RangeAlloc {
   std::map<long long, long long> free_;
 };
 
+// One device allocation carved into a batch's tables.  Each cudaMalloc of a few MB or more costs
+// about 0.3 ms whatever its size, and a batch has some 80 tables, so a batch's creation sizes them
+// all in a planning pass, makes one allocation and carves it in a second pass (256-byte aligned).
+struct Slab {
+  char* base = nullptr;
+  size_t used = 0;
+  bool planning = true;
+  void* take(size_t bytes) {
+    const size_t off = used;
+    used += (bytes + 255) & ~size_t(255);
+    return planning ? nullptr : base + off;
+  }
+};
+// The slab that DevBuf::alloc carves from on this host thread (none outside a batch's creation).
+inline thread_local Slab* g_slab = nullptr;
+struct SlabScope {
+  explicit SlabScope(Slab* s) { g_slab = s; }
+  ~SlabScope() { g_slab = nullptr; }
+};
+
 template <class T> struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  bool owned = false;  // allocated by itself (else carved from a slab)
   bool alloc(size_t count, uint64_t* counter, std::string* error, const char* what) {
     n = count ? count : 1;
+    if (g_slab) {
+      p = static_cast<T*>(g_slab->take(n * sizeof(T)));
+      owned = false;
+      if (!g_slab->planning && counter) *counter += n * sizeof(T);
+      return true;
+    }
     if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&p), n * sizeof(T)), error, what)) return false;
+    owned = true;
     if (counter) *counter += n * sizeof(T);
     return true;
   }
   void free() {
-    if (p) cudaFree(p);
+    if (p && owned) cudaFree(p);
     p = nullptr;
+    owned = false;
   }
 };
 
@@ -328,6 +357,68 @@ template <class R> class Batch final : public BatchBase {
   Batch() = default;
   ~Batch() override { destroy(); }
 
+  // The batch's device tables (DevBuf::alloc carves them from the slab in scope).
+  bool alloc_tables(const amr_batch_config_t& c, std::string* error) {
+    uint64_t* A = &stats_.allocated_bytes;
+    const long long nc = cap_cells_;
+    bool ok = ctl_.alloc(c.max_cases, A, error, "ctl") && cfg_.alloc(c.max_cases, A, error, "cfg") &&
+              tiles_.alloc(cap_tiles_, A, error, "tiles") && bar_.alloc(1, A, error, "barrier") &&
+              c_case_.alloc(nc, A, error, "cells") && c_vol_.alloc(nc, A, error, "cells") &&
+              c_area_.alloc(nc, A, error, "cells") && c_gvol_.alloc(nc, A, error, "cells") &&
+              c_flags_.alloc(nc, A, error, "cells") && c_slot_.alloc(nc, A, error, "cells") &&
+              c_wall_.alloc(nc, A, error, "cells") && c_term_.alloc(nc, A, error, "cells") &&
+              c_cx_.alloc(nc, A, error, "cells") && c_cy_.alloc(nc, A, error, "cells") &&
+              s_own_.alloc(slot_fluxes_ ? cap_slots_ : 0, A, error, "slots") && s_nb_.alloc(cap_slots_, A, error, "slots") &&
+              s_meta_.alloc(cap_slots_, A, error, "slots") && s_len_.alloc(cap_slots_, A, error, "slots") &&
+              w_nx_.alloc(cap_walls_, A, error, "walls") && w_ny_.alloc(cap_walls_, A, error, "walls") &&
+              w_len_.alloc(cap_walls_, A, error, "walls") && w_dist_.alloc(cap_walls_, A, error, "walls") &&
+              w_donor_.alloc(cap_walls_, A, error, "walls") && w_xm_.alloc(cap_walls_, A, error, "walls") &&
+              w_ym_.alloc(cap_walls_, A, error, "walls") &&
+              g_mem_.alloc(cap_groups_ + c.max_cases, A, error, "srd") && g_cell_.alloc(cap_gmem_, A, error, "srd") &&
+              g_cnt_.alloc(cap_gmem_, A, error, "srd") && g_vol_.alloc(cap_groups_ + c.max_cases, A, error, "srd") &&
+              q_cell_.alloc(cap_q_ + c.max_cases, A, error, "srd") && q_grp_.alloc(cap_q_ + c.max_cases, A, error, "srd") &&
+              q_list_.alloc(cap_qlist_, A, error, "srd") && q_cnt_.alloc(cap_q_ + c.max_cases, A, error, "srd") &&
+              qhat_.alloc(4 * (cap_groups_ + c.max_cases), A, error, "srd") &&
+              U0_.alloc(nv_ * nc, A, error, "state") && U1_.alloc(nv_ * nc, A, error, "state") &&
+              U2_.alloc(nv_ * nc, A, error, "state") && R0_.alloc(nv_ * nc, A, error, "state") &&
+              diag_part_.alloc(9 * cap_tiles_, A, error, "diag") && diag_out_.alloc(9 * c.max_cases, A, error, "diag") &&
+              diag_cfg_.alloc(7 * c.max_cases, A, error, "diag") && case_tiles_.alloc(2 * c.max_cases, A, error, "diag") &&
+              ddt_.alloc(2 * nc, A, error, "diag");
+    if (!ok) return false;
+    if (sizeof(R) == 4 && !(L0_.alloc(nv_ * nc, A, error, "state") && L1_.alloc(nv_ * nc, A, error, "state")))
+      return false;
+    if (sizeof(R) == 4 && model_ == MODEL_SA &&
+        !(fsa_.alloc(cap_faces_, A, error, "faces") && wsa_.alloc(cap_walls_, A, error, "walls")))
+      return false;
+    if (!s_geo_.alloc(slot_fluxes_ ? 6 * cap_slots_ : 0, A, error, "slots")) return false;
+    // face and wall records of the split launch mode
+    ok = s_item_.alloc(cap_slots_, A, error, "slots") && f_case_.alloc(cap_faces_, A, error, "faces") &&
+         f_own_.alloc(cap_faces_, A, error, "faces") && f_nb_.alloc(cap_faces_, A, error, "faces") &&
+         f_meta_.alloc(cap_faces_, A, error, "faces") && f_len_.alloc(cap_faces_, A, error, "faces") &&
+         f_geo_.alloc(6 * cap_faces_, A, error, "faces") && fval_.alloc(rec_stride() * cap_faces_, A, error, "faces") &&
+         w_owner_.alloc(cap_walls_, A, error, "walls") && wval_.alloc(rec_stride() * cap_walls_, A, error, "walls") &&
+         live_end_.alloc(4, A, error, "ranges") && btiles_.alloc(cap_btiles_, A, error, "block tiles") &&
+         bt_halo_.alloc(cap_halo_, A, error, "block tiles") && bt_face_.alloc(cap_tface_, A, error, "block tiles") &&
+         bt_floc_.alloc(cap_tface_, A, error, "block tiles") &&
+         s_loc_.alloc(block_tiles_ ? cap_slots_ : 0, A, error, "slots") &&
+         w_ldon_.alloc(block_tiles_ ? cap_walls_ : 0, A, error, "walls");
+    if (!ok) return false;
+    if (model_ >= MODEL_LAMINAR) {
+      ok = crec_.alloc(CREC * nc, A, error, "scratch") && t_own_.alloc(slot_fluxes_ ? cap_terms_ : 0, A, error, "terms") &&
+           t_src_.alloc(cap_terms_, A, error, "terms") && t_x_.alloc(cap_terms_, A, error, "terms") &&
+           t_y_.alloc(cap_terms_, A, error, "terms") && grad_.alloc(4 * nc, A, error, "scratch") &&
+           mu_.alloc(nc, A, error, "scratch") && eddy_.alloc(nc, A, error, "scratch");
+      if (!ok) return false;
+    }
+    if (model_ == MODEL_SA) {
+      ok = c_wd_.alloc(nc, A, error, "cells") && sgrad_.alloc(2 * nc, A, error, "scratch") &&
+           sdiff_.alloc(nc, A, error, "scratch") && ssrc_.alloc(nc, A, error, "scratch") &&
+           srate_.alloc(nc, A, error, "scratch");
+      if (!ok) return false;
+    }
+    return true;
+  }
+
   bool init(const amr_batch_config_t& c, std::string* error) {
     config_ = c;
     model_ = c.model == AMR_B200_MODEL_EULER ? MODEL_EULER : (c.sa_model ? MODEL_SA : MODEL_LAMINAR);
@@ -394,63 +485,21 @@ template <class R> class Batch final : public BatchBase {
     stagers_.emplace_back(new Stager());
     if (!cuda_ok(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), error, "stream")) return false;
     if (!cuda_ok(cudaEventCreate(&ev0_), error, "event") || !cuda_ok(cudaEventCreate(&ev1_), error, "event")) return false;
-    uint64_t* A = &stats_.allocated_bytes;
+    // every table in one slab: a planning pass sizes them, one allocation, a carving pass
+    Slab slab;
+    {
+      const SlabScope scope(&slab);
+      if (!alloc_tables(c, error)) return false;
+    }
+    if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&slab_), slab.used), error, "tables")) return false;
+    slab.base = slab_;
+    slab.used = 0;
+    slab.planning = false;
+    {
+      const SlabScope scope(&slab);
+      if (!alloc_tables(c, error)) return false;
+    }
     const long long nc = cap_cells_;
-    bool ok = ctl_.alloc(c.max_cases, A, error, "ctl") && cfg_.alloc(c.max_cases, A, error, "cfg") &&
-              tiles_.alloc(cap_tiles_, A, error, "tiles") && bar_.alloc(1, A, error, "barrier") &&
-              c_case_.alloc(nc, A, error, "cells") && c_vol_.alloc(nc, A, error, "cells") &&
-              c_area_.alloc(nc, A, error, "cells") && c_gvol_.alloc(nc, A, error, "cells") &&
-              c_flags_.alloc(nc, A, error, "cells") && c_slot_.alloc(nc, A, error, "cells") &&
-              c_wall_.alloc(nc, A, error, "cells") && c_term_.alloc(nc, A, error, "cells") &&
-              c_cx_.alloc(nc, A, error, "cells") && c_cy_.alloc(nc, A, error, "cells") &&
-              s_own_.alloc(slot_fluxes_ ? cap_slots_ : 0, A, error, "slots") && s_nb_.alloc(cap_slots_, A, error, "slots") &&
-              s_meta_.alloc(cap_slots_, A, error, "slots") && s_len_.alloc(cap_slots_, A, error, "slots") &&
-              w_nx_.alloc(cap_walls_, A, error, "walls") && w_ny_.alloc(cap_walls_, A, error, "walls") &&
-              w_len_.alloc(cap_walls_, A, error, "walls") && w_dist_.alloc(cap_walls_, A, error, "walls") &&
-              w_donor_.alloc(cap_walls_, A, error, "walls") && w_xm_.alloc(cap_walls_, A, error, "walls") &&
-              w_ym_.alloc(cap_walls_, A, error, "walls") &&
-              g_mem_.alloc(cap_groups_ + c.max_cases, A, error, "srd") && g_cell_.alloc(cap_gmem_, A, error, "srd") &&
-              g_cnt_.alloc(cap_gmem_, A, error, "srd") && g_vol_.alloc(cap_groups_ + c.max_cases, A, error, "srd") &&
-              q_cell_.alloc(cap_q_ + c.max_cases, A, error, "srd") && q_grp_.alloc(cap_q_ + c.max_cases, A, error, "srd") &&
-              q_list_.alloc(cap_qlist_, A, error, "srd") && q_cnt_.alloc(cap_q_ + c.max_cases, A, error, "srd") &&
-              qhat_.alloc(4 * (cap_groups_ + c.max_cases), A, error, "srd") &&
-              U0_.alloc(nv_ * nc, A, error, "state") && U1_.alloc(nv_ * nc, A, error, "state") &&
-              U2_.alloc(nv_ * nc, A, error, "state") && R0_.alloc(nv_ * nc, A, error, "state") &&
-              diag_part_.alloc(9 * cap_tiles_, A, error, "diag") && diag_out_.alloc(9 * c.max_cases, A, error, "diag") &&
-              diag_cfg_.alloc(7 * c.max_cases, A, error, "diag") && case_tiles_.alloc(2 * c.max_cases, A, error, "diag") &&
-              ddt_.alloc(2 * nc, A, error, "diag");
-    if (!ok) return false;
-    if (sizeof(R) == 4 && !(L0_.alloc(nv_ * nc, A, error, "state") && L1_.alloc(nv_ * nc, A, error, "state")))
-      return false;
-    if (sizeof(R) == 4 && model_ == MODEL_SA &&
-        !(fsa_.alloc(cap_faces_, A, error, "faces") && wsa_.alloc(cap_walls_, A, error, "walls")))
-      return false;
-    if (!s_geo_.alloc(slot_fluxes_ ? 6 * cap_slots_ : 0, A, error, "slots")) return false;
-    // face and wall records of the split launch mode
-    ok = s_item_.alloc(cap_slots_, A, error, "slots") && f_case_.alloc(cap_faces_, A, error, "faces") &&
-         f_own_.alloc(cap_faces_, A, error, "faces") && f_nb_.alloc(cap_faces_, A, error, "faces") &&
-         f_meta_.alloc(cap_faces_, A, error, "faces") && f_len_.alloc(cap_faces_, A, error, "faces") &&
-         f_geo_.alloc(6 * cap_faces_, A, error, "faces") && fval_.alloc(rec_stride() * cap_faces_, A, error, "faces") &&
-         w_owner_.alloc(cap_walls_, A, error, "walls") && wval_.alloc(rec_stride() * cap_walls_, A, error, "walls") &&
-         live_end_.alloc(4, A, error, "ranges") && btiles_.alloc(cap_btiles_, A, error, "block tiles") &&
-         bt_halo_.alloc(cap_halo_, A, error, "block tiles") && bt_face_.alloc(cap_tface_, A, error, "block tiles") &&
-         bt_floc_.alloc(cap_tface_, A, error, "block tiles") &&
-         s_loc_.alloc(block_tiles_ ? cap_slots_ : 0, A, error, "slots") &&
-         w_ldon_.alloc(block_tiles_ ? cap_walls_ : 0, A, error, "walls");
-    if (!ok) return false;
-    if (model_ >= MODEL_LAMINAR) {
-      ok = crec_.alloc(CREC * nc, A, error, "scratch") && t_own_.alloc(slot_fluxes_ ? cap_terms_ : 0, A, error, "terms") &&
-           t_src_.alloc(cap_terms_, A, error, "terms") && t_x_.alloc(cap_terms_, A, error, "terms") &&
-           t_y_.alloc(cap_terms_, A, error, "terms") && grad_.alloc(4 * nc, A, error, "scratch") &&
-           mu_.alloc(nc, A, error, "scratch") && eddy_.alloc(nc, A, error, "scratch");
-      if (!ok) return false;
-    }
-    if (model_ == MODEL_SA) {
-      ok = c_wd_.alloc(nc, A, error, "cells") && sgrad_.alloc(2 * nc, A, error, "scratch") &&
-           sdiff_.alloc(nc, A, error, "scratch") && ssrc_.alloc(nc, A, error, "scratch") &&
-           srate_.alloc(nc, A, error, "scratch");
-      if (!ok) return false;
-    }
     cudaMemsetAsync(ctl_.p, 0, sizeof(CaseCtl) * c.max_cases, stream_);
     cudaMemsetAsync(c_case_.p, 0xff, sizeof(int) * nc, stream_);
     cudaMemsetAsync(f_case_.p, 0xff, sizeof(int) * cap_faces_, stream_);
@@ -2100,6 +2149,8 @@ template <class R> class Batch final : public BatchBase {
 
   void DevBufFreeAll() {
     free_arena();
+    if (slab_) cudaFree(slab_);  // the carved tables below only forget their pointers
+    slab_ = nullptr;
     stagers_.clear();
     ctl_.free(); cfg_.free(); tiles_.free(); bar_.free();
     c_case_.free(); c_vol_.free(); c_area_.free(); c_gvol_.free(); c_flags_.free(); c_slot_.free(); c_wall_.free();
@@ -2177,6 +2228,7 @@ template <class R> class Batch final : public BatchBase {
   DevBuf<double> diag_part_, diag_out_, diag_cfg_, ddt_, ex_buf_;
   DevBuf<int> case_tiles_;
   std::vector<std::unique_ptr<Stager>> stagers_;  // two per admission worker; the first also serves downloads
+  char* slab_ = nullptr;                           // one allocation holding every table (alloc_tables)
   char* arena_h_ = nullptr;                        // staging arena's host block, during a call
   PinnedPool::Lease arena_lease_;                  // (ensure_arena, return_arena_host)
   unsigned char* arena_d_ = nullptr;
