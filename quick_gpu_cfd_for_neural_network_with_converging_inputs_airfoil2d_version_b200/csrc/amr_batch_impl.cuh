@@ -769,8 +769,10 @@ template <class R> class Batch final : public BatchBase {
     arena_slice_ = 0;
   }
 
-  // Index checks the table fills rely on: every face, wall, donor, gradient source and SRD
-  // index in range, offsets non-decreasing from zero, walls grouped by owner cell.
+  // Index checks the tables built before reservation rely on: offsets non-decreasing from zero,
+  // every listed face index, wall, donor and gradient source in range, walls grouped by owner
+  // cell, every face's cells and boundary marker consistent.  That each listed face names its
+  // cell fill() checks where it reads the face anyway (here too when block tiles are built).
   bool check_topology(const AdmitJob& j, std::string* why) const {
     const amr_mesh_view_t* m = j.spec.mesh;
     const long long n = j.n, nf = j.nf, nw = j.nw;
@@ -784,12 +786,10 @@ template <class R> class Batch final : public BatchBase {
       for (uint64_t q = m->face_offsets[k]; q < m->face_offsets[k + 1]; ++q) {
         const uint64_t fi = m->cell_faces[q];
         if (fi >= (uint64_t)nf) return fail(why, "cell_faces index out of range");
-        const amr_face_t& f = m->faces[fi];
-        const bool own_left = f.left == (int)k;
-        if (!own_left && f.right != (int)k) return fail(why, "cell_faces lists a face of another cell");
-        const int other = own_left ? f.right : f.left;
-        if (other >= (int)n) return fail(why, "face neighbour out of range");
-        if ((other < 0) != (f.boundary >= 0) || f.boundary > 3) return fail(why, "face boundary marker inconsistent");
+        if (block_tiles_) {  // the block tiles, built before fill(), follow the faces' cells
+          const amr_face_t& f = m->faces[fi];
+          if (f.left != (int)k && f.right != (int)k) return fail(why, "cell_faces lists a face of another cell");
+        }
       }
       const amr_cell_t& c = m->cells[k];
       if (c.wall_begin != (uint64_t)wpos) return fail(why, "walls are not grouped by owner cell");
@@ -1014,8 +1014,11 @@ template <class R> class Batch final : public BatchBase {
         const uint64_t fi = m->cell_faces[q];
         const amr_face_t& f = m->faces[fi];
         const bool own_left = f.left == (int)k;
+        if (!own_left && f.right != (int)k) return job_fail(j, 1, "cell_faces lists a face of another cell");
         const int other = own_left ? f.right : f.left;
         const int side = f.boundary;
+        if (other >= (int)n) return job_fail(j, 1, "face neighbour out of range");
+        if ((other < 0) != (side >= 0) || side > 3) return job_fail(j, 1, "face boundary marker inconsistent");
         const int kind = side >= 0 ? kinds[side] : 0;
         if (sf) s_own[spos] = cb + (int)k;
         s_nb[spos] = other >= 0 ? cb + other : -1;

@@ -153,3 +153,28 @@ def test_download_many_equals_per_case_downloads():
     for s, u in zip(slots[::-1], bulk):
         assert np.array_equal(u, b.download(s))
     b.destroy()
+
+
+def test_face_listing_error_found_in_fill_releases_the_case():
+    """A mesh whose cell lists a face of another cell (indices in range) is refused while its
+    tables are filled, after its slot was reserved: the entry reports the error, its slot and
+    ranges are released, and a valid case admitted next computes bit for bit as alone."""
+    import dataclasses
+    mix = sa_mix()
+    items = items_of(mix, 8)
+    mesh, params, u0, ctl = items[0]
+    cf = mesh.cell_faces.copy()
+    cf[int(mesh.face_offsets[0])] = cf[int(mesh.face_offsets[-2])]  # cell 0 lists the last cell's face
+    bad = (dataclasses.replace(mesh, cell_faces=cf), params, u0, ctl)
+    b = Batch(precision=32, model=_abi.MODEL_LAMINAR, sa=True, max_cases=1,
+              max_cells=max(m.n_cells for _, m in mix) + 1000, **MODES['split'])
+    with pytest.raises(BatchError, match='lists a face of another cell'):
+        b.admit_many([bad])
+    with pytest.raises(BatchError, match='lists a face of another cell'):
+        b.admit(*bad)
+    slot = b.admit(*items[2])
+    assert slot == 0
+    b.advance(16)
+    alone = run([items[2]], 32, 'split', 1, 2, bulk=False)[1][0]
+    assert np.array_equal(b.download(slot), alone)
+    b.destroy()
