@@ -483,6 +483,26 @@ int amr_write_snapshot_files(const char* prefix, const amr_mesh_view_t* mesh, co
                              int64_t rejected, const char* backend, const amr_export_rows_t* rows, char* error,
                              uint64_t error_size);
 
+/* Tuning and introspection.  None has a counterpart in the reference. */
+/* Sets a case's advance target time and step cap (the driver's stop time and max steps). */
+int amr_batch_set_target(amr_batch* batch, int32_t slot, double target, int64_t maxsteps, char* error,
+                         uint64_t error_size);
+/* Evaluates the residual of every live case's accepted state (no update) and copies case `slot`'s
+ * (nv * n_cells values, SoA) to r. */
+int amr_batch_residual(amr_batch* batch, int32_t slot, double* r, uint64_t count, char* error, uint64_t error_size);
+/* Replays advances from CUDA graphs (on, the default) or launches their kernels directly. */
+int amr_batch_set_graph(amr_batch* batch, int32_t on);
+/* Split launch mode, viscous models without SRD: the live cases run as `lanes` (1 or 2) independent
+ * chains of kernels on two streams, each over about half the cells, so that one chain's kernels
+ * fill the tails of the other's.  Two lanes need every case of the first half to lie below every
+ * case of the second in the arena (as after admissions in one order); otherwise one lane runs. */
+int amr_batch_set_lanes(amr_batch* batch, int32_t lanes);
+/* The launch configuration chosen (mode, block, grid, graph or direct, lanes) as text. */
+int amr_batch_launch_config(const amr_batch* batch, char* out, uint64_t size);
+int amr_gpu_launch_config(const amr_gpu_session* session, char* out, uint64_t size);
+/* Kernels the session launched so far. */
+uint64_t amr_gpu_kernel_launches(const amr_gpu_session* session);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,6 +58,7 @@ SIGNATURES = {
     'amr_batch_autotune': (C.c_int, [_P, C.c_int32, _S, C.c_uint64]),
     'amr_batch_launch_config': (C.c_int, [_P, _S, C.c_uint64]),
     'amr_batch_set_graph': (C.c_int, [_P, C.c_int32]),
+    'amr_batch_set_lanes': (C.c_int, [_P, C.c_int32]),
     'amr_batch_set_target': (C.c_int, [_P, C.c_int32, C.c_double, C.c_int64, _S, C.c_uint64]),
     'amr_batch_residual': (C.c_int, [_P, C.c_int32, _P, C.c_uint64, _S, C.c_uint64]),
     'amr_gpu_launch_config': (C.c_int, [_P, _S, C.c_uint64]),

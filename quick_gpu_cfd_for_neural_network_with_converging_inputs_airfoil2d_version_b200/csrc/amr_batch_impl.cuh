@@ -361,7 +361,8 @@ template <class R> class Batch final : public BatchBase {
   bool alloc_tables(const amr_batch_config_t& c, std::string* error) {
     uint64_t* A = &stats_.allocated_bytes;
     const long long nc = cap_cells_;
-    bool ok = ctl_.alloc(c.max_cases, A, error, "ctl") && cfg_.alloc(c.max_cases, A, error, "cfg") &&
+    bool ok = lane_ranges_.alloc(16, A, error, "lanes") && case_lane_.alloc(c.max_cases, A, error, "lanes") &&
+              ctl_.alloc(c.max_cases, A, error, "ctl") && cfg_.alloc(c.max_cases, A, error, "cfg") &&
               tiles_.alloc(cap_tiles_, A, error, "tiles") && bar_.alloc(1, A, error, "barrier") &&
               c_case_.alloc(nc, A, error, "cells") && c_vol_.alloc(nc, A, error, "cells") &&
               c_area_.alloc(nc, A, error, "cells") && c_gvol_.alloc(nc, A, error, "cells") &&
@@ -484,6 +485,11 @@ template <class R> class Batch final : public BatchBase {
     stagers_.clear();
     stagers_.emplace_back(new Stager());
     if (!cuda_ok(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), error, "stream")) return false;
+    // the split mode's second lane: its stream and the events that fork it off and join it
+    if (!cuda_ok(cudaStreamCreateWithFlags(&aux_, cudaStreamNonBlocking), error, "stream") ||
+        !cuda_ok(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), error, "event") ||
+        !cuda_ok(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), error, "event"))
+      return false;
     if (!cuda_ok(cudaEventCreate(&ev0_), error, "event") || !cuda_ok(cudaEventCreate(&ev1_), error, "event")) return false;
     // every table in one slab: a planning pass sizes them, one allocation, a carving pass
     Slab slab;
@@ -1542,6 +1548,11 @@ template <class R> class Batch final : public BatchBase {
     graph_dirty_ = true;
   }
 
+  void set_lanes(int lanes) override {
+    lanes_wanted_ = lanes;
+    tiles_dirty_ = true;  // the next advance plans the lanes again
+  }
+
   std::string launch_config() const override {
     const char* name = mode_ == AMR_B200_LAUNCH_PHASES  ? "mode=phases"
                        : mode_ == AMR_B200_LAUNCH_SPLIT ? "mode=split"
@@ -1552,7 +1563,8 @@ template <class R> class Batch final : public BatchBase {
                      : mode_ == AMR_B200_LAUNCH_TILED ? sms_ * TiledOcc<R>::blocks
                                                       : grid_;
     return std::string(name) + " block=" + std::to_string(block_) + " grid=" + std::to_string(grid) +
-           (use_graph_ ? " graph" : " direct");
+           (use_graph_ ? " graph" : " direct") +
+           (mode_ == AMR_B200_LAUNCH_SPLIT && lanes_ > 1 ? " lanes=" + std::to_string(lanes_) : "");
   }
   int autotune(int trials, std::string* error) override;
   void restore(const std::vector<CaseCtl>& ctl_save, const DevBuf<R>& s0, const DevBuf<R>& s1, long long nbytes);
@@ -1895,6 +1907,55 @@ template <class R> class Batch final : public BatchBase {
     m.cur = c.cur;
   }
 
+  // Split mode, viscous models without SRD: the live cases in two lanes of about equal cells, each
+  // advanced by its own chain of kernels (so that one lane's kernels fill the tails of the
+  // other's).  A lane must own whole ranges: every first-lane case's cells, faces and walls lie
+  // below every second-lane case's, as they do after admissions in one order; otherwise (or with
+  // fewer than two cases) one lane.
+  bool plan_lanes(std::string* error) {
+    lanes_ = 1;
+    if (lanes_wanted_ < 2 || mode_ != AMR_B200_LAUNCH_SPLIT || model_ < MODEL_LAMINAR || any_srd()) return true;
+    std::vector<int> live;
+    for (int i = 0; i < config_.max_cases; ++i)
+      if (cases_[i].live) live.push_back(i);
+    if (live.size() < 2) return true;
+    std::sort(live.begin(), live.end(), [&](int a, int b) { return cases_[a].cells.b < cases_[b].cells.b; });
+    long long total = 0, acc = 0;
+    for (int i : live) total += cases_[i].cells.n;
+    size_t cut = 1;
+    for (size_t q = 0; q + 1 < live.size(); ++q) {
+      acc += cases_[live[q]].cells.n;
+      cut = q + 1;
+      if (2 * acc >= total) break;
+    }
+    // lane 0: [0, begin of lane 1) in every table; lane 1: from there to the live ends
+    long long end0[3] = {0, 0, 0}, begin1[3] = {hw_cells_, hw_faces_, hw_walls_};
+    for (size_t q = 0; q < live.size(); ++q) {
+      const HostCase<R>& hc = cases_[live[q]];
+      const Range r[3] = {hc.cells, hc.faces, hc.walls};
+      for (int t = 0; t < 3; ++t) {
+        if (r[t].n == 0) continue;
+        if (q < cut) end0[t] = std::max(end0[t], r[t].b + r[t].n);
+        else begin1[t] = std::min(begin1[t], r[t].b);
+      }
+    }
+    for (int t = 0; t < 3; ++t)
+      if (end0[t] > begin1[t]) return true;  // interleaved ranges: one lane
+    const int h[16] = {(int)begin1[0], (int)begin1[1], (int)begin1[2], h_live_end_[3], 0, 0, 0, 0,
+                       (int)hw_cells_, (int)hw_faces_, (int)hw_walls_, h_live_end_[3],
+                       (int)begin1[0], (int)begin1[1], (int)begin1[2], 0};
+    std::copy(h, h + 16, h_lane_ranges_);
+    h_case_lane_.assign(config_.max_cases, -1);
+    for (size_t q = 0; q < live.size(); ++q) h_case_lane_[live[q]] = q < cut ? 0 : 1;
+    if (!cuda_ok(cudaMemcpyAsync(lane_ranges_.p, h_lane_ranges_, sizeof(h_lane_ranges_), cudaMemcpyHostToDevice, stream_),
+                 error, "lanes") ||
+        !cuda_ok(cudaMemcpyAsync(case_lane_.p, h_case_lane_.data(), sizeof(int) * h_case_lane_.size(),
+                                 cudaMemcpyHostToDevice, stream_), error, "lanes"))
+      return false;
+    lanes_ = 2;
+    return true;
+  }
+
   bool sync_tiles(std::string* error) {
     if (!tiles_dirty_) return true;
     std::vector<Tile> all;
@@ -1915,6 +1976,7 @@ template <class R> class Batch final : public BatchBase {
     h_live_end_[0] = (int)hw_cells_;
     h_live_end_[1] = (int)hw_faces_;
     h_live_end_[2] = (int)hw_walls_;
+    if (!plan_lanes(error)) return false;
     std::vector<BTile> all_bt;
     for (auto& c : cases_)
       if (c.live) all_bt.insert(all_bt.end(), c.btiles.begin(), c.btiles.end());
@@ -1936,7 +1998,7 @@ template <class R> class Batch final : public BatchBase {
     // a split-mode graph reads the live ranges from the device and keeps its grids; it is
     // recaptured only when the set of kernels changes (SRD launches appear or vanish)
     if ((mode_ != AMR_B200_LAUNCH_SPLIT && mode_ != AMR_B200_LAUNCH_TILED) || any_srd() != graph_srd_ ||
-        any_srd_rate() != graph_srd_rate_)
+        any_srd_rate() != graph_srd_rate_ || lanes_ != graph_lanes_)
       graph_dirty_ = true;
     return cuda_ok(cudaStreamSynchronize(stream_), error, "tiles sync");
   }
@@ -2037,7 +2099,8 @@ template <class R> class Batch final : public BatchBase {
     const uint64_t flux = mode_ == AMR_B200_LAUNCH_SPLIT ? 2 : 1;
     const uint64_t grad = model_ >= MODEL_LAMINAR && mode_ != AMR_B200_LAUNCH_TILED ? 3 : 0;
     const uint64_t per_trial = 3 * flux + grad + 1 + (any_srd() ? 3 : 0) + 1 + (any_srd_rate() ? 1 : 0);
-    return 1 + per_trial * trials;
+    const uint64_t lanes = mode_ == AMR_B200_LAUNCH_SPLIT ? (uint64_t)lanes_ : 1;
+    return lanes * (1 + per_trial * trials);
   }
 
   bool any_srd() const {
@@ -2079,8 +2142,22 @@ template <class R> class Batch final : public BatchBase {
       ok = ok && cuda_ok(EngineOps<R>::launch_phases(dev(), model_, flux_, any_srd(), trials, mode, block_, stream_), error,
                          "phase kernel launch");
     } else if (mode_ == AMR_B200_LAUNCH_SPLIT) {
-      ok = ok && cuda_ok(EngineOps<R>::launch_split(dev(), model_, flux_, any_srd(), trials, mode, stream_, sms_), error,
-                         "split kernel launch");
+      SplitLanes<R> lanes;
+      if (lanes_ == 2) {
+        lanes.n = 2;
+        for (int l = 0; l < 2; ++l) {
+          lanes.dev[l] = dev();
+          lanes.dev[l].live_end = lane_ranges_.p + 8 * l;
+          lanes.dev[l].live_begin = lane_ranges_.p + 8 * l + 4;
+          lanes.dev[l].case_lane = case_lane_.p;
+          lanes.dev[l].lane = l;
+        }
+        lanes.aux = aux_;
+        lanes.fork = fork_;
+        lanes.join = join_;
+      }
+      ok = ok && cuda_ok(EngineOps<R>::launch_split(dev(), model_, flux_, any_srd(), trials, mode, stream_, sms_, &lanes),
+                         error, "split kernel launch");
     } else if (mode_ == AMR_B200_LAUNCH_TILED) {
       ok = ok && cuda_ok(EngineOps<R>::launch_tiled(dev(), model_, flux_, any_srd(), trials, mode, stream_, sms_), error,
                          "tiled kernel launch");
@@ -2128,6 +2205,7 @@ template <class R> class Batch final : public BatchBase {
     graph_trials_ = trials;
     graph_srd_ = any_srd();
     graph_srd_rate_ = any_srd_rate();
+    graph_lanes_ = lanes_;
     graph_dirty_ = false;
     return true;
   }
@@ -2147,6 +2225,11 @@ template <class R> class Batch final : public BatchBase {
     if (ev1_) cudaEventDestroy(ev1_);
     ev0_ = ev1_ = nullptr;
     if (stream_) cudaStreamDestroy(stream_);
+    if (aux_) cudaStreamDestroy(aux_);
+    if (fork_) cudaEventDestroy(fork_);
+    if (join_) cudaEventDestroy(join_);
+    aux_ = nullptr;
+    fork_ = join_ = nullptr;
     stream_ = nullptr;
   }
 
@@ -2179,6 +2262,14 @@ template <class R> class Batch final : public BatchBase {
   long long hw_cells_ = 0, hw_faces_ = 0, hw_walls_ = 0;
   int h_live_end_[4] = {0, 0, 0, 0};
   bool graph_srd_ = false, graph_srd_rate_ = false;
+  // split mode in lanes (plan_lanes): count, wanted count, the count the graph was captured with
+  int lanes_ = 1, lanes_wanted_ = 2, graph_lanes_ = 1;
+  int h_lane_ranges_[16] = {};
+  std::vector<int> h_case_lane_;
+  cudaStream_t aux_ = nullptr;
+  cudaEvent_t fork_ = nullptr, join_ = nullptr;
+  DevBuf<int> lane_ranges_;  // per lane: ends of cells, faces, walls, block tiles; begins of cells, faces, walls
+  DevBuf<int> case_lane_;    // per case slot: its lane (-1 not live)
 
   DevBuf<int> live_end_;
   long long cap_faces_ = 0;

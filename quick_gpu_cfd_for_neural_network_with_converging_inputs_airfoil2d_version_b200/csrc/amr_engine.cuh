@@ -191,6 +191,12 @@ template <class R> struct Dev {
   int cap_faces, cap_walls;       // record capacities
   const int* live_end;            // the same on the device: cells, faces, walls (read by the
                                   // graph-replayed kernels, so a graph outlives case changes)
+  // Split mode in lanes: the split kernels of lane `lane` cover cells, faces and walls from
+  // live_begin[0..2] to live_end[0..2] (null live_begin: from 0), and its per-case kernels only
+  // the cases whose case_lane entry is `lane` (null case_lane: every case).
+  const int* live_begin;
+  const int* case_lane;
+  int lane;
   GridBarrier* bar;
   unsigned long long barrier_cycles;
 };
@@ -1471,6 +1477,7 @@ __global__ void __launch_bounds__(128) dt_cases_kernel(Dev<R> d) {
   chain_begin();
   const int cs = blockIdx.x * blockDim.x + threadIdx.x;
   if (cs >= d.n_cases) return;
+  if (d.case_lane && d.case_lane[cs] != d.lane) return;
   const CaseCtl& c = d.ctl[cs];
   if (!c.live || !c.active) return;
   double dt;
@@ -1496,10 +1503,12 @@ __global__ void __launch_bounds__(MAX_BLOCK) phase_srd_kernel(Dev<R> d, int stag
 }
 
 // Accept/reject the trial (unless begin_only) and begin the next one, one thread per case.
-static __global__ void phase_commit_kernel(CaseCtl* ctl, int n_cases, int begin_only) {
+static __global__ void phase_commit_kernel(CaseCtl* ctl, int n_cases, int begin_only, const int* case_lane,
+                                           int lane) {
   chain_begin();
   const int cs = blockIdx.x * blockDim.x + threadIdx.x;
   if (cs >= n_cases) return;
+  if (case_lane && case_lane[cs] != lane) return;
   CaseCtl& c = ctl[cs];
   if (!begin_only) case_commit(c);
   case_begin(c);
@@ -1646,8 +1655,8 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitStageOcc<R, STAGE>::cell) gr
   constexpr int stage = STAGE;
   chain_begin();
   const int rule = stage_rule(stage);
-  const int ncells = d.live_end[0];
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ncells; k += gridDim.x * blockDim.x) {
+  const int ncells = d.live_end[0], c0 = d.live_begin ? d.live_begin[0] : 0;
+  for (int k = c0 + blockIdx.x * blockDim.x + threadIdx.x; k < ncells; k += gridDim.x * blockDim.x) {
     const int cs = d.c_case[k];
     if (cs < 0) continue;
     const CaseCtl& c = d.ctl[cs];
@@ -1679,12 +1688,14 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitStageOcc<R, STAGE>::item) it
   chain_begin();
   const int rule = stage_rule(stage);
   const bool base = stage == STAGE_BASE || stage == STAGE_DIAG;  // spectral columns wanted
-  const int nf = d.live_end[1], total = nf + d.live_end[2];
+  // this lane's faces [f0, nf), then its walls [w0, nw) at item indices nf - f0 on
+  const int f0 = d.live_begin ? d.live_begin[1] : 0, w0 = d.live_begin ? d.live_begin[2] : 0;
+  const int nf = d.live_end[1] - f0, total = nf + d.live_end[2] - w0;
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
     bool bad = false;
     int cs;
     if (idx < nf) {
-      const int f = idx;
+      const int f = f0 + idx;
       cs = d.f_case[f];
       if (cs < 0) continue;
       const CaseCtl& c = d.ctl[cs];
@@ -1701,7 +1712,7 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitStageOcc<R, STAGE>::item) it
       }
       store_item<R, MODEL>(d.fval + RecFormat<R, MODEL>::stride * (long long)f, rec, base, false, d.fsa + f);
     } else {
-      const int w = idx - nf;
+      const int w = w0 + idx - nf;
       const int owner = d.w_owner[w];
       if (owner < 0) continue;
       cs = d.c_case[owner];
@@ -1741,11 +1752,11 @@ __global__ void __launch_bounds__(PHASE_BLOCK, SplitStageOcc<R, STAGE>::gather) 
   constexpr int stage = STAGE;
   chain_begin();
   const int rule = stage_rule(stage);
-  const int ncells = d.live_end[0];
+  const int ncells = d.live_end[0], c0 = d.live_begin ? d.live_begin[0] : 0;
   const bool base = stage == STAGE_BASE;
   const int lane = threadIdx.x & 31;
   // the loop bound is warp-uniform so the segmented shuffles below see full warps
-  for (int k0 = blockIdx.x * blockDim.x; k0 < ncells; k0 += gridDim.x * blockDim.x) {
+  for (int k0 = c0 + blockIdx.x * blockDim.x; k0 < ncells; k0 += gridDim.x * blockDim.x) {
     const int k = k0 + threadIdx.x;
     int cs = -1, a = 0, b = 0, nw = 0;
     if (k < ncells) {
@@ -1941,6 +1952,15 @@ __global__ void __launch_bounds__(BT_THREADS, TiledOcc<R>::blocks) tiled_stage_k
   }
 }
 
+// The split mode in two lanes: each lane's Dev (its ranges and case filter), and the auxiliary
+// stream and fork/join events that run the second lane's chain beside the first's.
+template <class R> struct SplitLanes {
+  int n = 1;
+  Dev<R> dev[2];
+  cudaStream_t aux = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+
 // Host-visible launch helpers (defined in amr_engine_f64.cu / amr_engine_f32.cu).
 template <class R> struct EngineOps {
   static cudaError_t launch(const Dev<R>& d, int model, int flux, bool srd, int trials, int mode, int grid, int block,
@@ -1949,8 +1969,10 @@ template <class R> struct EngineOps {
   static cudaError_t launch_phases(const Dev<R>& d, int model, int flux, bool srd, int trials, int mode, int block,
                                    cudaStream_t stream);
   // The same with the split kernels (gradients per cell, fluxes per face record, gather per cell).
+  // With two lanes, their trials run as two independent chains (lanes->dev[0] on stream, dev[1]
+  // on lanes->aux), so that one lane's kernels fill the tails of the other's.
   static cudaError_t launch_split(const Dev<R>& d, int model, int flux, bool srd, int trials, int mode,
-                                  cudaStream_t stream, int sms);
+                                  cudaStream_t stream, int sms, const SplitLanes<R>* lanes = nullptr);
   // The same with one shared-memory tiled kernel per stage.
   static cudaError_t launch_tiled(const Dev<R>& d, int model, int flux, bool srd, int trials, int mode,
                                   cudaStream_t stream, int sms);

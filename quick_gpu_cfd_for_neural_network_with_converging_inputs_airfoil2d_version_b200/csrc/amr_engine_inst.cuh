@@ -68,7 +68,7 @@ static cudaError_t launch_phases_t(const Dev<R>& d, bool srd, int trials, int mo
     phase_pair(std::integral_constant<int, STAGE_DIAG>{});
     return cudaGetLastError();
   }
-  chain(phase_commit_kernel, dim3(cblocks), dim3(128), 0, st, d.ctl, cases, 1);
+  chain(phase_commit_kernel, dim3(cblocks), dim3(128), 0, st, d.ctl, cases, 1, (const int*)nullptr, 0);
   for (int t = 0; t < trials; ++t) {
     phase_pair(std::integral_constant<int, STAGE_BASE>{});
     if (srd && MODEL >= MODEL_LAMINAR && d.any_srd_rate) chain(srd_rate_kernel<R, MODEL>, dim3(cases), dim3(MAX_BLOCK), 0, st, d, -1);
@@ -81,7 +81,7 @@ static cudaError_t launch_phases_t(const Dev<R>& d, bool srd, int trials, int mo
         phase_pair(std::integral_constant<int, STAGE_2>{});
     }
     if (srd) chain(phase_srd_kernel<R, MODEL>, dim3(cases), dim3(block), 0, st, d, 3);
-    chain(phase_commit_kernel, dim3(cblocks), dim3(128), 0, st, d.ctl, cases, 0);
+    chain(phase_commit_kernel, dim3(cblocks), dim3(128), 0, st, d.ctl, cases, 0, (const int*)nullptr, 0);
   }
   return cudaGetLastError();
 }
@@ -102,7 +102,8 @@ cudaError_t EngineOps<R>::launch_phases(const Dev<R>& d, int model, int flux, bo
 // Grids are fixed by the arena's capacity (grid-stride loops over the live ranges, which the
 // kernels read from the device), so a captured graph stays valid when cases come and go.
 template <class R, int MODEL, int FLUX>
-static cudaError_t launch_split_t(const Dev<R>& d, bool srd, int trials, int mode, cudaStream_t st, int sms) {
+static cudaError_t launch_split_t(const Dev<R>& d, bool srd, int trials, int mode, cudaStream_t st, int sms,
+                                  const SplitLanes<R>* lanes) {
   const int B = PHASE_BLOCK;
   const long long ncap = d.ncap, icap = (long long)d.cap_faces + d.cap_walls;
   // grids of one wave of co-resident blocks at each kernel's register budget
@@ -115,64 +116,78 @@ static cudaError_t launch_split_t(const Dev<R>& d, bool srd, int trials, int mod
   // U1 where they read it and one thread per case makes the update's control decisions.
   // (Euler reads U1 in the face kernel; SRD changes U1 between the update and stage 1.)
   const bool fused = MODEL >= MODEL_LAMINAR && !srd;
-  const Dev<R>& dd = d;
-  auto stage_kernels = [&](auto stage_tag) {
-    constexpr int S = decltype(stage_tag)::value;
-    using O = SplitStageOcc<R, S>;
-    if constexpr (S == STAGE_1) {
-      if (fused) {
-        chain(grad_cells_kernel<R, MODEL, S, true>, dim3(cells_grid(O::cell)), dim3(B), 0, st, dd);
-        chain(item_kernel<R, MODEL, FLUX, S>, dim3(items_grid(O::item)), dim3(B), 0, st, dd);
-        chain(gather_kernel<R, MODEL, S, true>, dim3(cells_grid(O::gather)), dim3(B), 0, st, dd);
-        return;
+  // one lane's kernels on stream s
+  const auto run = [&](const Dev<R>& dd, cudaStream_t s) {
+    auto stage_kernels = [&](auto stage_tag) {
+      constexpr int S = decltype(stage_tag)::value;
+      using O = SplitStageOcc<R, S>;
+      if constexpr (S == STAGE_1) {
+        if (fused) {
+          chain(grad_cells_kernel<R, MODEL, S, true>, dim3(cells_grid(O::cell)), dim3(B), 0, s, dd);
+          chain(item_kernel<R, MODEL, FLUX, S>, dim3(items_grid(O::item)), dim3(B), 0, s, dd);
+          chain(gather_kernel<R, MODEL, S, true>, dim3(cells_grid(O::gather)), dim3(B), 0, s, dd);
+          return;
+        }
       }
+      if (MODEL >= MODEL_LAMINAR)
+        chain(grad_cells_kernel<R, MODEL, S>, dim3(cells_grid(O::cell)), dim3(B), 0, s, dd);
+      chain(item_kernel<R, MODEL, FLUX, S>, dim3(items_grid(O::item)), dim3(B), 0, s, dd);
+      chain(gather_kernel<R, MODEL, S>, dim3(cells_grid(O::gather)), dim3(B), 0, s, dd);
+    };
+    auto stage_seq = [&](int stage) {
+      switch (stage) {
+        case STAGE_BASE: stage_kernels(std::integral_constant<int, STAGE_BASE>{}); break;
+        case STAGE_1: stage_kernels(std::integral_constant<int, STAGE_1>{}); break;
+        case STAGE_2: stage_kernels(std::integral_constant<int, STAGE_2>{}); break;
+        default: stage_kernels(std::integral_constant<int, STAGE_DIAG>{}); break;
+      }
+    };
+    if (mode == MODE_RESIDUAL) {
+      stage_seq(STAGE_DIAG);
+      return;
     }
-    if (MODEL >= MODEL_LAMINAR)
-      chain(grad_cells_kernel<R, MODEL, S>, dim3(cells_grid(O::cell)), dim3(B), 0, st, dd);
-    chain(item_kernel<R, MODEL, FLUX, S>, dim3(items_grid(O::item)), dim3(B), 0, st, dd);
-    chain(gather_kernel<R, MODEL, S>, dim3(cells_grid(O::gather)), dim3(B), 0, st, dd);
+    chain(phase_commit_kernel, dim3(kblocks), dim3(128), 0, s, dd.ctl, cases, 1, dd.case_lane, dd.lane);
+    for (int t = 0; t < trials; ++t) {
+      stage_seq(STAGE_BASE);
+      if (srd && MODEL >= MODEL_LAMINAR && dd.any_srd_rate)
+        chain(srd_rate_kernel<R, MODEL>, dim3(cases), dim3(MAX_BLOCK), 0, s, dd, -1);
+      if (fused)
+        chain(dt_cases_kernel<R>, dim3(kblocks), dim3(128), 0, s, dd);
+      else
+        chain(phase_first_cells_kernel<R, MODEL>, dim3(fblocks), dim3(256), 0, s, dd);
+      for (int stage = 1; stage <= 2; ++stage) {
+        if (srd) chain(phase_srd_kernel<R, MODEL>, dim3(cases), dim3(MAX_BLOCK), 0, s, dd, stage);
+        stage_seq(stage);
+      }
+      if (srd) chain(phase_srd_kernel<R, MODEL>, dim3(cases), dim3(MAX_BLOCK), 0, s, dd, 3);
+      chain(phase_commit_kernel, dim3(kblocks), dim3(128), 0, s, dd.ctl, cases, 0, dd.case_lane, dd.lane);
+    }
   };
-  auto stage_seq = [&](int stage) {
-    switch (stage) {
-      case STAGE_BASE: stage_kernels(std::integral_constant<int, STAGE_BASE>{}); break;
-      case STAGE_1: stage_kernels(std::integral_constant<int, STAGE_1>{}); break;
-      case STAGE_2: stage_kernels(std::integral_constant<int, STAGE_2>{}); break;
-      default: stage_kernels(std::integral_constant<int, STAGE_DIAG>{}); break;
-    }
-  };
-  if (mode == MODE_RESIDUAL) {
-    stage_seq(STAGE_DIAG);
-    return cudaGetLastError();
-  }
-  chain(phase_commit_kernel, dim3(kblocks), dim3(128), 0, st, d.ctl, cases, 1);
-  for (int t = 0; t < trials; ++t) {
-    stage_seq(STAGE_BASE);
-    if (srd && MODEL >= MODEL_LAMINAR && d.any_srd_rate) chain(srd_rate_kernel<R, MODEL>, dim3(cases), dim3(MAX_BLOCK), 0, st, d, -1);
-    if (fused)
-      chain(dt_cases_kernel<R>, dim3(kblocks), dim3(128), 0, st, d);
-    else
-      chain(phase_first_cells_kernel<R, MODEL>, dim3(fblocks), dim3(256), 0, st, d);
-    for (int stage = 1; stage <= 2; ++stage) {
-      if (srd) chain(phase_srd_kernel<R, MODEL>, dim3(cases), dim3(MAX_BLOCK), 0, st, d, stage);
-      stage_seq(stage);
-    }
-    if (srd) chain(phase_srd_kernel<R, MODEL>, dim3(cases), dim3(MAX_BLOCK), 0, st, d, 3);
-    chain(phase_commit_kernel, dim3(kblocks), dim3(128), 0, st, d.ctl, cases, 0);
+  if (mode == MODE_TRIALS && lanes && lanes->n == 2) {
+    // the second lane's chain forks off the launch stream and joins it at the end
+    cudaEventRecord(lanes->fork, st);
+    cudaStreamWaitEvent(lanes->aux, lanes->fork, 0);
+    run(lanes->dev[0], st);
+    run(lanes->dev[1], lanes->aux);
+    cudaEventRecord(lanes->join, lanes->aux);
+    cudaStreamWaitEvent(st, lanes->join, 0);
+  } else {
+    run(d, st);
   }
   return cudaGetLastError();
 }
 
 template <class R>
 cudaError_t EngineOps<R>::launch_split(const Dev<R>& d, int model, int flux, bool srd, int trials, int mode,
-                                       cudaStream_t stream, int sms) {
+                                       cudaStream_t stream, int sms, const SplitLanes<R>* lanes) {
   if (model == MODEL_EULER)
-    return flux == FLUX_HLLC ? launch_split_t<R, MODEL_EULER, FLUX_HLLC>(d, srd, trials, mode, stream, sms)
-                             : launch_split_t<R, MODEL_EULER, FLUX_AUSM>(d, srd, trials, mode, stream, sms);
+    return flux == FLUX_HLLC ? launch_split_t<R, MODEL_EULER, FLUX_HLLC>(d, srd, trials, mode, stream, sms, lanes)
+                             : launch_split_t<R, MODEL_EULER, FLUX_AUSM>(d, srd, trials, mode, stream, sms, lanes);
   if (model == MODEL_LAMINAR)
-    return flux == FLUX_HLLC ? launch_split_t<R, MODEL_LAMINAR, FLUX_HLLC>(d, srd, trials, mode, stream, sms)
-                             : launch_split_t<R, MODEL_LAMINAR, FLUX_AUSM>(d, srd, trials, mode, stream, sms);
-  return flux == FLUX_HLLC ? launch_split_t<R, MODEL_SA, FLUX_HLLC>(d, srd, trials, mode, stream, sms)
-                           : launch_split_t<R, MODEL_SA, FLUX_AUSM>(d, srd, trials, mode, stream, sms);
+    return flux == FLUX_HLLC ? launch_split_t<R, MODEL_LAMINAR, FLUX_HLLC>(d, srd, trials, mode, stream, sms, lanes)
+                             : launch_split_t<R, MODEL_LAMINAR, FLUX_AUSM>(d, srd, trials, mode, stream, sms, lanes);
+  return flux == FLUX_HLLC ? launch_split_t<R, MODEL_SA, FLUX_HLLC>(d, srd, trials, mode, stream, sms, lanes)
+                           : launch_split_t<R, MODEL_SA, FLUX_AUSM>(d, srd, trials, mode, stream, sms, lanes);
 }
 
 template <class R, int MODEL, int FLUX>
@@ -186,7 +201,7 @@ static cudaError_t launch_tiled_t(const Dev<R>& d, bool srd, int trials, int mod
     chain(tiled_stage_kernel<R, MODEL, FLUX>, dim3(grid), dim3(BT_THREADS), sm, st, d, STAGE_DIAG);
     return cudaGetLastError();
   }
-  chain(phase_commit_kernel, dim3(kblocks), dim3(128), 0, st, d.ctl, cases, 1);
+  chain(phase_commit_kernel, dim3(kblocks), dim3(128), 0, st, d.ctl, cases, 1, (const int*)nullptr, 0);
   for (int t = 0; t < trials; ++t) {
     chain(tiled_stage_kernel<R, MODEL, FLUX>, dim3(grid), dim3(BT_THREADS), sm, st, d, STAGE_BASE);
     if (srd && MODEL >= MODEL_LAMINAR && d.any_srd_rate) chain(srd_rate_kernel<R, MODEL>, dim3(cases), dim3(MAX_BLOCK), 0, st, d, -1);
@@ -196,7 +211,7 @@ static cudaError_t launch_tiled_t(const Dev<R>& d, bool srd, int trials, int mod
       chain(tiled_stage_kernel<R, MODEL, FLUX>, dim3(grid), dim3(BT_THREADS), sm, st, d, stage);
     }
     if (srd) chain(phase_srd_kernel<R, MODEL>, dim3(cases), dim3(MAX_BLOCK), 0, st, d, 3);
-    chain(phase_commit_kernel, dim3(kblocks), dim3(128), 0, st, d.ctl, cases, 0);
+    chain(phase_commit_kernel, dim3(kblocks), dim3(128), 0, st, d.ctl, cases, 0, (const int*)nullptr, 0);
   }
   return cudaGetLastError();
 }

@@ -82,6 +82,7 @@ class BatchBase {
   virtual int autotune(int trials, std::string* error) = 0;
   virtual void set_event_timing(bool on) = 0;
   virtual void set_graph(bool on) = 0;
+  virtual void set_lanes(int lanes) = 0;
   virtual std::string launch_config() const = 0;
 };
 
