@@ -492,10 +492,11 @@ int amr_batch_set_target(amr_batch* batch, int32_t slot, double target, int64_t 
 int amr_batch_residual(amr_batch* batch, int32_t slot, double* r, uint64_t count, char* error, uint64_t error_size);
 /* Replays advances from CUDA graphs (on, the default) or launches their kernels directly. */
 int amr_batch_set_graph(amr_batch* batch, int32_t on);
-/* Split launch mode, viscous models without SRD: the live cases run as `lanes` (1 or 2) independent
- * chains of kernels on two streams, each over about half the cells, so that one chain's kernels
- * fill the tails of the other's.  Two lanes need every case of the first half to lie below every
- * case of the second in the arena (as after admissions in one order); otherwise one lane runs. */
+/* Split launch mode, viscous models without SRD: the live cases run as `lanes` (1..4, default 3)
+ * independent chains of kernels, each on its own stream over about an equal share of the cells, so
+ * that one chain's kernels fill the tails of the others'.  Lanes need every case of one lane to lie
+ * below every case of the next in the arena (as after admissions in one order); otherwise one lane
+ * runs.  Returns 1 for a count outside 1..4. */
 int amr_batch_set_lanes(amr_batch* batch, int32_t lanes);
 /* The launch configuration chosen (mode, block, grid, graph or direct, lanes) as text. */
 int amr_batch_launch_config(const amr_batch* batch, char* out, uint64_t size);

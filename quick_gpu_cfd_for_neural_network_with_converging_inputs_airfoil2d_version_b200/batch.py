@@ -201,10 +201,10 @@ class Batch:
         lib().amr_batch_set_graph(self._h, int(bool(on)))
 
     def set_lanes(self, lanes):
-        """Split mode, viscous models without SRD: run the live cases as `lanes` (1 or 2) chains of
+        """Split mode, viscous models without SRD: run the live cases as `lanes` (1..4) chains of
         kernels in flight together (amr_batch_set_lanes)."""
         if lib().amr_batch_set_lanes(self._h, int(lanes)):
-            raise BatchError('lanes must be 1 or 2')
+            raise BatchError('lanes must be 1..4')
 
     def launch_config(self):
         b = errbuf(128)

@@ -361,7 +361,7 @@ template <class R> class Batch final : public BatchBase {
   bool alloc_tables(const amr_batch_config_t& c, std::string* error) {
     uint64_t* A = &stats_.allocated_bytes;
     const long long nc = cap_cells_;
-    bool ok = lane_ranges_.alloc(16, A, error, "lanes") && case_lane_.alloc(c.max_cases, A, error, "lanes") &&
+    bool ok = lane_ranges_.alloc(8 * MAX_LANES, A, error, "lanes") && case_lane_.alloc(c.max_cases, A, error, "lanes") &&
               ctl_.alloc(c.max_cases, A, error, "ctl") && cfg_.alloc(c.max_cases, A, error, "cfg") &&
               tiles_.alloc(cap_tiles_, A, error, "tiles") && bar_.alloc(1, A, error, "barrier") &&
               c_case_.alloc(nc, A, error, "cells") && c_vol_.alloc(nc, A, error, "cells") &&
@@ -485,11 +485,12 @@ template <class R> class Batch final : public BatchBase {
     stagers_.clear();
     stagers_.emplace_back(new Stager());
     if (!cuda_ok(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), error, "stream")) return false;
-    // the split mode's second lane: its stream and the events that fork it off and join it
-    if (!cuda_ok(cudaStreamCreateWithFlags(&aux_, cudaStreamNonBlocking), error, "stream") ||
-        !cuda_ok(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), error, "event") ||
-        !cuda_ok(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), error, "event"))
-      return false;
+    // the split mode's other lanes: their streams and the events that fork them off and join them
+    if (!cuda_ok(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), error, "event")) return false;
+    for (int l = 0; l < MAX_LANES - 1; ++l)
+      if (!cuda_ok(cudaStreamCreateWithFlags(&aux_[l], cudaStreamNonBlocking), error, "stream") ||
+          !cuda_ok(cudaEventCreateWithFlags(&join_[l], cudaEventDisableTiming), error, "event"))
+        return false;
     if (!cuda_ok(cudaEventCreate(&ev0_), error, "event") || !cuda_ok(cudaEventCreate(&ev1_), error, "event")) return false;
     // every table in one slab: a planning pass sizes them, one allocation, a carving pass
     Slab slab;
@@ -1548,9 +1549,11 @@ template <class R> class Batch final : public BatchBase {
     graph_dirty_ = true;
   }
 
-  void set_lanes(int lanes) override {
+  int set_lanes(int lanes) override {
+    if (lanes < 1 || lanes > MAX_LANES) return 1;
     lanes_wanted_ = lanes;
     tiles_dirty_ = true;  // the next advance plans the lanes again
+    return 0;
   }
 
   std::string launch_config() const override {
@@ -1907,52 +1910,79 @@ template <class R> class Batch final : public BatchBase {
     m.cur = c.cur;
   }
 
-  // Split mode, viscous models without SRD: the live cases in two lanes of about equal cells, each
-  // advanced by its own chain of kernels (so that one lane's kernels fill the tails of the
-  // other's).  A lane must own whole ranges: every first-lane case's cells, faces and walls lie
-  // below every second-lane case's, as they do after admissions in one order; otherwise (or with
-  // fewer than two cases) one lane.
+  // Split mode, viscous models without SRD: the live cases in up to lanes_wanted_ lanes of about
+  // equal cells, each advanced by its own chain of kernels (so that one lane's kernels fill the
+  // tails of the others').  A lane must own whole ranges: every case of a lane has its cells, faces
+  // and walls below every case of the next lane, as after admissions in one order; otherwise (or
+  // with fewer than two cases) one lane.
   bool plan_lanes(std::string* error) {
     lanes_ = 1;
     if (lanes_wanted_ < 2 || mode_ != AMR_B200_LAUNCH_SPLIT || model_ < MODEL_LAMINAR || any_srd()) return true;
     std::vector<int> live;
     for (int i = 0; i < config_.max_cases; ++i)
       if (cases_[i].live) live.push_back(i);
-    if (live.size() < 2) return true;
+    const int want = std::min<int>(lanes_wanted_, (int)live.size());
+    if (want < 2) return true;
     std::sort(live.begin(), live.end(), [&](int a, int b) { return cases_[a].cells.b < cases_[b].cells.b; });
-    long long total = 0, acc = 0;
-    for (int i : live) total += cases_[i].cells.n;
-    size_t cut = 1;
-    for (size_t q = 0; q + 1 < live.size(); ++q) {
-      acc += cases_[live[q]].cells.n;
-      cut = q + 1;
-      if (2 * acc >= total) break;
+    // cut[l]: the first case of lane l, where the cells before it first reach l / want of the
+    // total, with at least one case in every lane
+    const size_t m = live.size();
+    std::vector<long long> before(m + 1, 0);
+    for (size_t q = 0; q < m; ++q) before[q + 1] = before[q] + cases_[live[q]].cells.n;
+    std::vector<size_t> cut(want + 1, 0);
+    cut[want] = m;
+    for (int l = 1; l < want; ++l) {
+      size_t q = cut[l - 1] + 1;
+      const size_t last = m - (size_t)(want - l);
+      while (q < last && before[q] * want < (long long)l * before[m]) ++q;
+      cut[l] = q;
     }
-    // lane 0: [0, begin of lane 1) in every table; lane 1: from there to the live ends
-    long long end0[3] = {0, 0, 0}, begin1[3] = {hw_cells_, hw_faces_, hw_walls_};
+    std::vector<int> lane_of(m, 0);
+    for (int l = 0; l < want; ++l)
+      for (size_t q = cut[l]; q < cut[l + 1]; ++q) lane_of[q] = l;
+    // per lane and table (cells, faces, walls): the lowest begin and the highest end of its ranges
+    const long long hw[3] = {hw_cells_, hw_faces_, hw_walls_};
+    long long lo[MAX_LANES][3], hi[MAX_LANES][3];
+    for (int l = 0; l < want; ++l)
+      for (int t = 0; t < 3; ++t) {
+        lo[l][t] = hw[t];
+        hi[l][t] = 0;
+      }
     for (size_t q = 0; q < live.size(); ++q) {
       const HostCase<R>& hc = cases_[live[q]];
       const Range r[3] = {hc.cells, hc.faces, hc.walls};
-      for (int t = 0; t < 3; ++t) {
-        if (r[t].n == 0) continue;
-        if (q < cut) end0[t] = std::max(end0[t], r[t].b + r[t].n);
-        else begin1[t] = std::min(begin1[t], r[t].b);
-      }
+      for (int t = 0; t < 3; ++t)
+        if (r[t].n) {
+          lo[lane_of[q]][t] = std::min(lo[lane_of[q]][t], r[t].b);
+          hi[lane_of[q]][t] = std::max(hi[lane_of[q]][t], r[t].b + r[t].n);
+        }
     }
-    for (int t = 0; t < 3; ++t)
-      if (end0[t] > begin1[t]) return true;  // interleaved ranges: one lane
-    const int h[16] = {(int)begin1[0], (int)begin1[1], (int)begin1[2], h_live_end_[3], 0, 0, 0, 0,
-                       (int)hw_cells_, (int)hw_faces_, (int)hw_walls_, h_live_end_[3],
-                       (int)begin1[0], (int)begin1[1], (int)begin1[2], 0};
-    std::copy(h, h + 16, h_lane_ranges_);
+    // lane boundaries from the top: lane l covers [bound[l], bound[l + 1])
+    long long bound[MAX_LANES + 1][3];
+    for (int t = 0; t < 3; ++t) {
+      bound[want][t] = hw[t];
+      for (int l = want - 1; l >= 1; --l) bound[l][t] = std::min(bound[l + 1][t], lo[l][t]);
+      bound[0][t] = 0;
+      for (int l = 0; l < want; ++l)
+        if (hi[l][t] > bound[l + 1][t]) return true;  // interleaved ranges: one lane
+    }
+    for (int l = 0; l < want; ++l) {
+      int* h = h_lane_ranges_ + 8 * l;
+      for (int t = 0; t < 3; ++t) {
+        h[t] = (int)bound[l + 1][t];
+        h[4 + t] = (int)bound[l][t];
+      }
+      h[3] = h_live_end_[3];
+      h[7] = 0;
+    }
     h_case_lane_.assign(config_.max_cases, -1);
-    for (size_t q = 0; q < live.size(); ++q) h_case_lane_[live[q]] = q < cut ? 0 : 1;
-    if (!cuda_ok(cudaMemcpyAsync(lane_ranges_.p, h_lane_ranges_, sizeof(h_lane_ranges_), cudaMemcpyHostToDevice, stream_),
+    for (size_t q = 0; q < live.size(); ++q) h_case_lane_[live[q]] = lane_of[q];
+    if (!cuda_ok(cudaMemcpyAsync(lane_ranges_.p, h_lane_ranges_, sizeof(int) * 8 * want, cudaMemcpyHostToDevice, stream_),
                  error, "lanes") ||
         !cuda_ok(cudaMemcpyAsync(case_lane_.p, h_case_lane_.data(), sizeof(int) * h_case_lane_.size(),
                                  cudaMemcpyHostToDevice, stream_), error, "lanes"))
       return false;
-    lanes_ = 2;
+    lanes_ = want;
     return true;
   }
 
@@ -2143,18 +2173,20 @@ template <class R> class Batch final : public BatchBase {
                          "phase kernel launch");
     } else if (mode_ == AMR_B200_LAUNCH_SPLIT) {
       SplitLanes<R> lanes;
-      if (lanes_ == 2) {
-        lanes.n = 2;
-        for (int l = 0; l < 2; ++l) {
+      if (lanes_ >= 2) {
+        lanes.n = lanes_;
+        for (int l = 0; l < lanes_; ++l) {
           lanes.dev[l] = dev();
           lanes.dev[l].live_end = lane_ranges_.p + 8 * l;
           lanes.dev[l].live_begin = lane_ranges_.p + 8 * l + 4;
           lanes.dev[l].case_lane = case_lane_.p;
           lanes.dev[l].lane = l;
         }
-        lanes.aux = aux_;
+        for (int l = 0; l < MAX_LANES - 1; ++l) {
+          lanes.aux[l] = aux_[l];
+          lanes.join[l] = join_[l];
+        }
         lanes.fork = fork_;
-        lanes.join = join_;
       }
       ok = ok && cuda_ok(EngineOps<R>::launch_split(dev(), model_, flux_, any_srd(), trials, mode, stream_, sms_, &lanes),
                          error, "split kernel launch");
@@ -2225,11 +2257,14 @@ template <class R> class Batch final : public BatchBase {
     if (ev1_) cudaEventDestroy(ev1_);
     ev0_ = ev1_ = nullptr;
     if (stream_) cudaStreamDestroy(stream_);
-    if (aux_) cudaStreamDestroy(aux_);
+    for (int l = 0; l < MAX_LANES - 1; ++l) {
+      if (aux_[l]) cudaStreamDestroy(aux_[l]);
+      if (join_[l]) cudaEventDestroy(join_[l]);
+      aux_[l] = nullptr;
+      join_[l] = nullptr;
+    }
     if (fork_) cudaEventDestroy(fork_);
-    if (join_) cudaEventDestroy(join_);
-    aux_ = nullptr;
-    fork_ = join_ = nullptr;
+    fork_ = nullptr;
     stream_ = nullptr;
   }
 
@@ -2263,11 +2298,12 @@ template <class R> class Batch final : public BatchBase {
   int h_live_end_[4] = {0, 0, 0, 0};
   bool graph_srd_ = false, graph_srd_rate_ = false;
   // split mode in lanes (plan_lanes): count, wanted count, the count the graph was captured with
-  int lanes_ = 1, lanes_wanted_ = 2, graph_lanes_ = 1;
-  int h_lane_ranges_[16] = {};
+  // (three lanes measured fastest on 256 cases: 0.72-0.73 ms/step, two 0.75, four 0.73-0.74, one 0.78)
+  int lanes_ = 1, lanes_wanted_ = 3, graph_lanes_ = 1;
+  int h_lane_ranges_[8 * MAX_LANES] = {};
   std::vector<int> h_case_lane_;
-  cudaStream_t aux_ = nullptr;
-  cudaEvent_t fork_ = nullptr, join_ = nullptr;
+  cudaStream_t aux_[MAX_LANES - 1] = {};
+  cudaEvent_t fork_ = nullptr, join_[MAX_LANES - 1] = {};
   DevBuf<int> lane_ranges_;  // per lane: ends of cells, faces, walls, block tiles; begins of cells, faces, walls
   DevBuf<int> case_lane_;    // per case slot: its lane (-1 not live)
 

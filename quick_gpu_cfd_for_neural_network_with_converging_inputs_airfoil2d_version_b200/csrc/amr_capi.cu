@@ -636,9 +636,8 @@ int amr_batch_set_graph(amr_batch* b, int32_t on) {
 }
 
 int amr_batch_set_lanes(amr_batch* b, int32_t lanes) {
-  if (!b || lanes < 1 || lanes > 2) return 1;
-  b->batch->set_lanes(lanes);
-  return 0;
+  if (!b) return 1;
+  return b->batch->set_lanes(lanes);
 }
 
 int amr_batch_set_target(amr_batch* b, int32_t slot, double target, int64_t maxsteps, char* error, uint64_t error_size) {

@@ -1952,13 +1952,15 @@ __global__ void __launch_bounds__(BT_THREADS, TiledOcc<R>::blocks) tiled_stage_k
   }
 }
 
-// The split mode in two lanes: each lane's Dev (its ranges and case filter), and the auxiliary
-// stream and fork/join events that run the second lane's chain beside the first's.
+// The split mode in lanes: each lane's Dev (its ranges and case filter), and the auxiliary
+// streams and fork/join events that run lanes 1.. beside lane 0.
+constexpr int MAX_LANES = 4;
 template <class R> struct SplitLanes {
   int n = 1;
-  Dev<R> dev[2];
-  cudaStream_t aux = nullptr;
-  cudaEvent_t fork = nullptr, join = nullptr;
+  Dev<R> dev[MAX_LANES];
+  cudaStream_t aux[MAX_LANES - 1] = {};
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t join[MAX_LANES - 1] = {};
 };
 
 // Host-visible launch helpers (defined in amr_engine_f64.cu / amr_engine_f32.cu).
@@ -1969,8 +1971,8 @@ template <class R> struct EngineOps {
   static cudaError_t launch_phases(const Dev<R>& d, int model, int flux, bool srd, int trials, int mode, int block,
                                    cudaStream_t stream);
   // The same with the split kernels (gradients per cell, fluxes per face record, gather per cell).
-  // With two lanes, their trials run as two independent chains (lanes->dev[0] on stream, dev[1]
-  // on lanes->aux), so that one lane's kernels fill the tails of the other's.
+  // With lanes, their trials run as independent chains (lanes->dev[0] on stream, dev[i] on
+  // lanes->aux[i - 1]), so that one lane's kernels fill the tails of the others'.
   static cudaError_t launch_split(const Dev<R>& d, int model, int flux, bool srd, int trials, int mode,
                                   cudaStream_t stream, int sms, const SplitLanes<R>* lanes = nullptr);
   // The same with one shared-memory tiled kernel per stage.

@@ -163,14 +163,16 @@ static cudaError_t launch_split_t(const Dev<R>& d, bool srd, int trials, int mod
       chain(phase_commit_kernel, dim3(kblocks), dim3(128), 0, s, dd.ctl, cases, 0, dd.case_lane, dd.lane);
     }
   };
-  if (mode == MODE_TRIALS && lanes && lanes->n == 2) {
-    // the second lane's chain forks off the launch stream and joins it at the end
+  if (mode == MODE_TRIALS && lanes && lanes->n >= 2) {
+    // the other lanes' chains fork off the launch stream and join it at the end
     cudaEventRecord(lanes->fork, st);
-    cudaStreamWaitEvent(lanes->aux, lanes->fork, 0);
+    for (int l = 1; l < lanes->n; ++l) cudaStreamWaitEvent(lanes->aux[l - 1], lanes->fork, 0);
     run(lanes->dev[0], st);
-    run(lanes->dev[1], lanes->aux);
-    cudaEventRecord(lanes->join, lanes->aux);
-    cudaStreamWaitEvent(st, lanes->join, 0);
+    for (int l = 1; l < lanes->n; ++l) run(lanes->dev[l], lanes->aux[l - 1]);
+    for (int l = 1; l < lanes->n; ++l) {
+      cudaEventRecord(lanes->join[l - 1], lanes->aux[l - 1]);
+      cudaStreamWaitEvent(st, lanes->join[l - 1], 0);
+    }
   } else {
     run(d, st);
   }

@@ -82,7 +82,7 @@ class BatchBase {
   virtual int autotune(int trials, std::string* error) = 0;
   virtual void set_event_timing(bool on) = 0;
   virtual void set_graph(bool on) = 0;
-  virtual void set_lanes(int lanes) = 0;
+  virtual int set_lanes(int lanes) = 0;  // 1 if lanes is not 1..4
   virtual std::string launch_config() const = 0;
 };
 

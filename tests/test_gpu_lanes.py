@@ -1,6 +1,7 @@
-"""GPU tests of the split mode in two lanes (amr_batch_set_lanes): the live cases run as two
-independent chains of kernels on two streams.  Every case must end bit for bit where it ends in one
-lane, in FP32 and FP64, also after a release and a new admission have reordered the arena ranges."""
+"""GPU tests of the split mode in lanes (amr_batch_set_lanes): the live cases run as independent
+chains of kernels, one stream each.  Every case must end bit for bit where it ends in one lane, in
+FP32 and FP64, with two and four lanes, also after a release and a new admission have reordered the
+arena ranges."""
 import numpy as np
 import pytest
 
@@ -30,18 +31,18 @@ def run(items, precision, lanes, churn=False):
         b.destroy()
 
 
-@pytest.mark.parametrize('precision', [32, 64])
-def test_two_lanes_equal_one(precision):
+@pytest.mark.parametrize('precision,lanes', [(32, 2), (64, 2), (32, 4)])
+def test_lanes_equal_one(precision, lanes):
     items = items_of(sa_mix() * 2, 48)  # six cases
     one, steps1, cfg1 = run(items, precision, 1)
-    two, steps2, cfg2 = run(items, precision, 2)
-    assert 'lanes' not in cfg1 and 'lanes=2' in cfg2, (cfg1, cfg2)
+    two, steps2, cfg2 = run(items, precision, lanes)
+    assert 'lanes' not in cfg1 and f'lanes={lanes}' in cfg2, (cfg1, cfg2)
     assert steps1 == steps2
     for a, b in zip(one, two):
         assert np.array_equal(a, b)
 
 
-def test_two_lanes_after_release_and_readmission():
+def test_lanes_after_release_and_readmission():
     items = items_of(sa_mix() * 2, 60)
     one, steps1, _ = run(items, 32, 1, churn=True)
     two, steps2, _ = run(items, 32, 2, churn=True)
