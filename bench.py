@@ -57,7 +57,7 @@ SOLVE_STEPS = 5000  # steps per solve of the batched workload
 # It comes from that separate capture, not from the timed run.
 SPLIT_256_TRAFFIC_PER_STEP = 2.412e9
 TRAFFIC_SOURCE = ('separate ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, cold cache) of the nine '
-                  'split-kernel launches of one trial of `bench.py --profile split --cases 64`, scaled by cells to '
+                  'split-kernel launches of one trial of `bench.py --profile split --cases 64 --lanes 1`, scaled by cells to '
                   'the 256-case workload')
 
 
@@ -219,9 +219,15 @@ def parse_launch(cfg):
     return block, grid, mode
 
 
+LANES = 0  # --lanes: split-mode lanes of the batched and profile legs (0: the engine's default)
+
+
 def new_batch(case_list, precision, device=0, block=0, grid=0, mode=0):
     kw = workloads.batch_kwargs(case_list)
-    return Batch(precision=precision, device=device, block_threads=block, grid_blocks=grid, launch_mode=mode, **kw)
+    b = Batch(precision=precision, device=device, block_threads=block, grid_blocks=grid, launch_mode=mode, **kw)
+    if LANES:
+        b.set_lanes(LANES)
+    return b
 
 
 def admit_all(b, case_list, steps_cap=10 ** 9):
@@ -760,6 +766,8 @@ def main():
     ap.add_argument('--no-solve', action='store_true', help='skip the measured full-solve leg')
     ap.add_argument('--arenas', type=int, default=1,
                     help='batched workload: arenas (batches) the cases are dealt into, advanced together')
+    ap.add_argument('--lanes', type=int, default=0,
+                    help='split-mode lanes (amr_batch_set_lanes) of the batched and profile legs; 0: default (3)')
     ap.add_argument('--profile', choices=['persistent', 'phases', 'split', 'tiled'], default=None,
                     help='only the timed batched loop, with this launch mode and --block (for ncu)')
     ap.add_argument('--block', type=int, default=128)
@@ -776,6 +784,8 @@ def main():
     ap.add_argument('--accuracy-steps', type=int, default=20000)
     ap.add_argument('--ta-cases', type=int, default=128)
     args = ap.parse_args()
+    global LANES
+    LANES = args.lanes
     args.warmup = max(3, args.warmup)
     rank, world, local = dist_setup(args.gpus)
     if args.impl == 'reference':
